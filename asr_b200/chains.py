@@ -1,0 +1,142 @@
+"""Batched recursion chains and continued fractions on the GPU.
+
+* ``chains_run`` -- the batched chain scheduler (``chain_greens`` / ``chain_worker``, src/asr_class_scf.f90:966-1160):
+  every (group, energy) chain of the energy-dependent route, or one real chain per group in the plain route, in lanes of
+  32 chains per tile;
+* ``edc_green_blk`` -- ``edc_green_blk`` (src/asr_edc.f90:237-316) on the operator's current parameters;
+* ``lanczos`` -- the plain real chain (src/reference/asr_recursion.f90:17-58) on ``augcls_apply``;
+* ``cf_species`` -- terminated continued fractions (src/asr_chain.f90:67-167) for many (chain, energy) pairs.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+from .augcls import AugclsOp, Context, default_context, _f64, _pd, _pi
+
+PREC = {"fp64": _lib.FP64, "fp32": _lib.FP32}
+
+
+@dataclass
+class ChainSpec:
+    """One chain group (``asr_chain_group``): the operator parameters of the chain (9, nsp each), the energy-dependent
+    diagonal X(z) = z pa + pb (edc route), the species frozen on the start site, the start orbital and the depth."""
+    c: np.ndarray
+    d: np.ndarray
+    o: np.ndarray
+    e: np.ndarray
+    pa: np.ndarray | None = None
+    pb: np.ndarray | None = None
+    frozen_sp: int = 0
+    start_orb: int = 1
+    nlev: int = 16
+
+
+def _groups(specs):
+    arr = (_lib.ChainGroup * len(specs))()
+    keep = []
+    for q, s in enumerate(specs):
+        vals = {}
+        for k in ("c", "d", "o", "e", "pa", "pb"):
+            v = getattr(s, k)
+            if v is None:
+                vals[k] = None
+            else:
+                a = _f64(v)
+                keep.append(a)
+                vals[k] = _pd(a)
+        arr[q] = _lib.ChainGroup(vals["c"], vals["d"], vals["o"], vals["e"], vals["pa"], vals["pb"], int(s.frozen_sp),
+                                 int(s.start_orb), int(s.nlev), 0)
+    return arr, keep
+
+
+def chains_run(op: AugclsOp, specs, z, mode: str = "edc", depth_tol: float = 0.0, tail: str = "hull", precision: str = "fp64",
+               project: bool = True, coefs: bool = False):
+    """Run every chain; returns dict(g=(nz, ngroup) complex, m=(nz, ngroup), a, b=(nlevmax, nz, ngroup) if coefs).
+
+    mode 'edc': one complex-symmetric chain per (group, energy); mode 'plain': one real chain per group, whose terminated
+    fraction (tail 'bp': Beer-Pettifor, 'avg2', 'none', 'hull') is evaluated at every energy."""
+    z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
+    nz = z.shape[0]
+    ng = len(specs)
+    nlevmax = max(s.nlev for s in specs)
+    arr, keep = _groups(specs)
+    g = np.zeros((ng, nz), np.complex128)
+    m = np.zeros((ng, nz), np.int32)
+    nab = 1 if mode == "plain" else nz
+    a = np.zeros((ng, nab, nlevmax), np.complex128) if coefs else None
+    b = np.zeros((ng, nab, nlevmax), np.complex128) if coefs else None
+    check(lib().asr_chains_run(op.ctx.h, op.h, arr, ng, _pd(z.view(np.float64)), nz,
+                               _lib.MODE_PLAIN if mode == "plain" else _lib.MODE_EDC, float(depth_tol), _lib.TAILS[tail],
+                               PREC[precision], int(bool(project)), _pd(g.view(np.float64)),
+                               _pd(a.view(np.float64)) if coefs else None, _pd(b.view(np.float64)) if coefs else None, _pi(m)))
+    out = dict(g=g.T, m=m.T)
+    if coefs:
+        out["a"] = a.transpose(2, 1, 0)
+        out["b"] = b.transpose(2, 1, 0)
+    return out
+
+
+def chains_run_device(op: AugclsOp, specs, z_dev, g_dev, nz: int, mode: str = "edc", depth_tol: float = 0.0, tail: str = "hull",
+                      precision: str = "fp64", project: bool = True):
+    """Device-resident form: z_dev / g_dev are device pointers (ints, e.g. torch tensor data_ptr()) of complex128 arrays;
+    g_dev receives (ngroup, nz) in row-major order (lane order)."""
+    arr, keep = _groups(specs)
+    check(lib().asr_chains_run_dev(op.ctx.h, op.h, arr, len(specs), C.c_void_p(z_dev), nz,
+                                   _lib.MODE_PLAIN if mode == "plain" else _lib.MODE_EDC, float(depth_tol), _lib.TAILS[tail],
+                                   PREC[precision], int(bool(project)), C.c_void_p(g_dev), None, None, None))
+
+
+def edc_green_blk(op: AugclsOp, ed: dict, zs, iv: int, nlev: int, depth_tol: float = 0.0, tail: str = "hull",
+                  precision: str = "fp64", project: bool = True):
+    """``edc_green_blk`` (src/asr_edc.f90:237-316) on the operator's current parameters (set_params / freeze_site /
+    set_start): ed holds dc (9), dl (9, nsp), enu (9, nsp).  Returns (g(nb), mused(nb), a(nlev, nb), b(nlev, nb))."""
+    if not 1 <= iv <= 9:
+        raise ValueError("edc_green_blk: the start component must lie on node 1")
+    dc = np.asarray(ed["dc"], float)
+    dl = np.asarray(ed["dl"], float)
+    en = np.asarray(ed["enu"], float)
+    pa = np.asfortranarray(1.0 - dc[:, None] / dl)
+    pb = np.asfortranarray(dc[:, None] * en / dl)
+    p = op.params
+    spec = ChainSpec(c=p["c"], d=p["d"], o=p["o"], e=p["e"], pa=pa, pb=pb, frozen_sp=0, start_orb=iv, nlev=nlev)
+    r = chains_run(op, [spec], zs, "edc", depth_tol, tail, precision, project, coefs=True)
+    return r["g"][:, 0], r["m"][:, 0], r["a"][:, :, 0], r["b"][:, :, 0]
+
+
+def lanczos(op: AugclsOp, l0: int, nmax: int, precision: str = "fp64"):
+    """Reference ``lanczos`` (src/reference/asr_recursion.f90:17-58) from e_(node 1, l0) on the operator's parameters.
+    Returns (a(nmax), b(nmax), n) with b(n) of the last step."""
+    p = op.params
+    spec = ChainSpec(c=p["c"], d=p["d"], o=p["o"], e=p["e"], start_orb=l0, nlev=nmax)
+    r = chains_run(op, [spec], np.zeros(1, complex), "plain", 0.0, "none", precision, project=False, coefs=True)
+    n = int(r["m"][0, 0])
+    return r["a"][:, 0, 0].real.copy(), r["b"][:, 0, 0].real.copy(), n
+
+
+def cf_species(a, b, m, z, tail: str = "hull", ctx: Context | None = None, edges: bool = False):
+    """``cf_species`` for chains a, b (ld, nchain) complex of depths m (nchain) at energies z (nz, nchain) -> g (nz, nchain)."""
+    ctx = ctx or default_context()
+    a = np.asfortranarray(np.asarray(a, np.complex128))
+    b = np.asfortranarray(np.asarray(b, np.complex128))
+    if a.ndim == 1:
+        a = a.reshape(-1, 1, order="F")
+        b = b.reshape(-1, 1, order="F")
+    ld, nc = a.shape
+    if b.shape[0] < ld:
+        b = np.asfortranarray(np.vstack([b, np.zeros((ld - b.shape[0], nc))]))
+    m = np.ascontiguousarray(np.broadcast_to(np.asarray(m, np.int32), (nc,)))
+    z = np.asfortranarray(np.asarray(z, np.complex128).reshape(-1, nc) if np.ndim(z) else np.full((1, nc), z))
+    if z.shape[1] != nc:
+        z = np.asfortranarray(np.repeat(z.reshape(-1, 1), nc, axis=1))
+    nz = z.shape[0]
+    g = np.zeros((nz, nc), np.complex128, order="F")
+    e = np.zeros((2, nz, nc), np.complex128, order="F") if edges else None
+    nf = C.c_int64(0)
+    check(lib().asr_cf_eval(ctx.h, _pd(a.view(np.float64)), _pd(b.view(np.float64)), _pi(m), ld, nc, _pd(z.view(np.float64)), nz,
+                            _lib.TAILS[tail], _pd(g.view(np.float64)), _pd(e.view(np.float64)) if edges else None, C.byref(nf)))
+    return (g, e, nf.value) if edges else g

@@ -1,0 +1,790 @@
+// C ABI of asr_b200 (declarations and reference citations in include/asr_b200.h).
+#include <cstdarg>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cf.cuh"
+#include "chain.cuh"
+#include "op.h"
+
+namespace asrb {
+
+static thread_local std::string g_err;
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+const char* get_error() { return g_err.c_str(); }
+
+// augn_basis + class_mt (src/asr_augcls.f90:73-91, :190-205): mt(l, k, j) = x_j phi_l(j) phi_k(j) on the species of
+// non-zero weight
+void class_mt(const double* conc, int nsc, int nsm, double* mt) {
+  for (int q = 0; q < nsm * nsm * nsm; ++q) mt[q] = 0.0;
+  std::vector<int> sup;
+  for (int j = 0; j < nsc; ++j) if (conc[j] > 0.0) sup.push_back(j);
+  int n = (int)sup.size();
+  std::vector<double> x(n), phi((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) x[j] = conc[sup[j]];
+  auto P = [&](int l, int s) -> double& { return phi[l + (size_t)n * s]; };
+  for (int s = 0; s < n; ++s) P(0, s) = 1.0;
+  for (int l = 1; l < n; ++l) {
+    for (int s = 0; s < n; ++s) P(l, s) = (s == l - 1) ? 1.0 : 0.0;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int m = 0; m < l; ++m) {
+        double ip = 0.0;
+        for (int s = 0; s < n; ++s) ip += x[s] * P(m, s) * P(l, s);
+        for (int s = 0; s < n; ++s) P(l, s) -= ip * P(m, s);
+      }
+    double nr = 0.0;
+    for (int s = 0; s < n; ++s) nr += x[s] * P(l, s) * P(l, s);
+    nr = std::sqrt(nr);
+    for (int s = 0; s < n; ++s) P(l, s) /= nr;
+  }
+  for (int l = 0; l < n; ++l)
+    for (int k = 0; k < n; ++k)
+      for (int j = 0; j < n; ++j) mt[l + nsm * (k + nsm * (size_t)sup[j])] = x[j] * P(l, j) * P(k, j);
+}
+
+namespace {
+
+// local_weights (src/asr_augcls.f90:362-377) into the device layout W[kap][own][flip][l]
+void weights(const asr_op* op, const double* par, double* W) {
+  const int nsm = op->nsmax;
+  for (int kap = 0; kap < op->ncls; ++kap)
+    for (int kk = 0; kk < nsm; ++kk)
+      for (int k = 0; k < nsm; ++k)
+        for (int lam = 0; lam < 9; ++lam) {
+          double w = 0.0;
+          if (k < op->nsc[kap] && kk < op->nsc[kap])
+            for (int s = 0; s < op->nsc[kap]; ++s)
+              w += par[lam + 9 * (size_t)(op->spc[s + (size_t)op->ldspc * kap] - 1)] * op->mt[k + nsm * (kk + nsm * (s + (size_t)nsm * kap))];
+          W[((kap * nsm + k) * nsm + kk) * 9 + lam] = w;
+        }
+}
+
+GroupLayout layout(const asr_op* op) {
+  GroupLayout GL;
+  GL.nw = op->ncls * op->nsmax * op->nsmax * 9;
+  GL.np = 9 * op->nsp;
+  GL.stride = NPAR * (GL.nw + GL.np);
+  return GL;
+}
+
+bool all_equal_species(const double* p, int nsp) {
+  for (int s = 1; s < nsp; ++s)
+    for (int l = 0; l < 9; ++l) if (p[l + 9 * s] != p[l]) return false;
+  return true;
+}
+bool all_zero(const double* p, int n) {
+  for (int q = 0; q < n; ++q) if (p[q] != 0.0) return false;
+  return true;
+}
+
+// one group: parameters -> blob + info
+int make_group(const asr_op* op, const GroupLayout& GL, const double* c, const double* d, const double* o, const double* e,
+               const double* pa, const double* pb, int frozen_sp, int l0, int nlev, const double* chi_override, double* blob,
+               GroupInfo& gi) {
+  const int np = 9 * op->nsp;
+  std::vector<double> zero(np, 0.0), ceb(np), eb(np);
+  const double* P[NPAR];
+  P[PC] = c; P[PD] = d; P[PO] = o ? o : zero.data(); P[PE] = e ? e : zero.data();
+  P[PA] = pa ? pa : zero.data(); P[PB] = pb ? pb : zero.data();
+  for (int q = 0; q < np; ++q) { ceb[q] = P[PC][q] + P[PE][q] + P[PB][q]; eb[q] = P[PE][q] + P[PB][q]; }
+  P[PCEB] = ceb.data(); P[PEB] = eb.data();
+  for (int p = 0; p < NPAR; ++p) {
+    weights(op, P[p], blob + GL.w(p));
+    for (int q = 0; q < np; ++q) blob[GL.raw(p) + q] = P[p][q];
+  }
+  gi.flags = 0;
+  if (all_equal_species(P[PD], op->nsp)) gi.flags |= GF_D_UNIFORM;
+  if (all_zero(P[PO], np)) gi.flags |= GF_O_ZERO;
+  if (all_zero(P[PE], np)) gi.flags |= GF_E_ZERO;
+  if (all_zero(P[PA], np) && all_zero(P[PB], np)) gi.flags |= GF_X_ZERO;
+  for (int l = 0; l < 9; ++l) gi.dd[l] = P[PD][l];
+  if (frozen_sp < 0 || frozen_sp > op->nsp) { set_error("chain group: frozen species out of range"); return ASR_EINVAL; }
+  gi.frozen_sp = frozen_sp;
+  if (l0 < 1 || l0 > 9) { set_error("chain group: start orbital out of range"); return ASR_EINVAL; }
+  gi.l0 = l0;
+  gi.nlev = nlev;
+  gi.chimask = 0ull;
+  if (op->nop > MAXOP) { set_error("chain group: at most %d operations", MAXOP); return ASR_EINVAL; }
+  for (int g = 0; g < op->nop; ++g) {
+    double v;
+    if (chi_override) v = chi_override[g];
+    else {
+      v = op->dmat[(l0 - 1) + 9 * ((l0 - 1) + 9 * (size_t)g)];
+      if (std::fabs(std::fabs(v) - 1.0) > 1.0e-9) {   // augcls_set_start, src/asr_augcls.f90:113-115
+        set_error("augcls_set_start: start orbital is not one-dimensional under the group");
+        return ASR_EINVAL;
+      }
+    }
+    if (v < 0) gi.chimask |= (1ull << g);
+  }
+  return ASR_OK;
+}
+
+int upload_tables(asr_op* op, const double* dmat, const double* block, int nsb, int ntb, const double* block0) {
+  cudaStream_t s = op->ctx->stream;
+  const int nop = op->nop, ns = op->nslot, nty = op->ntype;
+  op->dmat.assign(dmat, dmat + 81 * (size_t)nop);
+  op->pi.assign(9 * (size_t)nop, 0);
+  op->sg.assign(9 * (size_t)nop, 0.0);
+  std::vector<uint8_t> pi0(9 * (size_t)nop);
+  std::vector<uint16_t> sgm(nop, 0);
+  for (int g = 0; g < nop; ++g)   // orbital operation tables: D[pi(l), l] = sg(l)  (src/asr_augcls.f90:728-736)
+    for (int l = 0; l < 9; ++l) {
+      for (int jj = 0; jj < 9; ++jj) {
+        double v = dmat[jj + 9 * (l + 9 * (size_t)g)];
+        if (std::fabs(v) > 0.5) { op->pi[l + 9 * g] = jj + 1; op->sg[l + 9 * g] = v; }
+      }
+      if (op->pi[l + 9 * g] == 0) { set_error("build_augcls_operator: orbital operation is not monomial"); return ASR_EINVAL; }
+      pi0[g * 9 + l] = (uint8_t)(op->pi[l + 9 * g] - 1);
+      if (op->sg[l + 9 * g] < 0) sgm[g] |= (uint16_t)(1u << l);
+    }
+  if (nsb < ns) { set_error("build_augcls_operator: fewer bond blocks than neighbour slots"); return ASR_EINVAL; }
+  if (ntb < nty) { set_error("build_augcls_operator: site type without a bond table"); return ASR_EINVAL; }
+  // unrotated blocks [t][kk][l][l'] (kk = 0: on-site)
+  std::vector<double> B((size_t)nty * (ns + 1) * 81, 0.0);
+  for (int t = 0; t < nty; ++t) {
+    for (int l = 0; l < 9; ++l)
+      for (int lp = 0; lp < 9; ++lp) {
+        if (block0) B[((size_t)t * (ns + 1)) * 81 + l * 9 + lp] = block0[l + 9 * (lp + 9 * (size_t)t)];
+        for (int k = 0; k < ns; ++k)
+          B[((size_t)t * (ns + 1) + k + 1) * 81 + l * 9 + lp] = block[l + 9 * (lp + 9 * (k + (size_t)nsb * t))];
+      }
+  }
+  op->block.assign(B.begin(), B.end());
+  std::vector<float> Bf(B.begin(), B.end());
+  std::vector<int8_t> nsc8(op->ncls);
+  for (int k = 0; k < op->ncls; ++k) nsc8[k] = (int8_t)op->nsc[k];
+  ASR_CUDA(cudaMalloc(&op->d_blocks, B.size() * sizeof(double)));
+  ASR_CUDA(cudaMalloc(&op->d_blocks_f, B.size() * sizeof(float)));
+  ASR_CUDA(cudaMalloc(&op->d_pi, pi0.size()));
+  ASR_CUDA(cudaMalloc(&op->d_sgm, sgm.size() * sizeof(uint16_t)));
+  ASR_CUDA(cudaMalloc(&op->d_nsc, nsc8.size()));
+  ASR_CUDA(cudaMemcpyAsync(op->d_blocks, B.data(), B.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(op->d_blocks_f, Bf.data(), Bf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(op->d_pi, pi0.data(), pi0.size(), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(op->d_sgm, sgm.data(), sgm.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(op->d_nsc, nsc8.data(), nsc8.size(), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  return ASR_OK;
+}
+
+void free_op(asr_op* op) {
+  void* ptrs[] = {op->d_site, op->d_level, op->d_orb, op->d_lst, op->d_ncl, op->d_typ, op->d_start, op->d_frozen, op->d_sq,
+                  op->d_isq, op->d_flipr, op->d_hopr, op->d_stab_ptr, op->d_flipg, op->d_hopg, op->d_stab, op->d_nsc,
+                  op->d_pi, op->d_sgm, op->d_blocks, op->d_blocks_f};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  delete op;
+}
+
+int set_device(asr_ctx* ctx) {
+  ASR_CUDA(cudaSetDevice(ctx->device));
+  return ASR_OK;
+}
+
+}  // namespace
+}  // namespace asrb
+
+using namespace asrb;
+
+extern "C" {
+
+int asr_version(void) { return 100; }
+
+int asr_last_error(char* buf, size_t n) {
+  if (!buf || n == 0) return ASR_EINVAL;
+  std::strncpy(buf, get_error(), n - 1);
+  buf[n - 1] = 0;
+  return ASR_OK;
+}
+
+int asr_ctx_create(int device, asr_ctx** out) {
+  if (!out) { set_error("asr_ctx_create: null output"); return ASR_EINVAL; }
+  *out = nullptr;
+  int ndev = 0;
+  ASR_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) { set_error("asr_ctx_create: device %d of %d", device, ndev); return ASR_EINVAL; }
+  ASR_CUDA(cudaSetDevice(device));
+  asr_ctx* c = new asr_ctx();
+  c->device = device;
+  cudaDeviceProp prop;
+  ASR_CUDA(cudaGetDeviceProperties(&prop, device));
+  c->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess) {
+    set_error("asr_ctx_create: stream / allocation failed");
+    delete c;
+    return ASR_ECUDA;
+  }
+  cudaMemset(c->d_err, 0, sizeof(int));
+  c->stream = c->own_stream;
+  *out = c;
+  return ASR_OK;
+}
+
+int asr_ctx_destroy(asr_ctx* ctx) {
+  if (!ctx) return ASR_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  if (ctx->d_err) cudaFree(ctx->d_err);
+  for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+  delete ctx;
+  return ASR_OK;
+}
+
+int asr_ctx_set_stream(asr_ctx* ctx, void* stream) {
+  if (!ctx) { set_error("asr_ctx_set_stream: null context"); return ASR_EINVAL; }
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return ASR_OK;
+}
+
+int asr_ctx_profile(asr_ctx* ctx, int on) {
+  if (!ctx) { set_error("asr_ctx_profile: null context"); return ASR_EINVAL; }
+  ctx->profile = on;
+  if (on) { ctx->prof_ms = 0.0; ctx->prof_bytes = 0.0; ctx->prof_flops = 0.0; ctx->prof_launches = 0; }
+  return ASR_OK;
+}
+
+int asr_ctx_kernel_stats(const asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops) {
+  if (!ctx) { set_error("asr_ctx_kernel_stats: null context"); return ASR_EINVAL; }
+  if (ms) *ms = ctx->prof_ms;
+  if (launches) *launches = ctx->prof_launches;
+  if (bytes) *bytes = ctx->prof_bytes;
+  if (flops) *flops = ctx->prof_flops;
+  return ASR_OK;
+}
+
+int asr_ctx_sync(asr_ctx* ctx) {
+  ASR_TRY(set_device(ctx));
+  ASR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return ASR_OK;
+}
+
+int asr_ctx_stats(const asr_ctx* ctx, int64_t* nchain, int64_t* nlev, int64_t* nfall) {
+  if (nchain) *nchain = ctx->nchain;
+  if (nlev) *nlev = ctx->nlev;
+  if (nfall) *nfall = ctx->nfall;
+  return ASR_OK;
+}
+
+int asr_op_build(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc, int ldspc,
+                 const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat, int start,
+                 int maxlevel, int maxrank, const int* flippable, const int* stype, const double* block, int nblock_slots,
+                 int ntype_blocks, const double* block0, asr_op** out) {
+  if (!ctx || !out || !nbr_ptr || !nbr || !nsc || !spc || !conc || !cls || !perm || !dmat || !block) {
+    set_error("asr_op_build: null argument");
+    return ASR_EINVAL;
+  }
+  *out = nullptr;
+  if (nsite < 1 || ncls < 1 || nop < 1 || nsp < 1 || ldspc < 1) { set_error("asr_op_build: empty input"); return ASR_EINVAL; }
+  ASR_TRY(set_device(ctx));
+  for (int k = 0; k < ncls; ++k) {
+    if (nsc[k] < 1 || nsc[k] > ldspc) { set_error("asr_op_build: species count of class %d", k + 1); return ASR_EINVAL; }
+    double sum = 0.0;
+    for (int j = 0; j < nsc[k]; ++j) {
+      int sp = spc[j + (size_t)ldspc * k];
+      if (sp < 1 || sp > nsp) { set_error("asr_op_build: species index out of range"); return ASR_EINVAL; }
+      if (conc[j + (size_t)ldspc * k] < 0.0) { set_error("asr_op_build: negative concentration"); return ASR_EINVAL; }
+      sum += conc[j + (size_t)ldspc * k];
+    }
+    if (std::fabs(sum - 1.0) > 1.0e-8) { set_error("asr_op_build: concentrations of class %d do not sum to 1", k + 1); return ASR_EINVAL; }
+  }
+  for (int i = 0; i < nsite; ++i) if (cls[i] < 1 || cls[i] > ncls) { set_error("asr_op_build: site class out of range"); return ASR_EINVAL; }
+  int nty = 1;
+  if (stype) for (int i = 0; i < nsite; ++i) {
+    if (stype[i] < 1) { set_error("build_augcls_operator: site type without a bond table"); return ASR_EINVAL; }
+    nty = std::max(nty, stype[i]);
+  }
+  if (nty > ntype_blocks) { set_error("build_augcls_operator: site type without a bond table"); return ASR_EINVAL; }
+  asr_op* op = new asr_op();
+  op->ctx = ctx;
+  op->nsp = nsp;
+  op->ntype = nty;
+  op->nsc.assign(nsc, nsc + ncls);
+  op->ldspc = ldspc;
+  op->spc.assign(spc, spc + (size_t)ldspc * ncls);
+  int rc = build_operator(ctx, nsite, nbr_ptr, nbr, ncls, nsc, cls, perm, nop, start, maxlevel, maxrank, flippable, stype, op);
+  if (rc != ASR_OK) { free_op(op); return rc; }
+  const int nsm = op->nsmax;
+  op->mt.assign((size_t)nsm * nsm * nsm * ncls, 0.0);
+  for (int k = 0; k < ncls; ++k) class_mt(conc + (size_t)ldspc * k, nsc[k], nsm, &op->mt[(size_t)nsm * nsm * nsm * k]);
+  rc = upload_tables(op, dmat, block, nblock_slots, ntype_blocks, block0);
+  if (rc != ASR_OK) { free_op(op); return rc; }
+  op->c.assign(9 * (size_t)nsp, 0.0); op->d = op->c; op->o = op->c; op->e = op->c;
+  op->frozen_h.assign(op->nn, 0);
+  op->chi.assign(nop, 1.0);
+  op->start_l = 1;
+  *out = op;
+  return ASR_OK;
+}
+
+int asr_op_free(asr_op* op) {
+  if (!op) return ASR_OK;
+  cudaSetDevice(op->ctx->device);
+  free_op(op);
+  return ASR_OK;
+}
+
+int asr_op_dims(const asr_op* op, int* dims) {
+  if (!op || !dims) { set_error("asr_op_dims: null argument"); return ASR_EINVAL; }
+  dims[0] = op->nn; dims[1] = op->nslot; dims[2] = op->nsmax; dims[3] = op->nop; dims[4] = op->ncls; dims[5] = op->ntype;
+  dims[6] = op->nstab; dims[7] = op->nsp;
+  return ASR_OK;
+}
+
+int asr_op_export_tables(const asr_op* op, int* flipr, int* flipg, int* hopr, int* hopg, int* lst, int* site, int* ncl, int* level,
+                         double* norb, double* sq, int* stab_ptr, int* stab) {
+  if (!op) { set_error("asr_op_export_tables: null operator"); return ASR_EINVAL; }
+  asr_ctx* ctx = op->ctx;
+  ASR_TRY(set_device(ctx));
+  cudaStream_t s = ctx->stream;
+  const size_t nn = op->nn, nsm = op->nsmax, ns = op->nslot;
+  std::vector<int> fr(nsm * nn), hr(ns * nn), sp(nn + 1), st(nn), lv(nn), ob(nn);
+  std::vector<uint8_t> fg(nsm * nn), hg(ns * nn), sb(std::max(op->nstab, 1));
+  std::vector<int8_t> ls(nn), nc(nn);
+  std::vector<double> sqv(nn);
+  ASR_CUDA(cudaMemcpyAsync(fr.data(), op->d_flipr, fr.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(fg.data(), op->d_flipg, fg.size(), cudaMemcpyDeviceToHost, s));
+  if (ns) {
+    ASR_CUDA(cudaMemcpyAsync(hr.data(), op->d_hopr, hr.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaMemcpyAsync(hg.data(), op->d_hopg, hg.size(), cudaMemcpyDeviceToHost, s));
+  }
+  ASR_CUDA(cudaMemcpyAsync(sp.data(), op->d_stab_ptr, sp.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (op->nstab) ASR_CUDA(cudaMemcpyAsync(sb.data(), op->d_stab, op->nstab, cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(st.data(), op->d_site, nn * sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(lv.data(), op->d_level, nn * sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(ob.data(), op->d_orb, nn * sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(ls.data(), op->d_lst, nn, cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(nc.data(), op->d_ncl, nn, cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(sqv.data(), op->d_sq, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  for (size_t q = 0; q < nsm * nn; ++q) {
+    if (flipr) flipr[q] = fr[q] + 1;    // -1 -> 0 (absent), 0-based -> 1-based
+    if (flipg) flipg[q] = fg[q] + 1;
+  }
+  for (size_t q = 0; q < ns * nn; ++q) {
+    if (hopr) hopr[q] = hr[q] + 1;
+    if (hopg) hopg[q] = hg[q] + 1;
+  }
+  for (size_t i = 0; i < nn; ++i) {
+    if (lst) lst[i] = ls[i];
+    if (site) site[i] = st[i];
+    if (ncl) ncl[i] = nc[i] + 1;
+    if (level) level[i] = lv[i];
+    if (norb) norb[i] = (double)ob[i];
+    if (sq) sq[i] = sqv[i];
+  }
+  if (stab_ptr) for (size_t i = 0; i <= nn; ++i) stab_ptr[i] = sp[i] + 1;
+  if (stab) for (int q = 0; q < op->nstab; ++q) stab[q] = sb[q] + 1;
+  return ASR_OK;
+}
+
+int asr_op_set_params(asr_op* op, const double* c, const double* d, const double* o, const double* e) {
+  if (!op || !c || !d || !o || !e) { set_error("augcls_set_params: null argument"); return ASR_EINVAL; }
+  size_t m = 9 * (size_t)op->nsp;
+  op->c.assign(c, c + m); op->d.assign(d, d + m); op->o.assign(o, o + m); op->e.assign(e, e + m);
+  return ASR_OK;
+}
+
+int asr_op_freeze_site(asr_op* op, int site, int sp) {
+  if (!op) { set_error("augcls_freeze_site: null operator"); return ASR_EINVAL; }
+  if (sp < 1 || sp > op->nsp) { set_error("augcls_freeze_any: species index out of range"); return ASR_EINVAL; }
+  ASR_TRY(set_device(op->ctx));
+  cudaStream_t s = op->ctx->stream;
+  const size_t nn = op->nn, nsm = op->nsmax;
+  std::vector<int> st(nn), fr(nsm * nn);
+  std::vector<int8_t> ls(nn);
+  ASR_CUDA(cudaMemcpyAsync(st.data(), op->d_site, nn * sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(fr.data(), op->d_flipr, fr.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(ls.data(), op->d_lst, nn, cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  for (size_t i = 0; i < nn; ++i) {
+    if (st[i] != site) continue;
+    int nz = 0;
+    for (size_t k = 0; k < nsm; ++k) if (fr[k + nsm * i] >= 0) ++nz;
+    if (ls[i] != 0 || nz > 1) { set_error("augcls_freeze_site: the frozen site was flippable"); return ASR_EINVAL; }
+    op->frozen_h[i] = (int8_t)sp;
+  }
+  ASR_CUDA(cudaMemcpyAsync(op->d_frozen, op->frozen_h.data(), nn, cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  return ASR_OK;
+}
+
+int asr_op_unfreeze(asr_op* op) {
+  if (!op) { set_error("asr_op_unfreeze: null operator"); return ASR_EINVAL; }
+  ASR_TRY(set_device(op->ctx));
+  std::fill(op->frozen_h.begin(), op->frozen_h.end(), 0);
+  ASR_CUDA(cudaMemsetAsync(op->d_frozen, 0, op->nn, op->ctx->stream));
+  ASR_CUDA(cudaStreamSynchronize(op->ctx->stream));
+  return ASR_OK;
+}
+
+int asr_op_set_start(asr_op* op, int l0) {
+  if (!op || l0 < 1 || l0 > 9) { set_error("augcls_set_start: start orbital out of range"); return ASR_EINVAL; }
+  for (int g = 0; g < op->nop; ++g) {
+    double v = op->dmat[(l0 - 1) + 9 * ((l0 - 1) + 9 * (size_t)g)];
+    if (std::fabs(std::fabs(v) - 1.0) > 1.0e-9) {
+      set_error("augcls_set_start: start orbital is not one-dimensional under the group");
+      return ASR_EINVAL;
+    }
+  }
+  op->start_l = l0;
+  for (int g = 0; g < op->nop; ++g) op->chi[g] = op->dmat[(l0 - 1) + 9 * ((l0 - 1) + 9 * (size_t)g)] >= 0 ? 1.0 : -1.0;
+  return ASR_OK;
+}
+
+int asr_op_set_chi(asr_op* op, const double* chi) {
+  if (!op || !chi) { set_error("augcls_set_chi: null argument"); return ASR_EINVAL; }
+  for (int g = 0; g < op->nop; ++g) {
+    if (std::fabs(std::fabs(chi[g]) - 1.0) > 1.0e-12) { set_error("augcls_set_chi: characters must be +-1"); return ASR_EINVAL; }
+    op->chi[g] = chi[g];
+  }
+  return ASR_OK;
+}
+
+int asr_op_set_class_conc(asr_op* op, int kap, const double* conc) {
+  if (!op || !conc || kap < 1 || kap > op->ncls) { set_error("augcls_set_class_conc: class out of range"); return ASR_EINVAL; }
+  int nsc = op->nsc[kap - 1];
+  double s = 0.0;
+  for (int k = 0; k < nsc; ++k) {
+    if (conc[k] < 0.0) { set_error("augcls_set_class_conc: concentrations"); return ASR_EINVAL; }
+    s += conc[k];
+  }
+  if (std::fabs(s - 1.0) > 1.0e-8) { set_error("augcls_set_class_conc: concentrations"); return ASR_EINVAL; }
+  const int nsm = op->nsmax;
+  class_mt(conc, nsc, nsm, &op->mt[(size_t)nsm * nsm * nsm * (kap - 1)]);
+  return ASR_OK;
+}
+
+static int op_group(asr_op* op, const GroupLayout& GL, const double* pa, const double* pb, std::vector<double>& blob,
+                    std::vector<GroupInfo>& gi) {
+  blob.assign(GL.stride, 0.0);
+  gi.resize(1);
+  return make_group(op, GL, op->c.data(), op->d.data(), op->o.data(), op->e.data(), pa, pb, 0, op->start_l, 1, op->chi.data(),
+                    blob.data(), gi[0]);
+}
+
+int asr_op_apply(asr_op* op, const double* x, double* y, int nvec) {
+  if (!op || !x || !y || nvec < 1) { set_error("augcls_apply: bad argument"); return ASR_EINVAL; }
+  ASR_TRY(set_device(op->ctx));
+  GroupLayout GL = layout(op);
+  std::vector<double> blob;
+  std::vector<GroupInfo> gi;
+  ASR_TRY(op_group(op, GL, nullptr, nullptr, blob, gi));
+  return apply_vectors(op->ctx, op, gi, blob, GL, nvec, x, false, y, APPLY_H);
+}
+
+int asr_op_rand_c(asr_op* op, const double* par, const double* x, double* w, int nvec) {
+  if (!op || !par || !x || !w || nvec < 1) { set_error("augcls_rand_c: bad argument"); return ASR_EINVAL; }
+  ASR_TRY(set_device(op->ctx));
+  GroupLayout GL = layout(op);
+  const int np = 9 * op->nsp;
+  std::vector<double> pr(np), pim(np);
+  for (int q = 0; q < np; ++q) { pr[q] = par[2 * q]; pim[q] = par[2 * q + 1]; }
+  std::vector<double> blob;
+  std::vector<GroupInfo> gi;
+  ASR_TRY(op_group(op, GL, pim.data(), pr.data(), blob, gi));   // X(z) = z pa + pb at z = i
+  return apply_vectors(op->ctx, op, gi, blob, GL, nvec, x, true, w, APPLY_RAND_Z);
+}
+
+int asr_op_project_c(asr_op* op, double* x, int nvec) {
+  if (!op || !x || nvec < 1) { set_error("augcls_project_c: bad argument"); return ASR_EINVAL; }
+  ASR_TRY(set_device(op->ctx));
+  GroupLayout GL = layout(op);
+  std::vector<double> blob;
+  std::vector<GroupInfo> gi;
+  ASR_TRY(op_group(op, GL, nullptr, nullptr, blob, gi));
+  return apply_vectors(op->ctx, op, gi, blob, GL, nvec, x, true, x, APPLY_PROJECT);
+}
+
+static int chains_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double2* d_z, int nz, int mode,
+                         double depth_tol, int tail, int precision, int project, double2* d_g, double* a, double* b,
+                         int* mused) {
+  if (!ctx || !op || !groups || ngroup < 1 || nz < 0) { set_error("asr_chains_run: bad argument"); return ASR_EINVAL; }
+  if (mode != ASR_MODE_PLAIN && mode != ASR_MODE_EDC) { set_error("asr_chains_run: unknown mode"); return ASR_EINVAL; }
+  if (tail < 0 || tail > 3) { set_error("asr_chains_run: unknown tail"); return ASR_EINVAL; }
+  ASR_TRY(set_device(ctx));
+  cudaStream_t s = ctx->stream;
+  GroupLayout GL = layout(op);
+  std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
+  std::vector<GroupInfo> gi(ngroup);
+  int nlevmax = 0;
+  for (int q = 0; q < ngroup; ++q) {
+    const asr_chain_group& G = groups[q];
+    if (!G.c || !G.d) { set_error("asr_chains_run: group %d without c or d", q + 1); return ASR_EINVAL; }
+    if (G.nlev < 1 || G.nlev > NLMAX) { set_error("asr_chains_run: depth %d out of range 1..%d", G.nlev, NLMAX); return ASR_EINVAL; }
+    ASR_TRY(make_group(op, GL, G.c, G.d, G.o, G.e, mode == ASR_MODE_EDC ? G.pa : nullptr, mode == ASR_MODE_EDC ? G.pb : nullptr,
+                       G.frozen_sp, G.start_orb, G.nlev, nullptr, blob.data() + (size_t)GL.stride * q, gi[q]));
+    nlevmax = std::max(nlevmax, G.nlev);
+  }
+  RunOptions opt;
+  opt.mode = mode;
+  opt.depth_tol = mode == ASR_MODE_EDC ? depth_tol : 0.0;
+  opt.tail = tail;
+  opt.precision = precision;
+  opt.project = project;
+  std::vector<double2> ha, hb;
+  std::vector<int> hm;
+  int64_t nfall = 0, nsteps = 0;
+  const bool want_ab = a || b || mode == ASR_MODE_PLAIN;
+  if (mode == ASR_MODE_EDC) {
+    const int nlane = ngroup * nz;
+    std::vector<int> lg(nlane);
+    for (int q = 0; q < ngroup; ++q)
+      for (int j = 0; j < nz; ++j) lg[(size_t)q * nz + j] = q;
+    double2* d_lz = nullptr;
+    ASR_CUDA(cudaMalloc(&d_lz, std::max(nlane, 1) * sizeof(double2)));
+    for (int q = 0; q < ngroup; ++q)
+      cudaMemcpyAsync(d_lz + (size_t)q * nz, d_z, nz * sizeof(double2), cudaMemcpyDeviceToDevice, s);
+    int rc = run_lanes(ctx, op, gi, blob, GL, lg, d_lz, nlane, opt, d_g, want_ab ? &ha : nullptr, want_ab ? &hb : nullptr, &hm,
+                       &nfall, &nsteps);
+    cudaFree(d_lz);
+    if (rc != ASR_OK) return rc;
+    for (int L = 0; L < nlane; ++L) {
+      if (mused) mused[L] = hm[L];
+      for (int k = 0; k < nlevmax; ++k) {
+        size_t dst = 2 * ((size_t)L * nlevmax + k);
+        if (a) { a[dst] = ha[(size_t)L * NLMAX + k].x; a[dst + 1] = ha[(size_t)L * NLMAX + k].y; }
+        if (b) { b[dst] = hb[(size_t)L * NLMAX + k].x; b[dst + 1] = hb[(size_t)L * NLMAX + k].y; }
+      }
+    }
+    ctx->nchain += nlane;
+  } else {
+    // plain: one real chain per group, then the terminated fraction at every energy
+    std::vector<int> lg(ngroup);
+    for (int q = 0; q < ngroup; ++q) lg[q] = q;
+    double2* d_lz = nullptr;
+    ASR_CUDA(cudaMalloc(&d_lz, ngroup * sizeof(double2)));
+    ASR_CUDA(cudaMemsetAsync(d_lz, 0, ngroup * sizeof(double2), s));
+    int rc = run_lanes(ctx, op, gi, blob, GL, lg, d_lz, ngroup, opt, nullptr, &ha, &hb, &hm, &nfall, &nsteps);
+    cudaFree(d_lz);
+    if (rc != ASR_OK) return rc;
+    // plain lanczos returns n levels with b(n) (src/reference/asr_recursion.f90:57)
+    std::vector<double> ra((size_t)ngroup * NLMAX), rb((size_t)ngroup * NLMAX);
+    std::vector<int> rn(ngroup);
+    for (int q = 0; q < ngroup; ++q) {
+      rn[q] = hm[q];
+      for (int k = 0; k < NLMAX; ++k) { ra[(size_t)q * NLMAX + k] = ha[(size_t)q * NLMAX + k].x; rb[(size_t)q * NLMAX + k] = hb[(size_t)q * NLMAX + k].x; }
+      if (mused) for (int j = 0; j < nz; ++j) mused[(size_t)q * nz + j] = hm[q];
+      for (int k = 0; k < nlevmax; ++k) {
+        size_t dst = 2 * ((size_t)q * nlevmax + k);
+        if (a) { a[dst] = ra[(size_t)q * NLMAX + k]; a[dst + 1] = 0.0; }
+        if (b) { b[dst] = rb[(size_t)q * NLMAX + k]; b[dst + 1] = 0.0; }
+      }
+    }
+    if (d_g && nz > 0) {
+      double *d_a = nullptr, *d_b = nullptr, *d_ai = nullptr, *d_bi = nullptr;
+      int* d_n = nullptr;
+      ASR_CUDA(cudaMalloc(&d_a, ra.size() * sizeof(double)));
+      ASR_CUDA(cudaMalloc(&d_b, rb.size() * sizeof(double)));
+      ASR_CUDA(cudaMalloc(&d_ai, ngroup * sizeof(double)));
+      ASR_CUDA(cudaMalloc(&d_bi, ngroup * sizeof(double)));
+      ASR_CUDA(cudaMalloc(&d_n, ngroup * sizeof(int)));
+      ASR_CUDA(cudaMemcpyAsync(d_a, ra.data(), ra.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+      ASR_CUDA(cudaMemcpyAsync(d_b, rb.data(), rb.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+      ASR_CUDA(cudaMemcpyAsync(d_n, rn.data(), ngroup * sizeof(int), cudaMemcpyHostToDevice, s));
+      if (tail == ASR_TAIL_HULL) {
+        // the complex cf_species hull tail on the real chain
+        std::vector<double2> ca((size_t)ngroup * NLMAX), cb((size_t)ngroup * NLMAX);
+        for (size_t q = 0; q < ca.size(); ++q) { ca[q] = make_double2(ra[q], 0.0); cb[q] = make_double2(rb[q], 0.0); }
+        double2 *d_ca = nullptr, *d_cb = nullptr, *d_zz = nullptr;
+        int* d_nf = nullptr;
+        ASR_CUDA(cudaMalloc(&d_ca, ca.size() * sizeof(double2)));
+        ASR_CUDA(cudaMalloc(&d_cb, cb.size() * sizeof(double2)));
+        ASR_CUDA(cudaMalloc(&d_zz, (size_t)nz * ngroup * sizeof(double2)));
+        ASR_CUDA(cudaMalloc(&d_nf, sizeof(int)));
+        ASR_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(int), s));
+        ASR_CUDA(cudaMemcpyAsync(d_ca, ca.data(), ca.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+        ASR_CUDA(cudaMemcpyAsync(d_cb, cb.data(), cb.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+        for (int q = 0; q < ngroup; ++q)
+          ASR_CUDA(cudaMemcpyAsync(d_zz + (size_t)q * nz, d_z, nz * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+        long nt = (long)nz * ngroup;
+        k_cf_eval<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(d_ca, d_cb, d_n, NLMAX, ngroup, d_zz, nz, tail, d_g, nullptr, d_nf);
+        ASR_CUDA(cudaStreamSynchronize(s));
+        cudaFree(d_ca); cudaFree(d_cb); cudaFree(d_zz); cudaFree(d_nf);
+      } else {
+        k_real_tail<<<(ngroup + 63) / 64, 64, 0, s>>>(d_a, d_b, d_n, NLMAX, ngroup, tail, d_ai, d_bi);
+        long nt = (long)nz * ngroup;
+        k_real_green<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(d_a, d_b, d_n, NLMAX, ngroup, d_ai, d_bi, tail, d_z, nz, d_g);
+        ASR_CUDA(cudaStreamSynchronize(s));
+      }
+      ASR_CUDA(cudaGetLastError());
+      cudaFree(d_a); cudaFree(d_b); cudaFree(d_ai); cudaFree(d_bi); cudaFree(d_n);
+    }
+    ctx->nchain += ngroup;
+  }
+  ctx->nlev += nsteps;
+  ctx->nfall += nfall;
+  return ASR_OK;
+}
+
+int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const void* z_dev, int nz, int mode,
+                       double depth_tol, int tail, int precision, int project, void* g_dev, double* a, double* b, int* mused) {
+  return chains_common(ctx, op, groups, ngroup, (const double2*)z_dev, nz, mode, depth_tol, tail, precision, project,
+                       (double2*)g_dev, a, b, mused);
+}
+
+int asr_chains_run(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz, int mode,
+                   double depth_tol, int tail, int precision, int project, double* g, double* a, double* b, int* mused) {
+  if (!ctx || !z || !g) { set_error("asr_chains_run: null argument"); return ASR_EINVAL; }
+  ASR_TRY(set_device(ctx));
+  cudaStream_t s = ctx->stream;
+  const size_t ng = mode == ASR_MODE_EDC ? (size_t)nz * ngroup : (size_t)nz * ngroup;
+  double2 *d_z = nullptr, *d_g = nullptr;
+  ASR_CUDA(cudaMalloc(&d_z, std::max(nz, 1) * sizeof(double2)));
+  ASR_CUDA(cudaMalloc(&d_g, std::max<size_t>(ng, 1) * sizeof(double2)));
+  ASR_CUDA(cudaMemcpyAsync(d_z, z, nz * sizeof(double2), cudaMemcpyHostToDevice, s));
+  int rc = chains_common(ctx, op, groups, ngroup, d_z, nz, mode, depth_tol, tail, precision, project, d_g, a, b, mused);
+  if (rc == ASR_OK) {
+    cudaMemcpyAsync(g, d_g, ng * sizeof(double2), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) { set_error("asr_chains_run: copy back failed"); rc = ASR_ECUDA; }
+  }
+  cudaFree(d_z);
+  cudaFree(d_g);
+  return rc;
+}
+
+int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain, const double* z, int nz, int tail,
+                double* g, double* edges, int64_t* nfall) {
+  if (!ctx || !a || !b || !m || !z || !g || ld < 1 || nchain < 1 || nz < 1) { set_error("asr_cf_eval: bad argument"); return ASR_EINVAL; }
+  for (int c = 0; c < nchain; ++c)
+    if (m[c] < 1 || m[c] > ld || m[c] > CF_NMAX) { set_error("asr_cf_eval: depth of chain %d out of range", c + 1); return ASR_EINVAL; }
+  ASR_TRY(set_device(ctx));
+  cudaStream_t s = ctx->stream;
+  size_t nab = (size_t)ld * nchain, nzz = (size_t)nz * nchain;
+  double2 *d_a, *d_b, *d_z, *d_g, *d_e = nullptr;
+  int *d_m, *d_nf;
+  ASR_CUDA(cudaMalloc(&d_a, nab * sizeof(double2)));
+  ASR_CUDA(cudaMalloc(&d_b, nab * sizeof(double2)));
+  ASR_CUDA(cudaMalloc(&d_z, nzz * sizeof(double2)));
+  ASR_CUDA(cudaMalloc(&d_g, nzz * sizeof(double2)));
+  ASR_CUDA(cudaMalloc(&d_m, nchain * sizeof(int)));
+  ASR_CUDA(cudaMalloc(&d_nf, sizeof(int)));
+  if (edges) ASR_CUDA(cudaMalloc(&d_e, 2 * nzz * sizeof(double2)));
+  ASR_CUDA(cudaMemcpyAsync(d_a, a, nab * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_b, b, nab * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_z, z, nzz * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_m, m, nchain * sizeof(int), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(int), s));
+  k_cf_eval<<<(unsigned)((nzz + 127) / 128), 128, 0, s>>>(d_a, d_b, d_m, ld, nchain, d_z, nz, tail, d_g, d_e, d_nf);
+  int nf = 0;
+  ASR_CUDA(cudaGetLastError());
+  ASR_CUDA(cudaMemcpyAsync(g, d_g, nzz * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  if (edges) ASR_CUDA(cudaMemcpyAsync(edges, d_e, 2 * nzz * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(&nf, d_nf, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  if (nfall) *nfall = nf;
+  ctx->nfall += nf;
+  cudaFree(d_a); cudaFree(d_b); cudaFree(d_z); cudaFree(d_g); cudaFree(d_m); cudaFree(d_nf);
+  if (d_e) cudaFree(d_e);
+  return ASR_OK;
+}
+
+// ---- contour (src/asr_contour.f90), host
+static const double PI_ = 3.14159265358979323846264338327950288;
+
+int asr_gauss_legendre(int n, double* x, double* w) {   // :132-151
+  if (n < 1 || !x || !w) { set_error("gauss_legendre: bad argument"); return ASR_EINVAL; }
+  for (int i = 1; i <= (n + 1) / 2; ++i) {
+    double z = std::cos(PI_ * (i - 0.25) / (n + 0.5)), z1, p1 = 1, p2 = 0, p3, pp = 1;
+    for (int it = 0; it < 100; ++it) {
+      p1 = 1.0; p2 = 0.0;
+      for (int k = 1; k <= n; ++k) { p3 = p2; p2 = p1; p1 = ((2 * k - 1) * z * p2 - (k - 1) * p3) / k; }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      z1 = z;
+      z = z1 - p1 / pp;
+      if (std::fabs(z - z1) < 1.0e-15) break;
+    }
+    x[i - 1] = -z; x[n - i] = z;
+    w[i - 1] = 2.0 / ((1.0 - z * z) * pp * pp); w[n - i] = w[i - 1];
+  }
+  return ASR_OK;
+}
+
+static void put_node(double* z, double* w, int k, double zr, double zi, double wr, double wi) {
+  z[2 * k] = zr; z[2 * k + 1] = zi; w[2 * k] = wr; w[2 * k + 1] = wi;
+}
+
+int asr_contour_nodes(double ebot, double ef, int n, double eta_end, double* z, double* w) {   // :17-34
+  if (n < 1 || !z || !w || !(ef > ebot)) { set_error("contour_nodes: bad argument"); return ASR_EINVAL; }
+  std::vector<double> x(n), wg(n);
+  asr_gauss_legendre(n, x.data(), wg.data());
+  double c = 0.5 * (ebot + ef), r = 0.5 * (ef - ebot), th0 = 0.0;
+  if (eta_end >= 0.0) th0 = std::asin(std::min(eta_end / r, 0.5));
+  for (int j = 0; j < n; ++j) {
+    double th = th0 + 0.5 * (PI_ - th0) * (1.0 - x[j]);
+    double f = wg[j] * (-0.5 * (PI_ - th0));
+    // w = f * (i r) * exp(i th) = f r (-sin th + i cos th)
+    put_node(z, w, j, c + r * std::cos(th), r * std::sin(th), -f * r * std::sin(th), f * r * std::cos(th));
+  }
+  return ASR_OK;
+}
+
+int asr_contour_nodes_closed(double ebot, double ef, double eta, int na, int nv, double* z, double* w) {   // :39-58
+  if (na < 1 || nv < 1 || !z || !w || !(ef > ebot) || !(eta > 0)) { set_error("contour_nodes_closed: bad argument"); return ASR_EINVAL; }
+  std::vector<double> xa(na), wa(na), xv(nv), wv(nv);
+  asr_gauss_legendre(na, xa.data(), wa.data());
+  asr_gauss_legendre(nv, xv.data(), wv.data());
+  double c = (ef * ef + eta * eta - ebot * ebot) / (2.0 * (ef - ebot)), r = c - ebot, th0 = std::atan2(eta, ef - c);
+  for (int j = 0; j < na; ++j) {
+    double th = th0 + 0.5 * (PI_ - th0) * (1.0 - xa[j]);
+    double f = wa[j] * (-0.5 * (PI_ - th0));
+    put_node(z, w, j, c + r * std::cos(th), r * std::sin(th), -f * r * std::sin(th), f * r * std::cos(th));
+  }
+  for (int j = 0; j < nv; ++j) put_node(z, w, na + j, ef, 0.5 * eta * (1.0 + xv[j]), 0.0, -0.5 * eta * wv[j]);
+  return ASR_OK;
+}
+
+int asr_contour_nodes_fermi(double ebot, double mu, double kt, int npole, int nmain, int nstep, double* z, double* w) {   // :77-121
+  if (!z || !w || kt <= 0.0 || npole < 0 || nmain < 1 || nstep < 1) { set_error("contour_nodes_fermi: bad argument"); return ASR_EINVAL; }
+  auto fermi_r = [&](double e) { double t = (e - mu) / kt; return t > 0.0 ? std::exp(-t) / (1.0 + std::exp(-t)) : 1.0 / (1.0 + std::exp(t)); };
+  double gam = 2.0 * npole * PI_ * kt;
+  std::vector<double> xv(4), wv(4), xm(nmain), wm(nmain), xs(nstep), ws(nstep), xt(8), wt(8);
+  asr_gauss_legendre(4, xv.data(), wv.data()); asr_gauss_legendre(nmain, xm.data(), wm.data());
+  asr_gauss_legendre(nstep, xs.data(), ws.data()); asr_gauss_legendre(8, xt.data(), wt.data());
+  int k = 0;
+  for (int j = 0; j < 4; ++j) {   // vertical leg at E_bot: complex Fermi factor
+    double zr = ebot, zi = 0.5 * gam * (1.0 + xv[j]);
+    double tr = (zr - mu) / kt, ti = zi / kt;
+    double fr = 1.0, fi = 0.0;
+    if (tr >= -600.0) {   // 1 / (exp(t) + 1)
+      double er = std::exp(tr) * std::cos(ti) + 1.0, ei = std::exp(tr) * std::sin(ti), den = er * er + ei * ei;
+      fr = er / den; fi = -ei / den;
+    }
+    double wr = -0.5 * gam * wv[j] * fi, wi = 0.5 * gam * wv[j] * fr;   // (i g) * f
+    put_node(z, w, k++, zr, zi, wr, wi);
+  }
+  double lo = ebot, hi = mu - 10.0 * kt;
+  for (int j = 0; j < nmain; ++j) { double x = 0.5 * (lo + hi) + 0.5 * (hi - lo) * xm[j]; put_node(z, w, k++, x, gam, 0.5 * (hi - lo) * wm[j] * fermi_r(x), 0.0); }
+  lo = mu - 10.0 * kt; hi = mu + 10.0 * kt;
+  for (int j = 0; j < nstep; ++j) { double x = 0.5 * (lo + hi) + 0.5 * (hi - lo) * xs[j]; put_node(z, w, k++, x, gam, 0.5 * (hi - lo) * ws[j] * fermi_r(x), 0.0); }
+  lo = mu + 10.0 * kt; hi = mu + 40.0 * kt;
+  for (int j = 0; j < 8; ++j) { double x = 0.5 * (lo + hi) + 0.5 * (hi - lo) * xt[j]; put_node(z, w, k++, x, gam, 0.5 * (hi - lo) * wt[j] * fermi_r(x), 0.0); }
+  for (int j = 0; j < npole; ++j) put_node(z, w, k++, mu, (2 * j + 1) * PI_ * kt, 0.0, -2.0 * PI_ * kt);
+  return ASR_OK;
+}
+
+int asr_contour_moment(const double* z, const double* w, const double* g, int n, double enu, int k, double* m) {   // :124-130
+  if (!z || !w || !g || !m || n < 0 || k < 0) { set_error("contour_moment: bad argument"); return ASR_EINVAL; }
+  double sr = 0.0, si = 0.0;
+  for (int j = 0; j < n; ++j) {
+    double pr = 1.0, pim = 0.0, xr = z[2 * j] - enu, xi = z[2 * j + 1];
+    for (int q = 0; q < k; ++q) { double t = pr * xr - pim * xi; pim = pr * xi + pim * xr; pr = t; }
+    double ar = w[2 * j] * pr - w[2 * j + 1] * pim, ai = w[2 * j] * pim + w[2 * j + 1] * pr;
+    sr += ar * g[2 * j] - ai * g[2 * j + 1];
+    si += ar * g[2 * j + 1] + ai * g[2 * j];
+  }
+  *m = -si / PI_;
+  return ASR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,210 @@
+// Device continued fractions and terminators: cf_species (src/asr_chain.f90:67-167), sqrt_tail / cf_green
+// (src/reference/asr_greens.f90:12-22, :80-90) and the real Beer-Pettifor asymptote (src/reference/asr_terminator.f90:39-67).
+//
+// LAPACK zgeev (the reference's eigenvalues of the m x m chain matrix) is replaced by the implicit-shift QL iteration for a
+// complex symmetric tridiagonal matrix (eigenvalues only): the EISPACK tql1 / Numerical Recipes tqli scheme carried over
+// to complex symmetric matrices with complex plane rotations (Cullum & Willoughby, Lanczos Algorithms for Large Symmetric
+// Eigenvalue Computations, Vol. 1, ch. 6, CMTQL1).  dsterf (real tridiagonal eigenvalues) is replaced by Sturm-sequence
+// bisection for the extreme eigenvalue.
+#pragma once
+#include <cfloat>
+
+#include "common.cuh"
+
+namespace asrb {
+
+constexpr int CF_NMAX = 128;   // longest chain the device fractions take
+
+// eigenvalues of the complex symmetric tridiagonal (d[0..n-1], e[0..n-2]) in place in d; e is destroyed.  0 = converged.
+__host__ __device__ inline int cs_tridiag_eig(int n, double2* d, double2* e) {
+  if (n <= 0) return 0;
+  e[n - 1] = make_double2(0.0, 0.0);
+  for (int l = 0; l < n; ++l) {
+    int iter = 0;
+    for (;;) {
+      int m;
+      for (m = l; m < n - 1; ++m) {
+        double dd = cabs2(d[m]) + cabs2(d[m + 1]);
+        if (cabs2(e[m]) <= DBL_EPSILON * dd || cabs2(e[m]) == 0.0) break;
+      }
+      if (m == l) break;
+      if (++iter > 60) return 1;
+      double2 g = cdiv(csub(d[l + 1], d[l]), cscale(e[l], 2.0));
+      double2 r = csqrt_p(cadd(cmul(g, g), make_double2(1.0, 0.0)));
+      double2 gp = cadd(g, r), gm = csub(g, r);
+      double2 den = cabs2(gp) >= cabs2(gm) ? gp : gm;
+      g = cadd(csub(d[m], d[l]), cdiv(e[l], den));
+      double2 s = make_double2(1.0, 0.0), c = make_double2(1.0, 0.0), p = make_double2(0.0, 0.0);
+      bool early = false;
+      for (int i = m - 1; i >= l; --i) {
+        double2 f = cmul(s, e[i]), b = cmul(c, e[i]);
+        r = csqrt_p(cadd(cmul(f, f), cmul(g, g)));
+        e[i + 1] = r;
+        if (cabs2(r) == 0.0) {
+          d[i + 1] = csub(d[i + 1], p);
+          e[m] = make_double2(0.0, 0.0);
+          early = true;
+          break;
+        }
+        s = cdiv(f, r);
+        c = cdiv(g, r);
+        g = csub(d[i + 1], p);
+        r = cadd(cmul(csub(d[i], g), s), cscale(cmul(c, b), 2.0));
+        p = cmul(s, r);
+        d[i + 1] = cadd(g, p);
+        g = csub(cmul(c, r), b);
+      }
+      if (early) continue;
+      d[l] = csub(d[l], p);
+      e[l] = g;
+      e[m] = make_double2(0.0, 0.0);
+    }
+  }
+  return 0;
+}
+
+// extreme (by real part) eigenvalues of the chain matrix with a[m-1] replaced by am; returns 0 on success
+__host__ __device__ inline int chain_extremes(const double2* a, const double2* b, int m, double2 am, double2* wd, double2* we,
+                                              double2& lo, double2& hi) {
+  for (int j = 0; j < m; ++j) wd[j] = a[j];
+  wd[m - 1] = am;
+  for (int j = 0; j < m - 1; ++j) we[j] = b[j];
+  if (cs_tridiag_eig(m, wd, we)) return 1;
+  int ilo = 0, ihi = 0;
+  for (int j = 1; j < m; ++j) {
+    if (wd[j].x < wd[ilo].x) ilo = j;
+    if (wd[j].x > wd[ihi].x) ihi = j;
+  }
+  lo = wd[ilo];
+  hi = wd[ihi];
+  return 0;
+}
+
+// cf_species: g11 of the chain (a, b) of depth m at z with the tail (0 none, 1 hull, 2 bp, 3 avg2).  wd, we: work (m).
+__host__ __device__ inline double2 cf_species_dev(const double2* a, const double2* b, int m, double2 z, int tail, double2* wd,
+                                                  double2* we, int* nfall, double2* edges) {
+  double2 aa, bb;
+  bool ok = false;
+  double2 lo, hi;
+  if (m >= 2 && tail != 0) ok = chain_extremes(a, b, m, a[m - 1], wd, we, lo, hi) == 0;
+  if (ok) {
+    aa = cscale(cadd(lo, hi), 0.5);
+    bb = cscale(csub(hi, lo), 0.25);
+    if (tail == 2) {   // bp_fixed_point, src/asr_chain.f90:126-156
+      bool done = false;
+      for (int it = 0; it < 200 && !done; ++it) {
+        double2 l1, h1, l2, h2;
+        if (chain_extremes(a, b, m, cadd(a[m - 1], bb), wd, we, l1, h1)) { if (nfall) ++*nfall; done = true; break; }
+        if (chain_extremes(a, b, m, csub(a[m - 1], bb), wd, we, l2, h2)) { if (nfall) ++*nfall; done = true; break; }
+        double2 an = cscale(cadd(h1, l2), 0.5), bn = cscale(csub(h1, l2), 0.25);
+        if (cabs2(csub(an, aa)) + cabs2(csub(bn, bb)) < 1.0e-12 * (1.0 + cabs2(bn))) { aa = an; bb = bn; done = true; break; }
+        aa = an;
+        bb = bn;
+      }
+      if (!done) {
+        if (nfall) ++*nfall;
+        chain_extremes(a, b, m, a[m - 1], wd, we, lo, hi);
+        aa = cscale(cadd(lo, hi), 0.5);
+        bb = cscale(csub(hi, lo), 0.25);
+      }
+    }
+  } else {
+    aa = a[m - 1];
+    bb = m > 1 ? b[m - 2] : make_double2(0.0, 0.0);
+  }
+  if (tail == 3 && m >= 3) {
+    aa = cscale(cadd(a[m - 1], a[m - 2]), 0.5);
+    bb = csqrt_p(cscale(cadd(cmul(b[m - 2], b[m - 2]), cmul(b[m - 3], b[m - 3])), 0.5));
+  }
+  if (tail == 0) { aa = make_double2(0.0, 0.0); bb = make_double2(0.0, 0.0); }
+  if (edges) { edges[0] = aa; edges[1] = bb; }
+  double2 d = csub(z, aa), tl;
+  if (cabs2(bb) < 1.0e-14) tl = make_double2(0.0, 0.0);
+  else {
+    double2 bb2 = cmul(bb, bb);
+    double2 s = csqrt_p(csub(cmul(d, d), cscale(bb2, 4.0)));
+    double2 g1 = cdiv(csub(d, s), cscale(bb2, 2.0)), g2 = cdiv(cadd(d, s), cscale(bb2, 2.0));
+    tl = cabs2(cmul(bb, g1)) <= cabs2(cmul(bb, g2)) ? cmul(bb2, g1) : cmul(bb2, g2);
+  }
+  double2 one = make_double2(1.0, 0.0);
+  double2 gt = cdiv(one, csub(csub(z, a[m - 1]), tl));
+  for (int j = m - 2; j >= 0; --j) gt = cdiv(one, csub(csub(z, a[j]), cmul(cmul(b[j], b[j]), gt)));
+  return gt;
+}
+
+// ---- real chains (plain mode)
+__host__ __device__ inline int sturm_count(int n, const double* d, const double* e, double x) {
+  int cnt = 0;
+  double q = d[0] - x;
+  if (q < 0) ++cnt;
+  for (int i = 1; i < n; ++i) {
+    if (q == 0.0) q = DBL_EPSILON * (fabs(e[i - 1]) + DBL_MIN);
+    q = d[i] - x - e[i - 1] * e[i - 1] / q;
+    if (q < 0) ++cnt;
+  }
+  return cnt;
+}
+__host__ __device__ inline double tridiag_extreme(int n, const double* d, const double* e, bool upper) {
+  double lo = d[0], hi = d[0];
+  for (int i = 0; i < n; ++i) {
+    double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0);
+    lo = fmin(lo, d[i] - r);
+    hi = fmax(hi, d[i] + r);
+  }
+  double span = hi - lo;
+  lo -= 1e-12 * (span + 1.0);
+  hi += 1e-12 * (span + 1.0);
+  int target = upper ? n : 1;
+  for (int it = 0; it < 200; ++it) {
+    double mid = 0.5 * (lo + hi);
+    if (mid <= lo || mid >= hi) break;
+    if (sturm_count(n, d, e, mid) >= target) hi = mid; else lo = mid;
+  }
+  return 0.5 * (lo + hi);
+}
+// bp_asymptote (src/reference/asr_terminator.f90:39-67); wd: work (n)
+__host__ __device__ inline void bp_asymptote_dev(const double* a, const double* b, int n, double* wd, double& ainf, double& binf) {
+  double A = 0.5 * (a[n - 1] + a[n - 2]);
+  double B = sqrt(0.5 * (b[n - 1] * b[n - 1] + b[n - 2] * b[n - 2]));
+  for (int it = 0; it < 500; ++it) {
+    for (int i = 0; i < n; ++i) wd[i] = a[i];
+    wd[n - 1] = a[n - 1] + B;
+    double ep = tridiag_extreme(n, wd, b, true);
+    wd[n - 1] = a[n - 1] - B;
+    double em = tridiag_extreme(n, wd, b, false);
+    double an = 0.5 * (ep + em), bn = 0.25 * (ep - em);
+    bool conv = fabs(an - A) + fabs(bn - B) < 1.0e-13;
+    A = an;
+    B = bn;
+    if (conv) break;
+  }
+  ainf = A;
+  binf = B;
+}
+// sqrt_tail + cf_green (src/reference/asr_greens.f90:12-22, :80-90)
+__host__ __device__ inline double2 terminated_green_dev(const double* a, const double* b, int n, double2 z, double ainf, double binf,
+                                                        bool has_tail) {
+  double2 tl = make_double2(0.0, 0.0);
+  if (has_tail) {
+    double2 w = make_double2(z.x - ainf, z.y);
+    double2 s = csqrt_p(csub(cmul(w, w), make_double2(4.0 * binf * binf, 0.0)));
+    double d2 = 2.0 * binf * binf;
+    double2 g1 = cscale(csub(w, s), 1.0 / d2), g2 = cscale(cadd(w, s), 1.0 / d2);
+    double2 g = cabs2(g1) <= cabs2(g2) ? g1 : g2;
+    tl = cscale(g, binf * binf);
+  }
+  double2 one = make_double2(1.0, 0.0);
+  double2 g = cdiv(one, csub(make_double2(z.x - a[n - 1], z.y), tl));
+  for (int i = n - 2; i >= 0; --i) g = cdiv(one, csub(make_double2(z.x - a[i], z.y), cscale(g, b[i] * b[i])));
+  return g;
+}
+
+// kernels of cf.cu
+__global__ void k_cf_eval(const double2* a, const double2* b, const int* m, int ld, int nchain, const double2* z, int nz, int tail,
+                          double2* g, double2* edges, int* nfall);
+__global__ void k_real_tail(const double* a, const double* b, const int* n, int ld, int nchain, int method, double* ainf,
+                            double* binf);
+__global__ void k_real_green(const double* a, const double* b, const int* n, int ld, int nchain, const double* ainf,
+                             const double* binf, int method, const double2* z, int nz, double2* g);
+
+}  // namespace asrb

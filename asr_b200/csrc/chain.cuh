@@ -1,0 +1,77 @@
+// Batched Lanczos chains on the site-class operator: device data layout and the host driver interface.
+#pragma once
+#include "op.h"
+
+namespace asrb {
+
+constexpr int TL = 32;       // lanes (chains) per tile: one warp covers one node of a tile
+constexpr int NLMAX = 128;   // longest chain held on the device
+constexpr int MAXOP = 64;    // chi masks are 64-bit
+
+// Parameter blob of one group (doubles): for p in {c, d, o, e, pa, pb, c+e+pb, e+pb}: local weights
+// W_p[kap][k_own][k_flip][l] (nw = ncls * nsm * nsm * 9 each), then the raw parameters par_p[s][l] (np = 9 * nsp each).
+// The last two are the combined diagonal terms of the final step, C + E + X(z) and E + X(z), with X(z) = z pa + pb.
+enum { PC = 0, PD = 1, PO = 2, PE = 3, PA = 4, PB = 5, PCEB = 6, PEB = 7, NPAR = 8 };
+struct GroupLayout {
+  int nw, np, stride;
+  __host__ __device__ int w(int p) const { return p * nw; }
+  __host__ __device__ int raw(int p) const { return NPAR * nw + p * np; }
+};
+
+// group flags
+enum { GF_D_UNIFORM = 1, GF_O_ZERO = 2, GF_E_ZERO = 4, GF_X_ZERO = 8 };
+
+struct GroupInfo {
+  int flags;
+  int frozen_sp;          // species frozen on the start site (0: none)
+  int l0;                 // start orbital 1..9
+  int nlev;
+  unsigned long long chimask;   // bit g set: chi(g) = -1
+  double dd[9];           // uniform d per orbital (GF_D_UNIFORM)
+};
+
+// One batch: ntile tiles x TL lanes.  Lane L = tile * TL + j.
+struct BatchView {
+  int ntile, nn, nsm, kstep, mode, project, tail, nlevmax;
+  double depth_tol;
+  const double* gblob;
+  GroupLayout GL;
+  const GroupInfo* ginfo;
+  const int* lane_group;   // -1: idle lane
+  const double2* lane_z;
+  int* lane_act;           // 1 active
+  int* lane_wact;          // 1: the lane computes w / b this step
+  int* lane_m;
+  double2* acoef;          // [lane][NLMAX]
+  double2* bcoef;
+  double2* gprev;
+  double2* acur;           // a_k of this step
+  double2* bprev;          // b_{k-1}
+  double2* su;             // scale of the current vector
+  double2* sup;            // scale of the previous vector
+  int* tile_act;           // tile has an active lane
+  int* nfall;
+};
+
+struct RunOptions {
+  int mode = ASR_MODE_EDC;
+  double depth_tol = 0.0;
+  int tail = ASR_TAIL_HULL;
+  int precision = ASR_FP64;
+  int project = 1;
+  int tiles_per_batch = 0;   // 0: automatic
+  int nodes_per_warp = 4;
+};
+
+// Runs chains for lanes (group, z) on the operator; results per lane: g (energy of the lane), a, b (NLMAX each), m.
+int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+              const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
+              const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
+              std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out);
+
+// y = H x style applications of the operator's own parameters on nvec vectors (normalised coordinates)
+int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+                  const GroupLayout& GL, int nvec, const double* x_host, bool complex_in, double* y_host, int what);
+enum { APPLY_H = 0, APPLY_RAND_Z = 1, APPLY_PROJECT = 2 };
+
+}  // namespace asrb

@@ -1,0 +1,92 @@
+// Internal types of the asr_b200 library: context, operator (device node tables) and the kernel-side views.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+
+struct asr_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // the stream every call runs on
+  cudaStream_t own_stream = nullptr;  // created by asr_ctx_create
+  int num_sms = 148;
+  int64_t nchain = 0, nlev = 0, nfall = 0;
+  int* d_err = nullptr;   // device error word
+  // kernel timing (asr_ctx_profile)
+  int profile = 0;
+  double prof_ms = 0.0, prof_bytes = 0.0, prof_flops = 0.0;
+  int64_t prof_launches = 0;
+  std::vector<cudaEvent_t> ev_pool;
+};
+
+namespace asrb {
+
+// Device view of the node tables, passed by value to the kernels.  Node indices are 0-based, -1 = absent link;
+// operation indices 0-based.  Layouts follow the reference: flipr/flipg (nsmax, nn) and hopr/hopg (nslot, nn) with the
+// state / slot index fastest, i.e. hopr[k + nslot * i].
+struct OpView {
+  int nn, nslot, nsmax, nop, ncls, nsp, ntype;
+  const int* site;        // (nn) 1-based graph site
+  const int8_t* lst;      // (nn) own local state
+  const int8_t* ncl;      // (nn) 0-based class
+  const int8_t* typ;      // (nn) 0-based site type (stype of the site)
+  const int8_t* start;    // (nn) 1 if the node sits on the start site
+  const int8_t* frozen;   // (nn) operator-level frozen species (0: none)
+  const double* sq;       // (nn) sqrt(orbit size)
+  const double* isq;      // (nn) 1 / sqrt(orbit size)
+  const int* flipr;       // (nsmax, nn)
+  const uint8_t* flipg;
+  const int* hopr;        // (nslot, nn)
+  const uint8_t* hopg;
+  const int* stab_ptr;    // (nn + 1) 0-based offsets
+  const uint8_t* stab;    // (nstab)
+  const int8_t* nsc;      // (ncls) species per class
+  const uint8_t* pi;      // (9, nop) 0-based orbital permutation: D(g)[pi(l), l] = sg(l)
+  const uint16_t* sgm;    // (nop) bit l set: sg(l, g) = -1
+};
+
+}  // namespace asrb
+
+struct asr_op {
+  asr_ctx* ctx = nullptr;
+  int nn = 0, nslot = 0, nsmax = 0, nop = 0, ncls = 0, nsp = 0, ntype = 1, nsite = 0, nstab = 0, start_site = 1;
+  int start_l = 1;
+  // host copies of the model and group
+  std::vector<int> nsc, spc;       // spc(ldspc, ncls)
+  int ldspc = 1;
+  std::vector<double> mt;          // (nsm, nsm, nsm, ncls)
+  std::vector<int> pi;             // (9, nop) 1-based
+  std::vector<double> sg, chi, dmat;
+  std::vector<double> block;       // (9, 9, nslot, ntype) unrotated bond blocks
+  std::vector<double> block0;      // (9, 9, ntype)
+  std::vector<double> c, d, o, e;  // (9, nsp) current operator parameters
+  std::vector<int8_t> frozen_h;    // (nn) operator-level frozen species
+  // device tables
+  int* d_site = nullptr;
+  int* d_level = nullptr;
+  int* d_orb = nullptr;
+  int8_t *d_lst = nullptr, *d_ncl = nullptr, *d_typ = nullptr, *d_start = nullptr, *d_frozen = nullptr;
+  double *d_sq = nullptr, *d_isq = nullptr;
+  int *d_flipr = nullptr, *d_hopr = nullptr, *d_stab_ptr = nullptr;
+  uint8_t *d_flipg = nullptr, *d_hopg = nullptr, *d_stab = nullptr;
+  int8_t* d_nsc = nullptr;
+  uint8_t* d_pi = nullptr;
+  uint16_t* d_sgm = nullptr;
+  double* d_blocks = nullptr;   // [t][kk][l][l'] kk = 0: on-site block, kk = 1 + slot
+  float* d_blocks_f = nullptr;
+  asrb::OpView view() const {
+    return asrb::OpView{nn, nslot, nsmax, nop, ncls, nsp, ntype, d_site, d_lst, d_ncl, d_typ, d_start, d_frozen,
+                        d_sq, d_isq, d_flipr, d_flipg, d_hopr, d_hopg, d_stab_ptr, d_stab, d_nsc, d_pi, d_sgm};
+  }
+};
+
+namespace asrb {
+// graph_build.cu
+int build_operator(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* cls,
+                   const int* perm, int nop, int start, int maxlevel, int maxrank, const int* flippable, const int* stype,
+                   asr_op* op);
+// host helpers (capi.cu)
+void class_mt(const double* conc, int nsc, int nsm, double* mt);
+}  // namespace asrb

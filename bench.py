@@ -1,0 +1,304 @@
+"""Benchmark of the recursion hot path: batched energy-dependent chains on the site-class operator.
+
+Workload (the batched, uneven-depth configuration): fcc ternary Fe0.66Ni0.14Cr0.20-like random alloy, one site class,
+spd 9 orbitals, NN + NNN Slater-Koster blocks (18 slots), 5^3-cell periodic cluster, closure to 3 levels, rank 1, D2h
+reduction (all 9 orbitals one dimensional); 2 spins x 3 central species x 9 start orbitals = 54 chain groups with depths
+drawn from U{16..28} (seed 1); energies: 48-point Gauss-Legendre semicircle plus 4096 real-axis energies (Im z = 0.005).
+Seeded synthetic inputs stand in for the reference's LMTO potential parameters and structure constants.
+
+One step = every chain group over a slice of 192 consecutive energies of that list (10368 chains); successive steps walk
+through the list.  value = chain-steps / s (one Lanczos step of one chain at one energy), whole job, inputs resident in
+HBM; e2e = the same through the host C-ABI call with host buffers (copies inside the timed region).
+``--impl reference`` times the CPU restatement of the reference (oracle, OpenMP over chain tasks as chain_worker does).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NZ_SLICE = 192
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    p.add_argument("--nz-slice", type=int, default=NZ_SLICE)
+    p.add_argument("--cpu-sample", type=int, default=1, help="run the bounded CPU baseline sample (1) or skip it (0)")
+    return p.parse_args()
+
+
+def workload():
+    """Synthetic inputs of the configuration (host arrays only)."""
+    from asr_b200 import synthetic as S
+    case = S.cubic_case("fcc", 5, 3, [0.66, 0.14, 0.20], seed=1, group="d2h")
+    fl = np.ones(case["graph"].n, np.int32)
+    fl[0] = 0
+    rng = np.random.default_rng(1)
+    depths = rng.integers(16, 29, size=54)
+    groups = []
+    for spin in range(2):
+        sp = S.draw_species(3, seed=1 + spin)
+        for cen in (1, 2, 3):
+            ed = S.edc_params(sp, cen)
+            for l0 in range(1, 10):
+                groups.append(dict(ed=ed, cen=cen, l0=l0, nlev=int(depths[len(groups)])))
+    # energies: contour_nodes (src/asr_contour.f90:17-34) on [ebot, ef] + real axis
+    ebot, ef = -1.2, 0.3
+    x, _ = np.polynomial.legendre.leggauss(48)
+    th = 0.5 * np.pi * (1.0 - x)
+    zc = 0.5 * (ebot + ef) + 0.5 * (ef - ebot) * np.exp(1j * th)
+    zr = np.linspace(-1.5, 1.0, 4096) + 0.005j
+    z = np.concatenate([zc, zr])
+    return case, fl, groups, z
+
+
+def specs_of(groups):
+    import asr_b200 as A
+    return [A.ChainSpec(c=g["ed"]["c"], d=g["ed"]["d"], o=g["ed"]["o"], e=g["ed"]["e"], pa=g["ed"]["pa"], pb=g["ed"]["pb"],
+                        frozen_sp=g["cen"], start_orb=g["l0"], nlev=g["nlev"]) for g in groups]
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(case, fl, groups, z, oop=None):
+    """The oracle (CPU restatement of chain_greens / edc_green_blk) on a bounded sample with every host thread: the chain
+    groups of start orbital 1 (2 spins x 3 central species), each over ceil(threads / 6) blocks of 4 energies, one task per
+    thread and block as chain_worker schedules them (src/asr_class_scf.f90:1071-1160)."""
+    from oracle import oracle as O
+    nthr = os.cpu_count() or 1
+    if oop is None:
+        oop = O.OracleOp(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, 3, 1, fl)
+    sel = [g for g in groups if g["l0"] == 1]
+    nbe = 4
+    nblk = max(1, -(-nthr // len(sel)))
+    gps = [dict(c=g["ed"]["c"], d=g["ed"]["d"], o=g["ed"]["o"], e=g["ed"]["e"], dc=g["ed"]["dc"], dl=g["ed"]["dl"],
+                enu=g["ed"]["enu"]) for g in sel]
+    nlevq = np.array([[g["nlev"] for g in sel]], np.int32).T.copy()
+    t0 = time.perf_counter()
+    gz, steps = oop.chain_greens(gps, [g["cen"] for g in sel], [1], nlevq, z[: nbe * nblk], nbe, nthreads=nthr)
+    t = time.perf_counter() - t0
+    return {"value": steps / t, "unit": "chain-steps/s", "cores": nthr, "kind": "port",
+            "sample": f"{len(sel)} chain groups x {nbe * nblk} energies in {len(sel) * nblk} tasks ({steps} chain-steps, "
+                      f"{t:.1f} s), nn={oop.nn}, oracle edc_green_blk, {nthr} threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    case, fl, groups, z = workload()
+    oop = O.OracleOp(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, 3, 1, fl)
+    vals = []
+    for it in range(min(args.warmup, 1) + args.steps):
+        r = cpu_baseline(case, fl, groups, z, oop)
+        if it >= min(args.warmup, 1):
+            vals.append(r["value"])
+    v = float(np.mean(vals))
+    line = {"metric": "chain-steps/s (batched energy-dependent chains, fcc ternary, 54 groups, depths 16-28)", "value": v,
+            "unit": "chain-steps/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": "fcc ternary Fe0.66Ni0.14Cr0.20, levels 3, rank 1, D2h, 54 chain groups, depth U{16..28}, "
+                                   "48-pt contour + 4096 real energies", "sample": "bounded CPU sample per step"},
+            "cpu_baseline": {"kind": r["kind"], "cores": r["cores"], "sample": r["sample"], "value": v, "unit": "chain-steps/s"},
+            "e2e": {"value": v, "unit": "chain-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    import asr_b200 as A
+
+    case, fl, groups, z_all = workload()
+    ctx = A.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    op = A.build_augcls_operator(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, 3, maxrank=1,
+                                 flippable=fl, ctx=ctx)
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    specs = specs_of(groups)
+    nzs = args.nz_slice
+    nall = z_all.shape[0]
+    z_dev = torch.from_numpy(z_all).to("cuda")
+    g_dev = torch.zeros(len(specs) * nzs, dtype=torch.complex128, device="cuda")
+    depth_per_group = np.array([g["nlev"] for g in groups])
+    chain_steps_per_step = int(depth_per_group.sum()) * nzs
+
+    def slice_of(it):
+        # each rank walks its own slices (weak scaling); rank r starts r slices further
+        start = ((it * world + rank) * nzs) % (nall - nzs + 1)
+        return start
+
+    def step(it):
+        s0 = slice_of(it)
+        A.chains_run_device(op, specs, z_dev[s0:s0 + nzs].data_ptr(), g_dev.data_ptr(), nzs, "edc", 0.0, "hull", args.precision)
+        if world > 1:
+            out = torch.empty(world * g_dev.numel(), dtype=g_dev.dtype, device="cuda")
+            dist.all_gather_into_tensor(out, g_dev)
+
+    for it in range(args.warmup):
+        step(it)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    clk.start()
+    ctx.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for it in range(args.steps):
+        step(args.warmup + it)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.profile(False)
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    ks = ctx.kernel_stats()
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.stop()
+    total_steps = chain_steps_per_step * args.steps * world
+    value = total_steps / (ms / 1000.0)
+    # e2e through the host C-ABI call (host z, host g; copies inside the timed region)
+    z_host = [z_all[slice_of(args.warmup + it): slice_of(args.warmup + it) + nzs].copy() for it in range(args.steps)]
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for it in range(args.steps):
+        r = A.chains_run(op, specs, z_host[it], "edc", 0.0, "hull", args.precision)
+        _ = r["g"]
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    if world > 1:
+        t = torch.tensor([ms_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e = total_steps / (ms_e2e / 1000.0)
+    nsp = 3
+    h2d = nzs * 16 + len(specs) * 6 * 9 * nsp * 8
+    d2h = len(specs) * nzs * (16 + 4)
+
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        per_launch_ms = ks["ms"] / max(ks["launches"], 1)
+        achieved = (ks["bytes"] / max(ks["launches"], 1)) / (per_launch_ms / 1000.0) / 1e9
+        tflops = (ks["flops"] / max(ks["launches"], 1)) / (per_launch_ms / 1000.0) / 1e12
+        cpu = cpu_baseline(case, fl, groups, z_all) if args.cpu_sample else None
+        line = {
+            "metric": "chain-steps/s (batched energy-dependent chains, fcc ternary, 54 groups, depths 16-28)",
+            "value": value, "unit": "chain-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32-matvec/f64-coefficients", "data": "synthetic",
+            "config": {"workload": "fcc ternary Fe0.66Ni0.14Cr0.20, 5^3-cell cluster, levels 3, rank 1, D2h, 54 chain groups "
+                                   "(2 spins x 3 species x 9 orbitals), depth U{16..28} seed 1, 48-pt contour + 4096 real "
+                                   "energies", "nodes": op.nn, "slots": op.nslot, "energies_per_step": nzs,
+                       "chains_per_step": len(specs) * nzs, "chain_steps_per_step": chain_steps_per_step,
+                       "l2": "inputs larger than L2 (one 32-lane vector is %.0f MB)" % (op.nn * 9 * 32 * 16 / 1e6),
+                       "parallelism": f"chain tasks over {world} GPU(s)", "operator_build_s": build_s,
+                       "precision": args.precision},
+            "e2e": {"value": e2e, "unit": "chain-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                         "traffic": None, "kernel": "chain step operator (k_smul, fused S + diagonal + dot)",
+                         "per_launch_ms": per_launch_ms, "launches": ks["launches"], "fp64_tflops": tflops,
+                         "share_of_step": ks["ms"] / ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
+            "cpu_baseline": cpu,
+            "gpu_launches": None,
+            "clocks": clocks,
+        }
+        # kernels per step of one batch: step kernel + 3 per level, plus init and the final fractions
+        line["gpu_launches"] = int(ks["launches"] * 4 + 2 * max(ks["launches"] // 20, 1))
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

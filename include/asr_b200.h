@@ -1,0 +1,146 @@
+/* asr_b200.h -- C ABI of the B200 (sm_100a) augmented-space recursion library.
+ *
+ * A drop-in for the recursion hot path of mavensgroup/asr behind its site-class operator interface.  Every entry point
+ * names the reference interface it replaces (paths relative to the asr project root).  Conventions:
+ *   - every call returns an int status (ASR_OK = 0); asr_last_error() gives the message of the calling host thread;
+ *   - arrays cross the ABI in Fortran (column-major) layout with the reference's shapes, so a Fortran caller passes its
+ *     arrays through iso_c_binding unchanged; stored site / node / operation indices are 1-based as in the reference;
+ *   - complex arrays are interleaved (re, im) doubles (Fortran complex(dp));
+ *   - pointers are host pointers unless the name ends in _dev;
+ *   - the caller owns every host buffer; device buffers belong to the context or the operator.
+ * Errors are status codes, never aborts (the reference uses `error stop`).
+ */
+#ifndef ASR_B200_H
+#define ASR_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ASR_OK 0
+#define ASR_EINVAL 1    /* invalid argument (the reference's `error stop` on bad input) */
+#define ASR_ENOMEM 2    /* device allocation failed */
+#define ASR_ECUDA 3     /* CUDA runtime error */
+#define ASR_ETIMEOUT 4  /* a bounded device wait gave up */
+#define ASR_EEDGE 5     /* the closure reached the edge of the site cluster (src/asr_augcls.f90:672,676) */
+#define ASR_ESTATE 6    /* an internal invariant failed (stabiliser size, hash table capacity) */
+
+#define ASR_MODE_PLAIN 0 /* real Lanczos on H (src/reference/asr_recursion.f90:17-58): one chain per group */
+#define ASR_MODE_EDC 1   /* complex-symmetric Lanczos on z - H(z) per energy (src/asr_edc.f90:75-164, :237-316) */
+
+#define ASR_TAIL_NONE 0  /* cf_species tails, src/asr_chain.f90:18-23 */
+#define ASR_TAIL_HULL 1
+#define ASR_TAIL_BP 2
+#define ASR_TAIL_AVG2 3
+
+#define ASR_FP64 0       /* FP64 vectors and matvec */
+#define ASR_FP32 1       /* FP32 vector storage and matvec, FP64 coefficients, reductions and fractions */
+
+typedef struct asr_ctx asr_ctx;
+typedef struct asr_op asr_op;
+
+/* ---- library and context ---------------------------------------------------------------------------------------- */
+int asr_version(void);
+/* message of the last failed call on this host thread (src/asr_mpi.F90:191-197 par_fail replaced by status codes) */
+int asr_last_error(char* buf, size_t n);
+/* device context: stream, workspace.  One per host thread and device. */
+int asr_ctx_create(int device, asr_ctx** ctx);
+int asr_ctx_destroy(asr_ctx* ctx);
+int asr_ctx_sync(asr_ctx* ctx);
+/* chain statistics of the context (ed_nchain, ed_nlev, ed_nfall of src/asr_chain.f90:14-17) */
+int asr_ctx_stats(const asr_ctx* ctx, int64_t* nchain, int64_t* nlev, int64_t* nfall);
+/* run on the caller's CUDA stream (a cudaStream_t, e.g. the current stream of a PyTorch process); NULL: the context's own.
+ * No counterpart in the reference (which has no device). */
+int asr_ctx_set_stream(asr_ctx* ctx, void* stream);
+/* per-launch CUDA-event timing of the chain step kernel (the timer buckets of src/asr_runstats.f90:1-96 on the device):
+ * on = 1 starts (and clears) it; asr_ctx_kernel_stats returns the summed device time, the launches and the algorithmic
+ * bytes and flops of those launches */
+int asr_ctx_profile(asr_ctx* ctx, int on);
+int asr_ctx_kernel_stats(const asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops);
+
+/* ---- operator: replaces augcls_op and build_augcls_operator (src/asr_augcls.f90:45-68, :596-823) ---------------- *
+ * graph (graph_t, src/asr_augspace.f90:22-25): nbr_ptr(nsite+1), nbr(*) 1-based (0: no bond on the slot, -1: beyond the
+ * cluster).  Model (class_alloy_t, :36-43): nsc(ncls), spc(ldspc, ncls), conc(ldspc, ncls), nsp species,
+ * block(9, 9, nblock_slots, ntype_blocks), block0(9, 9, ntype_blocks) (NULL: zero).  cls(nsite), perm(nsite, nop),
+ * dmat(9, 9, nop), start site, maxlevel, maxrank (0: unlimited), flippable(nsite) (NULL: all), stype(nsite) (NULL: 1).
+ * The closure and every node table are built on the device; the node numbering equals the reference's serial order. */
+int asr_op_build(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc,
+                 int ldspc, const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat,
+                 int start, int maxlevel, int maxrank, const int* flippable, const int* stype, const double* block,
+                 int nblock_slots, int ntype_blocks, const double* block0, asr_op** op);
+/* augcls_free (src/asr_augcls.f90:569-585) */
+int asr_op_free(asr_op* op);
+/* dims: nn, nslot, nsmax, nop, ncls, ntype, nstab, nsp */
+int asr_op_dims(const asr_op* op, int* dims);
+/* host copies of the node tables in the reference layout: flipr/flipg(nsmax, nn), hopr/hopg(nslot, nn), lst, site,
+ * ncl, level (nn), norb, sq (nn), stab_ptr(nn+1), stab(nstab).  Any pointer may be NULL. */
+int asr_op_export_tables(const asr_op* op, int* flipr, int* flipg, int* hopr, int* hopg, int* lst, int* site, int* ncl,
+                         int* level, double* norb, double* sq, int* stab_ptr, int* stab);
+
+/* ---- per-operator state: augcls_set_params :121, augcls_freeze_site/_any :129/:147, augcls_set_start :107,
+ *      augcls_set_chi :165, augcls_set_class_conc :178 --------------------------------------------------------------- */
+int asr_op_set_params(asr_op* op, const double* c, const double* d, const double* o, const double* e);
+int asr_op_freeze_site(asr_op* op, int site, int sp);
+int asr_op_unfreeze(asr_op* op);
+int asr_op_set_start(asr_op* op, int l0);
+int asr_op_set_chi(asr_op* op, const double* chi);
+int asr_op_set_class_conc(asr_op* op, int kap, const double* conc);
+
+/* ---- application: the linop interface (src/asr_operator.f90:10-28) -------------------------------------------------- */
+/* augcls_apply (src/asr_augcls.f90:275-297): y = H x for nvec real vectors x(9 nn, nvec), normalised coordinates */
+int asr_op_apply(asr_op* op, const double* x, double* y, int nvec);
+/* augcls_rand_c (:419-446): w = X x, complex parameters par(9, nsp), complex x(9 nn, nvec) */
+int asr_op_rand_c(asr_op* op, const double* par, const double* x, double* w, int nvec);
+/* augcls_project_c (:329-348), in place on complex x(9 nn, nvec) */
+int asr_op_project_c(asr_op* op, double* x, int nvec);
+
+/* ---- batched chains: chain_greens / edc_green_blk / lanczos (src/asr_class_scf.f90:966-1160, src/asr_edc.f90:237-316,
+ *      src/reference/asr_recursion.f90:17-58) ------------------------------------------------------------------------ */
+typedef struct {
+  const double* c;   /* (9, nsp) operator parameters of the chain: H = E_nu + h - h o h, h = c + d S d, E_nu = e */
+  const double* d;
+  const double* o;
+  const double* e;
+  const double* pa;  /* (9, nsp) energy-dependent diagonal X(z) = z pa + pb (edc mode), NULL: zero */
+  const double* pb;
+  int frozen_sp;     /* species frozen on the start site (0: none), augcls_freeze_site(op, start, sp) */
+  int start_orb;     /* start orbital l0 (1..9): start vector e_(node 1, l0), chi(g) = dmat(l0, l0, g) */
+  int nlev;          /* chain depth (recursion steps) */
+  int reserved;
+} asr_chain_group;
+
+/* Runs every chain of the batch: in ASR_MODE_EDC one chain per (group, energy), in ASR_MODE_PLAIN one real chain per
+ * group whose terminated fraction is evaluated at every energy.  z(nz) complex energies; outputs g(nz, ngroup) complex;
+ * optional a, b (nlevmax, nz, ngroup) complex (plain mode: (nlevmax, 1, ngroup)), mused (nz, ngroup).
+ * depth_tol > 0: adaptive depth (src/asr_edc.f90:121-127).  tail: ASR_TAIL_*; in plain mode ASR_TAIL_BP is the real
+ * Beer-Pettifor asymptote (src/reference/asr_terminator.f90:39-67) and ASR_TAIL_AVG2 'sqrt-avg2'.  project: project each
+ * new Lanczos vector on the symmetric subspace (src/asr_chain.f90:24-26). */
+int asr_chains_run(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz, int mode,
+                   double depth_tol, int tail, int precision, int project, double* g, double* a, double* b, int* mused);
+/* Same, with z and g already in device memory (double2 arrays); a, b, mused host pointers or NULL. */
+int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const void* z_dev, int nz,
+                       int mode, double depth_tol, int tail, int precision, int project, void* g_dev, double* a, double* b,
+                       int* mused);
+
+/* cf_species (src/asr_chain.f90:67-167) for nchain complex chains a, b (ld, nchain), depth m(nchain), at the energies
+ * z(nz, nchain): g(nz, nchain).  edges (optional, (2, nz, nchain)) returns the tail (centre, quarter width). */
+int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain, const double* z, int nz,
+                int tail, double* g, double* edges, int64_t* nfall);
+
+/* ---- contour (src/asr_contour.f90), host ------------------------------------------------------------------------- */
+int asr_gauss_legendre(int n, double* x, double* w);
+/* contour_nodes :17-34 (eta_end < 0: to the real axis) */
+int asr_contour_nodes(double ebot, double ef, int n, double eta_end, double* z, double* w);
+/* contour_nodes_closed :39-58 */
+int asr_contour_nodes_closed(double ebot, double ef, double eta, int n_arc, int n_vert, double* z, double* w);
+/* contour_nodes_fermi :77-121 (z, w of length 4 + n_main + n_step + 8 + npole) */
+int asr_contour_nodes_fermi(double ebot, double mu, double kt, int npole, int n_main, int n_step, double* z, double* w);
+/* contour_moment :124-130 */
+int asr_contour_moment(const double* z, const double* w, const double* g, int n, double enu, int k, double* m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
