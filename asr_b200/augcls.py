@@ -70,6 +70,12 @@ class Context:
         check(lib().asr_ctx_kernel_stats(self.h, C.byref(ms), C.byref(n), C.byref(by), C.byref(fl)))
         return dict(ms=ms.value, launches=n.value, bytes=by.value, flops=fl.value)
 
+    def launches(self) -> int:
+        """Kernels launched by this context so far."""
+        n = C.c_int64()
+        check(lib().asr_ctx_launches(self.h, C.byref(n)))
+        return n.value
+
     def stats(self):
         """(ed_nchain, ed_nlev, ed_nfall) counters of src/asr_chain.f90:14-17."""
         a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
@@ -173,7 +179,7 @@ class AugclsOp:
         one = x.ndim == 1
         X = x.reshape(self.dim, -1, order="F")
         W = np.zeros_like(X, order="F")
-        check(lib().asr_op_rand_c(self.h, _pd(par.view(np.float64)), _pd(X.view(np.float64)), _pd(W.view(np.float64)),
+        check(lib().asr_op_rand_c(self.h, _pd(par), _pd(X), _pd(W),
                                   X.shape[1]))
         return W[:, 0] if one else W
 
@@ -181,7 +187,7 @@ class AugclsOp:
         """``augcls_project_c`` (returns the projected copy)."""
         X = _f64(x, True).reshape(self.dim, -1, order="F").copy(order="F")
         one = np.ndim(x) == 1
-        check(lib().asr_op_project_c(self.h, _pd(X.view(np.float64)), X.shape[1]))
+        check(lib().asr_op_project_c(self.h, _pd(X), X.shape[1]))
         return X[:, 0] if one else X
 
 

@@ -70,10 +70,10 @@ def chains_run(op: AugclsOp, specs, z, mode: str = "edc", depth_tol: float = 0.0
     nab = 1 if mode == "plain" else nz
     a = np.zeros((ng, nab, nlevmax), np.complex128) if coefs else None
     b = np.zeros((ng, nab, nlevmax), np.complex128) if coefs else None
-    check(lib().asr_chains_run(op.ctx.h, op.h, arr, ng, _pd(z.view(np.float64)), nz,
+    check(lib().asr_chains_run(op.ctx.h, op.h, arr, ng, _pd(z), nz,
                                _lib.MODE_PLAIN if mode == "plain" else _lib.MODE_EDC, float(depth_tol), _lib.TAILS[tail],
-                               PREC[precision], int(bool(project)), _pd(g.view(np.float64)),
-                               _pd(a.view(np.float64)) if coefs else None, _pd(b.view(np.float64)) if coefs else None, _pi(m)))
+                               PREC[precision], int(bool(project)), _pd(g),
+                               _pd(a) if coefs else None, _pd(b) if coefs else None, _pi(m)))
     out = dict(g=g.T, m=m.T)
     if coefs:
         out["a"] = a.transpose(2, 1, 0)
@@ -137,6 +137,6 @@ def cf_species(a, b, m, z, tail: str = "hull", ctx: Context | None = None, edges
     g = np.zeros((nz, nc), np.complex128, order="F")
     e = np.zeros((2, nz, nc), np.complex128, order="F") if edges else None
     nf = C.c_int64(0)
-    check(lib().asr_cf_eval(ctx.h, _pd(a.view(np.float64)), _pd(b.view(np.float64)), _pi(m), ld, nc, _pd(z.view(np.float64)), nz,
-                            _lib.TAILS[tail], _pd(g.view(np.float64)), _pd(e.view(np.float64)) if edges else None, C.byref(nf)))
+    check(lib().asr_cf_eval(ctx.h, _pd(a), _pd(b), _pi(m), ld, nc, _pd(z), nz,
+                            _lib.TAILS[tail], _pd(g), _pd(e) if edges else None, C.byref(nf)))
     return (g, e, nf.value) if edges else g

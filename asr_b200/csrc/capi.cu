@@ -247,15 +247,35 @@ int asr_ctx_set_stream(asr_ctx* ctx, void* stream) {
   return ASR_OK;
 }
 
+static int drain_events(asr_ctx* ctx) {
+  if (ctx->ev_used == 0) return ASR_OK;
+  ASR_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int q = 0; q < ctx->ev_used; ++q) {
+    float ms = 0.f;
+    ASR_CUDA(cudaEventElapsedTime(&ms, ctx->ev_pool[2 * q], ctx->ev_pool[2 * q + 1]));
+    ctx->prof_ms += ms;
+  }
+  ctx->ev_used = 0;
+  return ASR_OK;
+}
+
 int asr_ctx_profile(asr_ctx* ctx, int on) {
   if (!ctx) { set_error("asr_ctx_profile: null context"); return ASR_EINVAL; }
+  ASR_TRY(drain_events(ctx));
   ctx->profile = on;
   if (on) { ctx->prof_ms = 0.0; ctx->prof_bytes = 0.0; ctx->prof_flops = 0.0; ctx->prof_launches = 0; }
   return ASR_OK;
 }
 
-int asr_ctx_kernel_stats(const asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops) {
+int asr_ctx_launches(asr_ctx* ctx, int64_t* launches) {
+  if (!ctx || !launches) { set_error("asr_ctx_launches: null argument"); return ASR_EINVAL; }
+  *launches = ctx->launches;
+  return ASR_OK;
+}
+
+int asr_ctx_kernel_stats(asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops) {
   if (!ctx) { set_error("asr_ctx_kernel_stats: null context"); return ASR_EINVAL; }
+  ASR_TRY(drain_events(ctx));
   if (ms) *ms = ctx->prof_ms;
   if (launches) *launches = ctx->prof_launches;
   if (bytes) *bytes = ctx->prof_bytes;

@@ -154,15 +154,17 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
   const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
   const int L = it.tile * TL + lane;
   const int grp = live ? bv.lane_group[L] : -1;
-  GroupInfo gi;
-  if (grp >= 0) gi = bv.ginfo[grp];
-  else { gi.flags = 0; gi.frozen_sp = 0; gi.chimask = 0; for (int l = 0; l < 9; ++l) gi.dd[l] = 0.0; }
-  if (w == 0) for (int l = 0; l < 9; ++l) dds[lane * 9 + l] = gi.dd[l];
+  unsigned long long chimask = 0ull;
+  int gflags = 0, gfrozen = 0;
+  if (grp >= 0) {
+    chimask = bv.ginfo[grp].chimask;
+    gflags = bv.ginfo[grp].flags;
+    gfrozen = bv.ginfo[grp].frozen_sp;
+  }
+  if (w == 0)
+    for (int l = 0; l < 9; ++l) dds[lane * 9 + l] = grp >= 0 ? bv.ginfo[grp].dd[l] : 0.0;
   __syncthreads();
   if (!live) return;
-  const double* gb = bv.gblob + (size_t)(grp >= 0 ? grp : 0) * bv.GL.stride;
-  const double2 z = bv.lane_z[L];
-  const double2 s = bv.su[L];
   double2 dot = make_double2(0.0, 0.0);
   for (int qn = 0; qn < npw; ++qn) {
     int i = it.first + w + WPB * qn;
@@ -170,15 +172,15 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
     const ST* B = Bs + (size_t)op.typ[i] * ns1 * 81;
     T2 acc[9];
     for (int l = 0; l < 9; ++l) { acc[l].x = 0; acc[l].y = 0; }
-    double2 xi[9];   // own node: x0 = U / sq (FUSE_D) or t1
-    {
-      double f = FUSE_D ? op.isq[i] : 1.0;
-      for (int l = 0; l < 9; ++l) xi[l] = cscale(ld(in + vix(it.tile, bv.nn, i, l) + lane), f);
+    {   // on-site block: own node, t1 = d o (U / sq) (FUSE_D) or t1
+      const ST f = FUSE_D ? (ST)op.isq[i] : (ST)1;
+      const T2* src = in + vix(it.tile, bv.nn, i, 0) + lane;
       T2 v[9];
       for (int l2 = 0; l2 < 9; ++l2) {
-        double dl = FUSE_D ? dds[lane * 9 + l2] : 1.0;
-        v[l2].x = (ST)(xi[l2].x * dl);
-        v[l2].y = (ST)(xi[l2].y * dl);
+        T2 x = src[l2 * TL];
+        ST fl = FUSE_D ? f * (ST)dds[lane * 9 + l2] : f;
+        v[l2].x = x.x * fl;
+        v[l2].y = x.y * fl;
       }
       for (int l2 = 0; l2 < 9; ++l2)
         for (int l = 0; l < 9; ++l) {
@@ -192,7 +194,7 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
       if (r < 0) continue;
       int g = op.hopg[k + op.nslot * i];
       const uint32_t sgm = sgs[g];
-      const bool neg = (gi.chimask >> g) & 1ull;
+      const bool neg = (chimask >> g) & 1ull;
       const ST f = FUSE_D ? (ST)op.isq[r] : (ST)1;
       const T2* src = in + vix(it.tile, bv.nn, r, 0) + lane;
       T2 v[9];
@@ -215,15 +217,37 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
     if (!FINAL) {
       for (int l = 0; l < 9; ++l) stv(out + vix(it.tile, bv.nn, i, l) + lane, make_double2(acc[l].x, acc[l].y));
     } else {
-      double2 pt[9];
-      rand_term(op, gi, gb, bv.GL, PCEB, !(gi.flags & GF_X_ZERO), z, in, it.tile, i, lane, true, pt, xi);
-      double sqi = op.sq[i];
+      // y_l = s sq (d_l t2_l + P_l(x0)),  P = c + e + X(z) (src/asr_augblk.f90:219-250), orbital by orbital
+      const double* gb = bv.gblob + (size_t)(grp >= 0 ? grp : 0) * bv.GL.stride;
+      const double2 z = bv.lane_z[L];
+      const double2 s = bv.su[L];
+      const bool withx = !(gflags & GF_X_ZERO);
+      const double sqi = op.sq[i], isqi = op.isq[i];
+      const int fs = (op.start[i] && gfrozen > 0) ? gfrozen : (int)op.frozen[i];
+      const int nsm = op.nsmax, kap = op.ncl[i], l0 = op.lst[i], nk = op.nsc[kap];
       for (int l = 0; l < 9; ++l) {
+        double2 ui = ld(in + vix(it.tile, bv.nn, i, l) + lane);
+        double2 x0 = cscale(ui, isqi);
+        double2 pt;
+        if (fs > 0) {
+          pt = cmul(praw(gb, bv.GL, PCEB, withx, z, fs, l), x0);
+        } else {
+          pt = cmul(pweight(gb, bv.GL, PCEB, withx, z, nsm, kap, l0, l0, l), x0);
+          for (int k = 0; k < nk; ++k) {
+            if (k == l0) continue;
+            int r = op.flipr[k + nsm * i];
+            if (r < 0) continue;
+            int g = op.flipg[k + nsm * i];
+            bool neg = (chimask >> g) & 1ull;
+            double fr = ((((uint32_t)sgs[g] >> l) & 1u) ^ (neg ? 1u : 0u)) ? -op.isq[r] : op.isq[r];
+            double2 xr = cscale(ld(in + vix(it.tile, bv.nn, r, pis[g * 9 + l]) + lane), fr);
+            pt = cadd(pt, cmul(pweight(gb, bv.GL, PCEB, withx, z, nsm, kap, l0, k, l), xr));
+          }
+        }
         double2 h = cscale(make_double2(acc[l].x, acc[l].y), dds[lane * 9 + l]);
-        double2 y = cmul(s, cscale(cadd(h, pt[l]), sqi));
+        double2 y = cmul(s, cscale(cadd(h, pt), sqi));
         stv(out + vix(it.tile, bv.nn, i, l) + lane, y);
-        double2 u = cmul(s, cscale(xi[l], sqi));   // u = s U
-        dot = cadd(dot, cmul(u, y));
+        dot = cadd(dot, cmul(cmul(s, ui), y));
       }
     }
   }
@@ -459,18 +483,29 @@ __global__ void k_reduce_b(BatchView bv, const double2* part, int bpt, int k, do
   if (lane == 0) bv.tile_act[tile] = any != 0;
 }
 
-// final fraction of every lane: cf_species with the chosen tail (edc mode)
-__global__ void k_cf_final(BatchView bv, int nlane, double2* g) {
+// final fraction of every lane: cf_species with the chosen tail (edc mode); lmap: batch lane -> output lane (-1: none)
+__global__ void k_cf_final(BatchView bv, int nlane, const int* lmap, double2* g) {
   int L = blockIdx.x * blockDim.x + threadIdx.x;
   if (L >= nlane) return;
-  if (bv.lane_group[L] < 0) return;
+  int dst = lmap[L];
+  if (bv.lane_group[L] < 0 || dst < 0) return;
   int m = bv.lane_m[L];
   double2 wd[NLMAX], we[NLMAX];
   int nf = 0;
-  g[L] = m > 0 ? cf_species_dev(bv.acoef + (size_t)L * NLMAX, bv.bcoef + (size_t)L * NLMAX, m, bv.lane_z[L], bv.tail, wd, we, &nf,
-                                nullptr)
-               : make_double2(0, 0);
+  g[dst] = m > 0 ? cf_species_dev(bv.acoef + (size_t)L * NLMAX, bv.bcoef + (size_t)L * NLMAX, m, bv.lane_z[L], bv.tail, wd, we,
+                                  &nf, nullptr)
+                 : make_double2(0, 0);
   if (nf) atomicAdd(bv.nfall, nf);
+}
+
+// depths of the batch lanes into the run's array, and the energies of the batch lanes from the run's array
+__global__ void k_scatter_m(int nlane, const int* lmap, const int* m, int* m_all) {
+  int L = blockIdx.x * blockDim.x + threadIdx.x;
+  if (L < nlane && lmap[L] >= 0) m_all[lmap[L]] = m[L];
+}
+__global__ void k_gather_z(int nlane, const int* lmap, const double2* z_all, double2* z) {
+  int L = blockIdx.x * blockDim.x + threadIdx.x;
+  if (L < nlane) z[L] = lmap[L] >= 0 ? z_all[lmap[L]] : make_double2(0.0, 0.0);
 }
 
 // start vectors: U = e_(node 0, l0) with scale 1, UP = 0
@@ -603,21 +638,32 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   ASR_CUDA(cudaMemsetAsync(d_nfall.p, 0, sizeof(int), s));
   if (a_out) { a_out->assign((size_t)nlane * NLMAX, make_double2(0, 0)); b_out->assign((size_t)nlane * NLMAX, make_double2(0, 0)); }
   if (m_out) m_out->assign(nlane, 0);
-  std::vector<int> hgroup(nlp), hm(nlp);
+  std::vector<int> hgroup(nlp), lmap(nlp), hm_all(nlane, 0);
   std::vector<double2> ha, hb;
-  int64_t nsteps = 0;
-  const int grid = tpb * bpt;
+  Dev<int> d_lmap, d_m_all;
+  ASR_TRY(d_lmap.alloc(nlp));
+  ASR_TRY(d_m_all.alloc(nlane));
+  ASR_CUDA(cudaMemsetAsync(d_m_all.p, 0, nlane * sizeof(int), s));
+  // tiles of 32 consecutive lanes, deepest first, so that every batch runs to one depth
+  std::vector<int> tdepth(ntile_all, 0), order(ntile_all);
+  for (int L = 0; L < nlane; ++L) tdepth[L / TL] = std::max(tdepth[L / TL], ginfo[lane_group[L]].nlev);
+  for (int t = 0; t < ntile_all; ++t) order[t] = t;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return tdepth[x] > tdepth[y]; });
+  std::vector<double2> one(nlp, make_double2(1.0, 0.0));
   for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
     const int nt = std::min(tpb, ntile_all - t0);
-    for (int q = 0; q < nlp; ++q) {
-      int L = t0 * TL + q;
-      hgroup[q] = (q < nt * TL && L < nlane) ? lane_group[L] : -1;
-    }
-    int nactive_lanes = 0, kmax = 0;
-    for (int q = 0; q < nlp; ++q) if (hgroup[q] >= 0) { ++nactive_lanes; kmax = std::max(kmax, ginfo[hgroup[q]].nlev); }
+    int kmax = 0;
     std::vector<int> tact(tpb, 0), ones(nlp, 0);
-    for (int q = 0; q < nlp; ++q) if (hgroup[q] >= 0) { tact[q / TL] = 1; ones[q] = 1; }
+    for (int q = 0; q < nlp; ++q) {
+      int bt = q / TL;
+      int L = bt < nt ? order[t0 + bt] * TL + q % TL : -1;
+      if (L >= nlane) L = -1;
+      lmap[q] = L;
+      hgroup[q] = L >= 0 ? lane_group[L] : -1;
+      if (hgroup[q] >= 0) { kmax = std::max(kmax, ginfo[hgroup[q]].nlev); tact[bt] = 1; ones[q] = 1; }
+    }
     ASR_CUDA(cudaMemcpyAsync(d_lgroup.p, hgroup.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_lmap.p, lmap.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemcpyAsync(d_act.p, ones.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemcpyAsync(d_tact.p, tact.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemsetAsync(d_wact.p, 0, nlp * sizeof(int), s));
@@ -627,21 +673,16 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
     ASR_CUDA(cudaMemsetAsync(d_gprev.p, 0, nlp * sizeof(double2), s));
     ASR_CUDA(cudaMemsetAsync(d_bprev.p, 0, nlp * sizeof(double2), s));
     ASR_CUDA(cudaMemsetAsync(d_sup.p, 0, nlp * sizeof(double2), s));
-    ASR_CUDA(cudaMemsetAsync(d_z.p, 0, nlp * sizeof(double2), s));
-    {
-      int nl = std::min(nlp, nlane - t0 * TL);
-      ASR_CUDA(cudaMemcpyAsync(d_z.p, d_lane_z + (size_t)t0 * TL, nl * sizeof(double2), cudaMemcpyDeviceToDevice, s));
-      std::vector<double2> one(nlp, make_double2(1.0, 0.0));
-      ASR_CUDA(cudaMemcpyAsync(d_su.p, one.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
-    }
+    ASR_CUDA(cudaMemcpyAsync(d_su.p, one.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
+    k_gather_z<<<(nlp + 127) / 128, 128, 0, s>>>(nlp, d_lmap.p, d_lane_z, d_z.p);
     BatchView bv{nt, nn, op->nsmax, 0, opt.mode, opt.project, opt.tail, NLMAX, opt.depth_tol, d_gblob.p, GL, d_ginfo.p,
                  d_lgroup.p, d_z.p, d_act.p, d_wact.p, d_m.p, d_a.p, d_b.p, d_gprev.p, d_acur.p, d_bprev.p, d_su.p, d_sup.p,
                  d_tact.p, d_nfall.p};
     k_init<ST><<<std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256), 256, 0, s>>>(bv, V[1].p, V[0].p);
+    ctx->launches += 2;
     const int gridb = nt * bpt;
-    int nev = 0;
-    if (ctx->profile) {
-      while ((int)ctx->ev_pool.size() < 2 * kmax) {
+    if (ctx->profile) {   // event pairs stay pending until asr_ctx_kernel_stats reads them (no synchronisation here)
+      while ((int)ctx->ev_pool.size() < 2 * (ctx->ev_used + kmax)) {
         cudaEvent_t e;
         ASR_CUDA(cudaEventCreate(&e));
         ctx->ev_pool.push_back(e);
@@ -652,12 +693,12 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
       T2* U = V[k % 3].p;
       T2* UP = V[(k + 2) % 3].p;
       T2* Y = V[(k + 1) % 3].p;
-      if (ctx->profile) ASR_CUDA(cudaEventRecord(ctx->ev_pool[2 * nev], s));
+      if (ctx->profile) ASR_CUDA(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used], s));
       ASR_TRY(step_apply<ST>(ctx, op, bv, fused, any_o, all_dunif, U, Y, nvec > 3 ? V[3].p : nullptr, nvec > 3 ? V[4].p : nullptr,
                              nvec > 5 ? V[5].p : nullptr, nvec > 5 ? V[6].p : nullptr, d_part.p, npw, gridb));
       if (ctx->profile) {
-        ASR_CUDA(cudaEventRecord(ctx->ev_pool[2 * nev + 1], s));
-        ++nev;
+        ASR_CUDA(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used + 1], s));
+        ++ctx->ev_used;
         // algorithmic traffic of one operator pass: read U and write Y per (node, lane), plus the node tables per tile
         const double tab = (double)op->nslot * 5 + (double)op->nsmax * 5 + 8 + 8 + 4;
         ctx->prof_bytes += (double)nt * nn * (2.0 * 9 * TL * sizeof(T2) + tab);
@@ -667,40 +708,36 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
       k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
       k_lanczos_w<ST><<<gridb, WPB * TL, 0, s>>>(op->view(), bv, Y, U, UP, d_part.p, npw);
       k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
+      ctx->launches += 3 + (fused ? 1 : (any_o ? 7 : (all_dunif ? 2 : 3)));
     }
     ASR_CUDA(cudaGetLastError());
-    // results of the batch
     if (opt.mode == ASR_MODE_EDC && d_g_out) {
-      int nl = std::min(nlp, nlane - t0 * TL);
-      k_cf_final<<<(nl + 63) / 64, 64, 0, s>>>(bv, nl, d_g_out + (size_t)t0 * TL);
+      k_cf_final<<<(nlp + 63) / 64, 64, 0, s>>>(bv, nlp, d_lmap.p, d_g_out);
+      ctx->launches += 1;
     }
-    ha.resize((size_t)nlp * NLMAX); hb.resize((size_t)nlp * NLMAX);
-    ASR_CUDA(cudaMemcpyAsync(hm.data(), d_m.p, nlp * sizeof(int), cudaMemcpyDeviceToHost, s));
-    if (a_out) {
+    k_scatter_m<<<(nlp + 127) / 128, 128, 0, s>>>(nlp, d_lmap.p, d_m.p, d_m_all.p);
+    ctx->launches += 2;
+    if (a_out) {   // coefficients back to the host (tests): synchronise this batch
+      ha.resize((size_t)nlp * NLMAX); hb.resize((size_t)nlp * NLMAX);
       ASR_CUDA(cudaMemcpyAsync(ha.data(), d_a.p, (size_t)nlp * NLMAX * sizeof(double2), cudaMemcpyDeviceToHost, s));
       ASR_CUDA(cudaMemcpyAsync(hb.data(), d_b.p, (size_t)nlp * NLMAX * sizeof(double2), cudaMemcpyDeviceToHost, s));
-    }
-    ASR_CUDA(cudaStreamSynchronize(s));
-    ASR_CUDA(cudaGetLastError());
-    for (int q = 0; q < nev; ++q) {
-      float ms = 0.f;
-      ASR_CUDA(cudaEventElapsedTime(&ms, ctx->ev_pool[2 * q], ctx->ev_pool[2 * q + 1]));
-      ctx->prof_ms += ms;
-    }
-    for (int q = 0; q < nlp; ++q) {
-      int L = t0 * TL + q;
-      if (L >= nlane || hgroup[q] < 0) continue;
-      nsteps += hm[q];
-      if (m_out) (*m_out)[L] = hm[q];
-      if (a_out) {
-        std::memcpy(&(*a_out)[(size_t)L * NLMAX], &ha[(size_t)q * NLMAX], NLMAX * sizeof(double2));
-        std::memcpy(&(*b_out)[(size_t)L * NLMAX], &hb[(size_t)q * NLMAX], NLMAX * sizeof(double2));
-      }
+      ASR_CUDA(cudaStreamSynchronize(s));
+      ASR_CUDA(cudaGetLastError());
+        for (int q = 0; q < nlp; ++q) {
+          int L = lmap[q];
+          if (L < 0) continue;
+          std::memcpy(&(*a_out)[(size_t)L * NLMAX], &ha[(size_t)q * NLMAX], NLMAX * sizeof(double2));
+          std::memcpy(&(*b_out)[(size_t)L * NLMAX], &hb[(size_t)q * NLMAX], NLMAX * sizeof(double2));
+        }
     }
   }
+  ASR_CUDA(cudaMemcpyAsync(hm_all.data(), d_m_all.p, nlane * sizeof(int), cudaMemcpyDeviceToHost, s));
+  int64_t nsteps = 0;
   int nf = 0;
   ASR_CUDA(cudaMemcpyAsync(&nf, d_nfall.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaStreamSynchronize(s));
+  for (int L = 0; L < nlane; ++L) nsteps += hm_all[L];
+  if (m_out) *m_out = hm_all;
   if (nfall_out) *nfall_out = nf;
   if (nsteps_out) *nsteps_out = nsteps;
   return ASR_OK;

@@ -13,12 +13,14 @@ struct asr_ctx {
   cudaStream_t own_stream = nullptr;  // created by asr_ctx_create
   int num_sms = 148;
   int64_t nchain = 0, nlev = 0, nfall = 0;
+  int64_t launches = 0;   // kernels launched by this context
   int* d_err = nullptr;   // device error word
   // kernel timing (asr_ctx_profile)
   int profile = 0;
   double prof_ms = 0.0, prof_bytes = 0.0, prof_flops = 0.0;
   int64_t prof_launches = 0;
-  std::vector<cudaEvent_t> ev_pool;
+  std::vector<cudaEvent_t> ev_pool;   // pairs (start, end) of the timed launches
+  int ev_used = 0;                    // pairs recorded and not yet read
 };
 
 namespace asrb {

@@ -220,6 +220,7 @@ def main():
     clk = Clocks(local)
     clk.start()
     ctx.profile(True)
+    launches0 = ctx.launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for it in range(args.steps):
@@ -230,6 +231,7 @@ def main():
     if world > 1:
         dist.barrier()
     ms = e0.elapsed_time(e1)
+    launches = ctx.launches() - launches0
     ks = ctx.kernel_stats()
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -289,11 +291,9 @@ def main():
                          "per_launch_ms": per_launch_ms, "launches": ks["launches"], "fp64_tflops": tflops,
                          "share_of_step": ks["ms"] / ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
             "cpu_baseline": cpu,
-            "gpu_launches": None,
+            "gpu_launches": int(launches),
             "clocks": clocks,
         }
-        # kernels per step of one batch: step kernel + 3 per level, plus init and the final fractions
-        line["gpu_launches"] = int(ks["launches"] * 4 + 2 * max(ks["launches"] // 20, 1))
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

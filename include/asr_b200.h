@@ -58,7 +58,9 @@ int asr_ctx_set_stream(asr_ctx* ctx, void* stream);
  * on = 1 starts (and clears) it; asr_ctx_kernel_stats returns the summed device time, the launches and the algorithmic
  * bytes and flops of those launches */
 int asr_ctx_profile(asr_ctx* ctx, int on);
-int asr_ctx_kernel_stats(const asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops);
+int asr_ctx_kernel_stats(asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops);
+/* number of kernels this context has launched (all kinds) */
+int asr_ctx_launches(asr_ctx* ctx, int64_t* launches);
 
 /* ---- operator: replaces augcls_op and build_augcls_operator (src/asr_augcls.f90:45-68, :596-823) ---------------- *
  * graph (graph_t, src/asr_augspace.f90:22-25): nbr_ptr(nsite+1), nbr(*) 1-based (0: no bond on the slot, -1: beyond the
@@ -128,6 +130,30 @@ int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
  * z(nz, nchain): g(nz, nchain).  edges (optional, (2, nz, nchain)) returns the tail (centre, quarter width). */
 int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain, const double* z, int nz,
                 int tail, double* g, double* edges, int64_t* nfall);
+
+/* ---- KPM on an explicit supercell: kpm_moments / kpm_dos (src/reference/asr_kpm.f90:39-87) on the realisation operator
+ *      lmto_real_op (src/reference/asr_lmto_realization.f90:14-191), n species ------------------------------------------- */
+typedef struct asr_supercell asr_supercell;
+/* nbr(nslot, nsite) 1-based neighbour of every slot, spc(nsite) species 1..nsp, c/d/o/e(9, nsp), block(9, 9, nslot),
+ * block0(9, 9) (NULL: zero).  H = E_nu + h - h o h, h = c + d S d, per site by its species (build_lmto_ordered :49-77). */
+int asr_supercell_build(asr_ctx* ctx, int nsite, int nslot, const int* nbr, const int* spc, int nsp, const double* c,
+                        const double* d, const double* o, const double* e, const double* block, const double* block0,
+                        asr_supercell** sc);
+int asr_supercell_free(asr_supercell* sc);
+/* real_apply (:149-191): y = H x for nvec real vectors x(9 nsite, nvec) */
+int asr_supercell_apply(asr_supercell* sc, const double* x, double* y, int nvec);
+/* mu(0:nmom-1) = (1/nvec) sum_r <r|T_n((H - cen)/sc)|r> / dim over the Rademacher vectors v0 .. v0+nvec-1 of the
+ * counter-based generator (entry q of vector v is +1 iff bit 63 of splitmix64(seed * 0x9E3779B97F4A7C15 + (v << 40) + q)
+ * is clear); precision ASR_FP32: FP32 matvec and vectors, FP64 moments.  doubling = 1 takes two moments per matvec. */
+int asr_kpm_moments(asr_ctx* ctx, asr_supercell* sc, double cen, double scl, int nmom, int v0, int nvec, uint64_t seed,
+                    int precision, int doubling, double* mu);
+/* kpm_dos (:68-87), Jackson kernel, host */
+int asr_kpm_dos(const double* mu, int nmom, double cen, double scl, const double* e, int ne, double* rho);
+/* species layout with first-shell Warren-Cowley order (the role of tools/sqs.py --alpha and tools/sro_closure/sro_mc.c,
+ * own swap Monte Carlo): the first z slots of nbr(ldnbr, nsite) are the first shell; alpha(nsp, nsp) unlike-pair targets
+ * (NULL: random); spc(nsite) 1-based output; alpha_out(nsp, nsp) the achieved parameters.  Host. */
+int asr_sro_layout(int nsite, int z, const int* nbr, int ldnbr, int nsp, const double* conc, const double* alpha,
+                   uint64_t seed, int sweeps, int* spc, double* alpha_out);
 
 /* ---- contour (src/asr_contour.f90), host ------------------------------------------------------------------------- */
 int asr_gauss_legendre(int n, double* x, double* w);

@@ -184,18 +184,18 @@ class OracleOp:
         par = _f64(par, True)
         x = _f64(x, True)
         w = np.zeros_like(x)
-        lib().orc_rand_c(self.h, _pd(par.view(np.float64)), _pd(x.view(np.float64)), _pd(w.view(np.float64)))
+        lib().orc_rand_c(self.h, _pd(par), _pd(x), _pd(w))
         return w
 
     def project_c(self, x):
         x = _f64(x, True).copy()
-        lib().orc_project_c(self.h, _pd(x.view(np.float64)))
+        lib().orc_project_c(self.h, _pd(x))
         return x
 
     def hp_c(self, x):
         x = _f64(x, True)
         y = np.zeros_like(x)
-        lib().orc_hp_c(self.h, _pd(x.view(np.float64)), _pd(y.view(np.float64)))
+        lib().orc_hp_c(self.h, _pd(x), _pd(y))
         return y
 
     # ---- chains
@@ -217,7 +217,7 @@ class OracleOp:
         m = C.c_int()
         nf = C.c_long(0)
         lib().orc_edc_green(self.h, dl.shape[1], _pd(dc), _pd(dl), _pd(en), z.real, z.imag, iv, nlev, depth_tol, TAILS[tail],
-                            int(project), _pd(g), _pd(a.view(np.float64)), _pd(b.view(np.float64)), C.byref(m), C.byref(nf))
+                            int(project), _pd(g), _pd(a), _pd(b), C.byref(m), C.byref(nf))
         return complex(g[0], g[1]), a[: m.value], b[: m.value], m.value, nf.value
 
     def edc_green_blk(self, ed, zs, iv, nlev, depth_tol=0.0, tail="hull", project=True):
@@ -230,9 +230,9 @@ class OracleOp:
         a = np.zeros((nb, nlev), np.complex128)   # memory order of Fortran a(nlev, nb)
         b = np.zeros((nb, nlev), np.complex128)
         nf = C.c_long(0)
-        lib().orc_edc_green_blk(self.h, dl.shape[1], _pd(dc), _pd(dl), _pd(en), _pd(zs.view(np.float64)), nb, iv, nlev,
-                                depth_tol, TAILS[tail], int(project), _pd(g.view(np.float64)), _pi(mu),
-                                _pd(a.view(np.float64)), _pd(b.view(np.float64)), C.byref(nf))
+        lib().orc_edc_green_blk(self.h, dl.shape[1], _pd(dc), _pd(dl), _pd(en), _pd(zs), nb, iv, nlev,
+                                depth_tol, TAILS[tail], int(project), _pd(g), _pi(mu),
+                                _pd(a), _pd(b), C.byref(nf))
         return g, mu, a.T, b.T
 
     def chain_greens(self, groups, gcomp, iorb, nlevq, zs, nbe, depth_tol=0.0, tail="hull", project=True, nthreads=0):
@@ -249,8 +249,8 @@ class OracleOp:
         steps = C.c_long(0)
         assert P.shape[0] == len(groups) * (4 * 9 * nsp + 9 + 18 * nsp)
         _check(lib().orc_chain_greens(self.h, len(groups), _pd(P), _pi(gcomp), len(iorb), _pi(iorb), _pi(nlevq),
-                                      _pd(zs.view(np.float64)), nz, nbe, depth_tol, TAILS[tail], int(project), nthreads,
-                                      _pd(gz.view(np.float64)), C.byref(steps)))
+                                      _pd(zs), nz, nbe, depth_tol, TAILS[tail], int(project), nthreads,
+                                      _pd(gz), C.byref(steps)))
         return gz.transpose(2, 1, 0), steps.value
 
 
@@ -259,7 +259,7 @@ def chain_eigvals(a, b):
     a = np.ascontiguousarray(a, np.complex128)
     b = np.ascontiguousarray(b, np.complex128)
     ev = np.zeros(a.shape[0], np.complex128)
-    rc = lib().orc_chain_eigvals(a.shape[0], _pd(a.view(np.float64)), _pd(b.view(np.float64)), _pd(ev.view(np.float64)))
+    rc = lib().orc_chain_eigvals(a.shape[0], _pd(a), _pd(b), _pd(ev))
     if rc:
         raise RuntimeError("chain_eigvals: QR did not converge")
     return ev
@@ -277,8 +277,8 @@ def cf_species(a, b, m, z, tail="hull", c=None, want_pv=False):
     e = np.zeros(2, np.complex128)
     pv = np.zeros(max(m, 1), np.complex128)
     nf = C.c_long(0)
-    lib().orc_cf_species(_pd(a.view(np.float64)), _pd(b.view(np.float64)), _pd(cc.view(np.float64)), m, z.real, z.imag,
-                         TAILS[tail], _pd(g), _pd(f), _pd(e.view(np.float64)), _pd(pv.view(np.float64)), C.byref(nf))
+    lib().orc_cf_species(_pd(a), _pd(b), _pd(cc), m, z.real, z.imag,
+                         TAILS[tail], _pd(g), _pd(f), _pd(e), _pd(pv), C.byref(nf))
     return complex(g[0], g[1]), complex(f[0], f[1]), e, (pv if want_pv else None), nf.value
 
 
@@ -302,7 +302,7 @@ def terminated_green(a, b, n, z, method="beer-pettifor", join="butt", ninterp=0)
     g = np.zeros(z.shape[0], np.complex128)
     tp = np.zeros(3)
     _check(lib().orc_terminated_green(_pd(a), _pd(b), n, METHODS[method], 1 if join == "luchini-nex" else 0, ninterp,
-                                      _pd(z.view(np.float64)), z.shape[0], _pd(g.view(np.float64)), _pd(tp)))
+                                      _pd(z), z.shape[0], _pd(g), _pd(tp)))
     return g, tp
 
 
@@ -344,14 +344,14 @@ def gauss_legendre(n):
 def contour_nodes(ebot, ef, n, eta_end=None):
     z = np.zeros(n, np.complex128)
     w = np.zeros(n, np.complex128)
-    lib().orc_contour_nodes(ebot, ef, n, -1.0 if eta_end is None else eta_end, _pd(z.view(np.float64)), _pd(w.view(np.float64)))
+    lib().orc_contour_nodes(ebot, ef, n, -1.0 if eta_end is None else eta_end, _pd(z), _pd(w))
     return z, w
 
 
 def contour_nodes_closed(ebot, ef, eta, n_arc, n_vert):
     z = np.zeros(n_arc + n_vert, np.complex128)
     w = np.zeros(n_arc + n_vert, np.complex128)
-    lib().orc_contour_nodes_closed(ebot, ef, eta, n_arc, n_vert, _pd(z.view(np.float64)), _pd(w.view(np.float64)))
+    lib().orc_contour_nodes_closed(ebot, ef, eta, n_arc, n_vert, _pd(z), _pd(w))
     return z, w
 
 
@@ -359,7 +359,7 @@ def contour_nodes_fermi(ebot, mu, kt, npole, n_main, n_step):
     n = 4 + n_main + n_step + 8 + npole
     z = np.zeros(n, np.complex128)
     w = np.zeros(n, np.complex128)
-    lib().orc_contour_nodes_fermi(ebot, mu, kt, npole, n_main, n_step, _pd(z.view(np.float64)), _pd(w.view(np.float64)))
+    lib().orc_contour_nodes_fermi(ebot, mu, kt, npole, n_main, n_step, _pd(z), _pd(w))
     return z, w
 
 
@@ -367,7 +367,7 @@ def contour_moment(z, w, g, enu, k):
     z = np.ascontiguousarray(z, np.complex128)
     w = np.ascontiguousarray(w, np.complex128)
     g = np.ascontiguousarray(g, np.complex128)
-    return lib().orc_contour_moment(_pd(z.view(np.float64)), _pd(w.view(np.float64)), _pd(g.view(np.float64)), z.shape[0],
+    return lib().orc_contour_moment(_pd(z), _pd(w), _pd(g), z.shape[0],
                                     enu, k)
 
 
