@@ -709,6 +709,21 @@ int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, in
   return ASR_OK;
 }
 
+// reverse mode of one terminated fraction (host): abar/bbar(m) complex receive w dG/da_k, w dG/db_k
+int asr_cf_adjoint(const double* a, const double* b, int m, double zr, double zi, int tail, double wr, double wi, double* abar,
+                   double* bbar, double* g) {
+  if (!a || !b || !abar || !bbar || m < 1 || m > CF_NMAX || tail < 0 || tail > 3 || tail == ASR_TAIL_BP) {
+    set_error("asr_cf_adjoint: bad argument (tails none, hull, avg2; 1 <= m <= %d)", CF_NMAX);
+    return ASR_EINVAL;
+  }
+  std::vector<double2> gt(m), v(m), t(m), wd(m), we(m);
+  for (int k = 0; k < m; ++k) { ((double2*)abar)[k] = make_double2(0, 0); ((double2*)bbar)[k] = make_double2(0, 0); }
+  double2 G = cf_species_adjoint((const double2*)a, (const double2*)b, m, make_double2(zr, zi), tail, make_double2(wr, wi),
+                                 (double2*)abar, (double2*)bbar, gt.data(), v.data(), t.data(), wd.data(), we.data());
+  if (g) { g[0] = G.x; g[1] = G.y; }
+  return ASR_OK;
+}
+
 // ---- contour (src/asr_contour.f90), host
 static const double PI_ = 3.14159265358979323846264338327950288;
 

@@ -199,6 +199,121 @@ __host__ __device__ inline double2 terminated_green_dev(const double* a, const d
   return g;
 }
 
+
+// ---- reverse mode of cf_species (tails none, hull, avg2): abar_k += w dG/da_k, bbar_k += w dG/db_k.  G is holomorphic in
+// (a, b) away from the branch choices, so the complex derivatives compose.  The hull edges are extreme eigenvalues of
+// the chain matrix T; for a simple eigenvalue of a complex symmetric matrix d(lambda) = v^T dT v / (v^T v), with v from
+// inverse iteration on T - lambda.  wd, we, wx: work (m).  Returns 0 on success.
+__host__ __device__ inline int tridiag_solve_shift(int m, const double2* a, const double2* b, double2 lam, const double2* rhs,
+                                                   double2* x, double2* wd, double2* we) {
+  // (T - lam) x = rhs, Thomas algorithm on the complex symmetric tridiagonal (no pivoting; lam is perturbed off the
+  // eigenvalue by the caller)
+  double2 dd = csub(a[0], lam);
+  if (cabs2(dd) == 0.0) dd = make_double2(1e-300, 0.0);
+  wd[0] = dd;
+  x[0] = rhs[0];
+  for (int j = 1; j < m; ++j) {
+    double2 l = cdiv(b[j - 1], wd[j - 1]);
+    we[j - 1] = l;
+    double2 d = csub(csub(a[j], lam), cmul(l, b[j - 1]));
+    if (cabs2(d) == 0.0) d = make_double2(1e-300, 0.0);
+    wd[j] = d;
+    x[j] = csub(rhs[j], cmul(l, x[j - 1]));
+  }
+  x[m - 1] = cdiv(x[m - 1], wd[m - 1]);
+  for (int j = m - 2; j >= 0; --j) x[j] = cdiv(csub(x[j], cmul(b[j], x[j + 1])), wd[j]);
+  return 0;
+}
+
+__host__ __device__ inline void eig_grad(int m, const double2* a, const double2* b, double2 lam, double2 w, double2* abar,
+                                         double2* bbar, double2* v, double2* t, double2* wd, double2* we) {
+  // eigenvector by two steps of inverse iteration at a shift next to lam, then dlam/da_j = v_j^2 / (v.v)
+  double sc = 0.0;
+  for (int j = 0; j < m; ++j) sc = fmax(sc, cabs2(a[j]) + (j < m - 1 ? cabs2(b[j]) : 0.0));
+  double2 mu = cadd(lam, make_double2(1e-10 * (sc + 1.0), 1e-10 * (sc + 1.0)));
+  for (int j = 0; j < m; ++j) t[j] = make_double2(1.0 / sqrt((double)m), 0.0);
+  for (int it = 0; it < 3; ++it) {
+    tridiag_solve_shift(m, a, b, mu, t, v, wd, we);
+    double nr = 0.0;
+    for (int j = 0; j < m; ++j) nr = fmax(nr, cabs2(v[j]));
+    for (int j = 0; j < m; ++j) t[j] = cscale(v[j], 1.0 / nr);
+  }
+  double2 vv = make_double2(0.0, 0.0);
+  for (int j = 0; j < m; ++j) vv = cadd(vv, cmul(t[j], t[j]));
+  double2 f = cdiv(w, vv);
+  for (int j = 0; j < m; ++j) abar[j] = cadd(abar[j], cmul(f, cmul(t[j], t[j])));
+  for (int j = 0; j < m - 1; ++j) bbar[j] = cadd(bbar[j], cmul(f, cscale(cmul(t[j], t[j + 1]), 2.0)));
+}
+
+// w: seed; work arrays of length >= m each: gt, v, t, wd, we.  Returns G.
+__host__ __device__ inline double2 cf_species_adjoint(const double2* a, const double2* b, int m, double2 z, int tail, double2 w,
+                                                       double2* abar, double2* bbar, double2* gt, double2* v, double2* t, double2* wd,
+                                                       double2* we) {
+  // forward: tail parameters
+  double2 aa = make_double2(0, 0), bb = make_double2(0, 0), lo, hi;
+  int kind = 0;   // 0 none / finite, 1 hull, 3 avg2
+  if (tail == 3 && m >= 3) {
+    aa = cscale(cadd(a[m - 1], a[m - 2]), 0.5);
+    bb = csqrt_p(cscale(cadd(cmul(b[m - 2], b[m - 2]), cmul(b[m - 3], b[m - 3])), 0.5));
+    kind = 3;
+  } else if (tail == 1 && m >= 2 && chain_extremes(a, b, m, a[m - 1], wd, we, lo, hi) == 0) {
+    aa = cscale(cadd(lo, hi), 0.5);
+    bb = cscale(csub(hi, lo), 0.25);
+    kind = 1;
+  } else if (tail != 0 && m >= 1) {   // eigenvalue failure or m = 1: the last coefficients (src/asr_chain.f90:95)
+    aa = a[m - 1];
+    bb = m > 1 ? b[m - 2] : make_double2(0.0, 0.0);
+    kind = 2;
+  }
+  double2 d = csub(z, aa), tl = make_double2(0, 0), sroot = make_double2(0, 0);
+  double sig = 0.0;
+  bool has_tail = cabs2(bb) >= 1.0e-14;
+  if (has_tail) {
+    double2 bb2 = cmul(bb, bb);
+    sroot = csqrt_p(csub(cmul(d, d), cscale(bb2, 4.0)));
+    double2 g1 = cdiv(csub(d, sroot), cscale(bb2, 2.0)), g2 = cdiv(cadd(d, sroot), cscale(bb2, 2.0));
+    if (cabs2(cmul(bb, g1)) <= cabs2(cmul(bb, g2))) { tl = cmul(bb2, g1); sig = 1.0; }
+    else { tl = cmul(bb2, g2); sig = -1.0; }
+  }
+  double2 one = make_double2(1.0, 0.0);
+  gt[m - 1] = cdiv(one, csub(csub(z, a[m - 1]), tl));
+  for (int j = m - 2; j >= 0; --j) gt[j] = cdiv(one, csub(csub(z, a[j]), cmul(cmul(b[j], b[j]), gt[j + 1])));
+  // reverse: gbar_j is the adjoint of gt_j
+  double2 gbar = w;
+  double2 tbar = make_double2(0, 0);
+  for (int j = 0; j < m; ++j) {
+    double2 Dbar = cmul(cscale(cmul(gt[j], gt[j]), -1.0), gbar);   // d gt / dD = -gt^2
+    abar[j] = csub(abar[j], Dbar);
+    if (j < m - 1) {
+      bbar[j] = csub(bbar[j], cscale(cmul(cmul(b[j], gt[j + 1]), Dbar), 2.0));
+      gbar = csub(make_double2(0, 0), cmul(cmul(b[j], b[j]), Dbar));
+    } else {
+      tbar = csub(make_double2(0, 0), Dbar);
+    }
+  }
+  if (has_tail && kind != 0) {
+    // T = (d - sig s) / 2, s^2 = d^2 - 4 bb^2, d = z - aa
+    double2 aabar = cscale(cmul(tbar, csub(cscale(cdiv(d, sroot), sig), one)), 0.5);
+    double2 bbbar = cmul(tbar, cscale(cdiv(bb, sroot), 2.0 * sig));
+    if (kind == 3) {
+      abar[m - 1] = cadd(abar[m - 1], cscale(aabar, 0.5));
+      abar[m - 2] = cadd(abar[m - 2], cscale(aabar, 0.5));
+      double2 f = cdiv(bbbar, cscale(bb, 2.0));   // d bb / d b_j = b_j / (2 bb)
+      bbar[m - 2] = cadd(bbar[m - 2], cmul(f, b[m - 2]));
+      bbar[m - 3] = cadd(bbar[m - 3], cmul(f, b[m - 3]));
+    } else if (kind == 2) {
+      abar[m - 1] = cadd(abar[m - 1], aabar);
+      if (m > 1) bbar[m - 2] = cadd(bbar[m - 2], bbbar);
+    } else {
+      // aa = (lo + hi)/2, bb = (hi - lo)/4
+      double2 wlo = csub(cscale(aabar, 0.5), cscale(bbbar, 0.25)), whi = cadd(cscale(aabar, 0.5), cscale(bbbar, 0.25));
+      eig_grad(m, a, b, lo, wlo, abar, bbar, v, t, wd, we);
+      eig_grad(m, a, b, hi, whi, abar, bbar, v, t, wd, we);
+    }
+  }
+  return gt[0];
+}
+
 // kernels of cf.cu
 __global__ void k_cf_eval(const double2* a, const double2* b, const int* m, int ld, int nchain, const double2* z, int nz, int tail,
                           double2* g, double2* edges, int* nfall);

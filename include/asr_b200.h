@@ -131,6 +131,11 @@ int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
 int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain, const double* z, int nz,
                 int tail, double* g, double* edges, int64_t* nfall);
 
+/* reverse mode of cf_species for one chain (host): abar(m), bbar(m) complex receive w dG/da_k and w dG/db_k; g = G.
+ * Tails none, hull, avg2 (the bp fixed point has no derivative here).  No counterpart in the reference. */
+int asr_cf_adjoint(const double* a, const double* b, int m, double zr, double zi, int tail, double wr, double wi, double* abar,
+                   double* bbar, double* g);
+
 /* ---- KPM on an explicit supercell: kpm_moments / kpm_dos (src/reference/asr_kpm.f90:39-87) on the realisation operator
  *      lmto_real_op (src/reference/asr_lmto_realization.f90:14-191), n species ------------------------------------------- */
 typedef struct asr_supercell asr_supercell;
