@@ -81,6 +81,25 @@ def chains_run(op: AugclsOp, specs, z, mode: str = "edc", depth_tol: float = 0.0
     return out
 
 
+def chains_adjoint(op: AugclsOp, specs, z, w, tail: str = "hull", precision: str = "fp64", project: bool = True,
+                   stride: int = 0):
+    """Reverse mode of the energy-dependent chains (o = 0, fixed depth): returns (g (nz, ngroup), grad) where
+    grad[q, kind, s, l] = sum_j w[j, q] dG[j, q] / dpar_kind(l, s) of group q, kind 0: c (equally e and pb, which enter
+    as c + e + pb), 1: d, 2: pa.  w (nz, ngroup) complex seeds.  Lanczos vectors are kept every ``stride`` levels
+    (0: ceil(sqrt(depth))) and recomputed in between."""
+    z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
+    nz = z.shape[0]
+    ng = len(specs)
+    w = np.asarray(w, np.complex128).reshape(nz, ng)
+    wl = np.ascontiguousarray(w.T)                       # lane order (group, energy)
+    arr, keep = _groups(specs)
+    g = np.zeros((ng, nz), np.complex128)
+    grad = np.zeros((ng, 3, op.nsp, 9), np.complex128)
+    check(lib().asr_chains_adjoint(op.ctx.h, op.h, arr, ng, _pd(z), nz, _pd(wl), _lib.TAILS[tail], PREC[precision],
+                                   int(bool(project)), int(stride), _pd(g), _pd(grad)))
+    return g.T, grad
+
+
 def chains_run_device(op: AugclsOp, specs, z_dev, g_dev, nz: int, mode: str = "edc", depth_tol: float = 0.0, tail: str = "hull",
                       precision: str = "fp64", project: bool = True):
     """Device-resident form: z_dev / g_dev are device pointers (ints, e.g. torch tensor data_ptr()) of complex128 arrays;

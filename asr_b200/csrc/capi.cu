@@ -103,7 +103,13 @@ int make_group(const asr_op* op, const GroupLayout& GL, const double* c, const d
     for (int q = 0; q < np; ++q) blob[GL.raw(p) + q] = P[p][q];
   }
   gi.flags = 0;
-  if (all_equal_species(P[PD], op->nsp)) gi.flags |= GF_D_UNIFORM;
+  // d uniform over the species and invariant under the orbital permutations of the group: D x = d o x with d
+  // commuting with every link operation, so it folds into the bond blocks
+  bool dinv = true;
+  for (int g = 0; g < op->nop && dinv; ++g)
+    for (int l = 0; l < 9; ++l)
+      if (P[PD][op->pi[l + 9 * g] - 1] != P[PD][l]) { dinv = false; break; }
+  if (all_equal_species(P[PD], op->nsp) && dinv) gi.flags |= GF_D_UNIFORM;
   if (all_zero(P[PO], np)) gi.flags |= GF_O_ZERO;
   if (all_zero(P[PE], np)) gi.flags |= GF_E_ZERO;
   if (all_zero(P[PA], np) && all_zero(P[PB], np)) gi.flags |= GF_X_ZERO;
@@ -644,6 +650,77 @@ static int chains_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups
   }
   ctx->nlev += nsteps;
   ctx->nfall += nfall;
+  return ASR_OK;
+}
+
+int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz,
+                       const double* w, int tail, int precision, int project, int stride, double* g, double* grad) {
+  if (!ctx || !op || !groups || ngroup < 1 || nz < 1 || !z || !w || !grad) { set_error("asr_chains_adjoint: bad argument"); return ASR_EINVAL; }
+  if (tail != ASR_TAIL_NONE && tail != ASR_TAIL_HULL && tail != ASR_TAIL_AVG2) {
+    set_error("asr_chains_adjoint: tail must be none, hull or avg2");
+    return ASR_EINVAL;
+  }
+  ASR_TRY(set_device(ctx));
+  GroupLayout GL = layout(op);
+  std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
+  std::vector<GroupInfo> gi(ngroup);
+  for (int q = 0; q < ngroup; ++q) {
+    const asr_chain_group& G = groups[q];
+    if (!G.c || !G.d || !G.pa || !G.pb) { set_error("asr_chains_adjoint: group %d needs c, d, pa, pb", q + 1); return ASR_EINVAL; }
+    if (G.nlev < 1 || G.nlev > NLMAX) { set_error("asr_chains_adjoint: depth %d out of range 1..%d", G.nlev, NLMAX); return ASR_EINVAL; }
+    ASR_TRY(make_group(op, GL, G.c, G.d, G.o, G.e, G.pa, G.pb, G.frozen_sp, G.start_orb, G.nlev, nullptr,
+                       blob.data() + (size_t)GL.stride * q, gi[q]));
+  }
+  const int nlane = ngroup * nz;
+  std::vector<int> lg(nlane);
+  std::vector<double2> lz(nlane), lw(nlane), hg, hgrad;
+  for (int q = 0; q < ngroup; ++q)
+    for (int j = 0; j < nz; ++j) {
+      size_t L = (size_t)q * nz + j;
+      lg[L] = q;
+      lz[L] = make_double2(z[2 * j], z[2 * j + 1]);
+      lw[L] = make_double2(w[2 * L], w[2 * L + 1]);
+    }
+  int rc = run_adjoint(ctx, op, gi, blob, GL, lg, lz, lw, tail, project, stride, precision, hg, hgrad);
+  if (rc != ASR_OK) return rc;
+  if (g)
+    for (int L = 0; L < nlane; ++L) { g[2 * L] = hg[L].x; g[2 * L + 1] = hg[L].y; }
+  const int nsp = op->nsp;
+  // orbits of the orbitals under the point group (pi of every operation): the group-reduced operator represents
+  // only parameters that are constant on each orbit, so the gradient is reported symmetrised over the orbits -- exact
+  // along every invariant direction (per l, per irreducible orbit), while the single orbitals of a degenerate orbit are
+  // not independent parameters
+  std::vector<int> orbit(9);
+  for (int l = 0; l < 9; ++l) orbit[l] = l;
+  for (bool changed = true; changed;) {
+    changed = false;
+    for (int gop = 0; gop < op->nop; ++gop)
+      for (int l = 0; l < 9; ++l) {
+        int m = op->pi[l + 9 * gop] - 1, r = std::min(orbit[l], orbit[m]);
+        if (orbit[l] != r || orbit[m] != r) { orbit[l] = orbit[m] = r; changed = true; }
+      }
+  }
+  std::vector<double2> sym(hgrad.size(), make_double2(0, 0));
+  for (int q = 0; q < ngroup; ++q)
+    for (int kind = 0; kind < 3; ++kind)
+      for (int sp = 0; sp < nsp; ++sp)
+        for (int l = 0; l < 9; ++l) {
+          double2 acc = make_double2(0, 0);
+          int cnt = 0;
+          for (int l2 = 0; l2 < 9; ++l2)
+            if (orbit[l2] == orbit[l]) { acc = cadd(acc, hgrad[(((size_t)q * 3 + kind) * 9 + l2) * nsp + sp]); ++cnt; }
+          sym[(((size_t)q * 3 + kind) * 9 + l) * nsp + sp] = cscale(acc, 1.0 / cnt);
+        }
+  for (int q = 0; q < ngroup; ++q)
+    for (int kind = 0; kind < 3; ++kind)
+      for (int l = 0; l < 9; ++l)
+        for (int sp = 0; sp < nsp; ++sp) {
+          double2 v = sym[(((size_t)q * 3 + kind) * 9 + l) * nsp + sp];
+          size_t dst = 2 * (l + 9 * (sp + (size_t)nsp * (kind + 3 * (size_t)q)));
+          grad[dst] = v.x;
+          grad[dst + 1] = v.y;
+        }
+  ctx->nchain += nlane;
   return ASR_OK;
 }
 

@@ -11,7 +11,7 @@ __global__ void k_cf_eval(const double2* a, const double2* b, const int* m, int 
                           double2* g, double2* edges, int* nfall) {
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)nz * nchain) return;
-  int c = (int)(t / nz), j = (int)(t % nz);
+  int c = (int)(t / nz);
   int mc = m[c];
   if (mc < 1 || mc > CF_NMAX) { g[t] = make_double2(0.0, 0.0); return; }
   double2 wd[CF_NMAX], we[CF_NMAX];
@@ -47,11 +47,11 @@ __global__ void k_real_green(const double* a, const double* b, const int* n, int
                              const double* binf, int method, const double2* z, int nz, double2* g) {
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)nz * nchain) return;
-  int c = (int)(t / nz), j = (int)(t % nz);
+  int c = (int)(t / nz);
   int nc = n[c];
   if (nc < 1) { g[t] = make_double2(0, 0); return; }
   bool tail = method != ASR_TAIL_NONE && nc >= 2 && binf[c] != 0.0;
-  g[t] = terminated_green_dev(a + (size_t)ld * c, b + (size_t)ld * c, nc, z[j], ainf[c], binf[c], tail);
+  g[t] = terminated_green_dev(a + (size_t)ld * c, b + (size_t)ld * c, nc, z[t % nz], ainf[c], binf[c], tail);
 }
 
 }  // namespace asrb

@@ -12,12 +12,15 @@
 // instead of the reference's btab(9, 9, nslot, nop, ntype).
 //
 // One chain step (general operator H = E_nu + h - h o h, h = c + d S d, plus X(z) = z pa + pb) is a short sequence of
-// node-parallel kernels; with d uniform and o = 0 (the edc route) it is one fused kernel: y = sq (d S d x0 +
-// (c + e + X(z)) x0) with x0 = u / sq and the dot a = u . y.  Vectors are kept unnormalised with a complex scale per
-// lane (u = s U); every kernel works on U and applies s once per node, which turns the normalisation u = w / b into a
-// scalar update.  Reductions (a, b) are per block partial sums in a fixed order followed by a per-tile pass, so the
-// result is bitwise the same in every run.
+// node-parallel kernels; with d uniform and o = 0 (the edc route) it is one fused kernel: y = d S d x + (c + e + X(z)) x
+// and the dot a = u . y.  Vectors are stored in amplitude coordinates (x = u / sqrt(orbit size)), so gathers need no
+// scaling and the dots carry the orbit size; they are kept unnormalised with a complex scale per lane (x = s X); every
+// kernel works on X and applies s once per node, which turns the normalisation u = w / b into a scalar update.  Tiles
+// hold the lanes of one group, so d (folded into the shared-memory blocks) and the characters chi are per tile.
+// Reductions (a, b) are per block partial sums in a fixed order followed by a per-tile pass, so the result is bitwise
+// the same in every run.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -42,6 +45,11 @@ __device__ __forceinline__ double2 ld(const double2* p) { return *p; }
 __device__ __forceinline__ double2 ld(const float2* p) { float2 v = *p; return make_double2(v.x, v.y); }
 __device__ __forceinline__ void stv(double2* p, double2 v) { *p = v; }
 __device__ __forceinline__ void stv(float2* p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
+// evict-first store / last-use load: streams that are read once must not push the gathered vector out of L2
+__device__ __forceinline__ void stv_cs(double2* p, double2 v) { __stcs(p, v); }
+__device__ __forceinline__ void stv_cs(float2* p, double2 v) { __stcs(p, make_float2((float)v.x, (float)v.y)); }
+__device__ __forceinline__ double2 ld_cs(const double2* p) { return __ldcs(p); }
+__device__ __forceinline__ double2 ld_cs(const float2* p) { float2 v = __ldcs(p); return make_double2(v.x, v.y); }
 
 __device__ __forceinline__ size_t vix(int tile, int nn, int node, int l) {
   return (((size_t)tile * nn + node) * 9 + l) * TL;
@@ -71,11 +79,11 @@ __device__ __forceinline__ int frozen_of(const OpView& op, const GroupInfo& gi, 
   return (op.start[i] && gi.frozen_sp > 0) ? gi.frozen_sp : (int)op.frozen[i];
 }
 
-// R_p(x) at node i for one lane: the random site-diagonal operator of apply_rand (src/asr_augcls.f90:380-403) on the
-// vector v (unscaled); norm: v is in normalised coordinates (x = v / sq), else amplitude coordinates.
+// R_p(v) at node i for one lane: the random site-diagonal operator of apply_rand (src/asr_augcls.f90:380-403) on the
+// vector v (unscaled, amplitude coordinates); xi_own: the node's own values of v.
 template <typename T2>
 __device__ __forceinline__ void rand_term(const OpView& op, const GroupInfo& gi, const double* gb, const GroupLayout& GL, int p,
-                                          bool withx, double2 z, const T2* v, int tile, int i, int lane, bool norm, double2* out,
+                                          bool withx, double2 z, const T2* v, int tile, int i, int lane, double2* out,
                                           const double2* xi_own) {
   int fs = frozen_of(op, gi, i);
   if (fs > 0) {
@@ -91,13 +99,12 @@ __device__ __forceinline__ void rand_term(const OpView& op, const GroupInfo& gi,
     int r = op.flipr[k + nsm * i];
     if (r < 0) continue;
     int g = op.flipg[k + nsm * i];
-    double f = norm ? op.isq[r] : 1.0;
     bool neg = (gi.chimask >> g) & 1ull;
     uint32_t sgm = op.sgm[g];
     for (int l = 0; l < 9; ++l) {
       int pl = op.pi[g * 9 + l];
       double2 x = ld(v + vix(tile, op.nn, r, pl) + lane);
-      double sgn = (((sgm >> l) & 1u) ^ (neg ? 1u : 0u)) ? -f : f;
+      double sgn = (((sgm >> l) & 1u) ^ (neg ? 1u : 0u)) ? -1.0 : 1.0;
       out[l] = cadd(out[l], cmul(pweight(gb, GL, p, withx, z, nsm, kap, l0, k, l), cscale(x, sgn)));
     }
   }
@@ -130,30 +137,40 @@ __device__ __forceinline__ void block_reduce_store(double2 v, double2* part, int
   }
 }
 
+// sign flip of a complex value by the sign bit (no floating-point operation)
+__device__ __forceinline__ double2 flip_if(double2 x, uint32_t bit) {
+  unsigned long long m = (unsigned long long)bit << 63;
+  return make_double2(__longlong_as_double(__double_as_longlong(x.x) ^ m), __longlong_as_double(__double_as_longlong(x.y) ^ m));
+}
+__device__ __forceinline__ float2 flip_if(float2 x, uint32_t bit) {
+  unsigned m = bit << 31;
+  return make_float2(__uint_as_float(__float_as_uint(x.x) ^ m), __uint_as_float(__float_as_uint(x.y) ^ m));
+}
+template <typename ST> struct Pair;
+template <> struct Pair<double> { typedef double2 T; };
+template <> struct Pair<float> { typedef float2 T; };
+
+constexpr int RW = 12;   // padded row of a shared-memory block (16-byte aligned pairs for FP64 and FP32)
+
 // ------------------------------------------------------------------------------------------------ S application
 // t2 = S t1 (src/asr_augcls.f90:456-477 / src/asr_augblk.f90:170-203), unscaled amplitude coordinates.
-// FUSE_D: t1 = d o (U / sq) is formed on the fly from the current vector U (d uniform per orbital).
-// FINAL (needs FUSE_D, o = 0): y = s sq (d o t2 + (c + e + X(z)) x0) and the partial dot U . y.
+// FUSE_D: t1 = d o U is folded into the shared-memory blocks (the tile's d per orbital; d is invariant under the orbital
+// permutations of the group).  FINAL (needs FUSE_D, o = 0): y = s (d o S d o U + (c + e + X(z)) U) and the partial dot
+// sum_i norb_i (s U_i) . y_i (normalised-coordinate bilinear form).  Group data are per tile (single-group tiles).
 template <typename ST, bool FUSE_D, bool FINAL>
 __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, const ST* __restrict__ blocks,
                                                    const typename St2<ST>::T* __restrict__ in,
                                                    typename St2<ST>::T* __restrict__ out, double2* part, int npw) {
   typedef typename St2<ST>::T T2;
-  extern __shared__ unsigned char smem_raw[];
+  typedef typename Pair<ST>::T P2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ns1 = op.nslot + 1;
-  ST* Bs = (ST*)smem_raw;                                        // [ntype][ns1][81]
-  uint8_t* pis = (uint8_t*)(Bs + (size_t)op.ntype * ns1 * 81);  // [nop][9]
-  uint16_t* sgs = (uint16_t*)(pis + ((op.nop * 9 + 1) & ~1));    // [nop]
-  double* dds = (double*)(((uintptr_t)(sgs + op.nop) + 15) & ~(uintptr_t)15);   // [TL][9]
+  ST* Bs = (ST*)smem_raw;                                                        // [ntype][ns1][9][RW]
+  unsigned long long* piw = (unsigned long long*)(smem_raw + (((size_t)op.ntype * ns1 * 9 * RW * sizeof(ST) + 15) & ~(size_t)15));
   NodeIter it;
   int bpt;
   bool live = node_iter(bv, npw, it, bpt);
-  for (int q = threadIdx.x; q < op.ntype * ns1 * 81; q += blockDim.x) Bs[q] = blocks[q];
-  for (int q = threadIdx.x; q < op.nop * 9; q += blockDim.x) pis[q] = op.pi[q];
-  for (int q = threadIdx.x; q < op.nop; q += blockDim.x) sgs[q] = op.sgm[q];
-  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
-  const int L = it.tile * TL + lane;
-  const int grp = live ? bv.lane_group[L] : -1;
+  const int grp = live ? bv.tile_group[it.tile] : -1;
   unsigned long long chimask = 0ull;
   int gflags = 0, gfrozen = 0;
   if (grp >= 0) {
@@ -161,93 +178,106 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
     gflags = bv.ginfo[grp].flags;
     gfrozen = bv.ginfo[grp].frozen_sp;
   }
-  if (w == 0)
-    for (int l = 0; l < 9; ++l) dds[lane * 9 + l] = grp >= 0 ? bv.ginfo[grp].dd[l] : 0.0;
+  {
+    const double* dd = grp >= 0 ? bv.ginfo[grp].dd : nullptr;
+    const int nb = op.ntype * ns1 * 81;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+      int lp = q % 9, l = (q / 9) % 9, tk = q / 81;
+      double v = (double)blocks[q];
+      if (FUSE_D && dd) v *= dd[lp];
+      if (FINAL && dd) v *= dd[l];
+      Bs[((size_t)tk * 9 + l) * RW + lp] = (ST)v;
+    }
+    for (int g = threadIdx.x; g < op.nop; g += blockDim.x) {
+      unsigned long long w = 0ull;
+      for (int l = 0; l < 9; ++l) w |= (unsigned long long)op.pi[g * 9 + l] << (4 * l);
+      uint32_t sg = op.sgm[g] ^ (((chimask >> g) & 1ull) ? 0x1FFu : 0u);
+      piw[g] = w | ((unsigned long long)sg << 40);
+    }
+  }
   __syncthreads();
   if (!live) return;
+  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
+  const int L = it.tile * TL + lane;
   double2 dot = make_double2(0.0, 0.0);
   for (int qn = 0; qn < npw; ++qn) {
     int i = it.first + w + WPB * qn;
     if (i >= bv.nn) break;
-    const ST* B = Bs + (size_t)op.typ[i] * ns1 * 81;
+    const ST* B = Bs + (size_t)op.typ[i] * ns1 * 9 * RW;
     T2 acc[9];
     for (int l = 0; l < 9; ++l) { acc[l].x = 0; acc[l].y = 0; }
-    {   // on-site block: own node, t1 = d o (U / sq) (FUSE_D) or t1
-      const ST f = FUSE_D ? (ST)op.isq[i] : (ST)1;
+    {   // on-site block
       const T2* src = in + vix(it.tile, bv.nn, i, 0) + lane;
       T2 v[9];
-      for (int l2 = 0; l2 < 9; ++l2) {
-        T2 x = src[l2 * TL];
-        ST fl = FUSE_D ? f * (ST)dds[lane * 9 + l2] : f;
-        v[l2].x = x.x * fl;
-        v[l2].y = x.y * fl;
-      }
-      for (int l2 = 0; l2 < 9; ++l2)
-        for (int l = 0; l < 9; ++l) {
-          ST bb = B[l * 9 + l2];
-          acc[l].x = fma_(bb, v[l2].x, acc[l].x);
-          acc[l].y = fma_(bb, v[l2].y, acc[l].y);
+      for (int l2 = 0; l2 < 9; ++l2) v[l2] = src[l2 * TL];
+      for (int l = 0; l < 9; ++l) {
+        const ST* row = B + l * RW;
+        for (int lp = 0; lp < 8; lp += 2) {
+          P2 bb = *(const P2*)(row + lp);
+          acc[l].x = fma_(bb.x, v[lp].x, acc[l].x);
+          acc[l].y = fma_(bb.x, v[lp].y, acc[l].y);
+          acc[l].x = fma_(bb.y, v[lp + 1].x, acc[l].x);
+          acc[l].y = fma_(bb.y, v[lp + 1].y, acc[l].y);
         }
+        acc[l].x = fma_(row[8], v[8].x, acc[l].x);
+        acc[l].y = fma_(row[8], v[8].y, acc[l].y);
+      }
     }
     for (int k = 0; k < op.nslot; ++k) {
       int r = op.hopr[k + op.nslot * i];
       if (r < 0) continue;
-      int g = op.hopg[k + op.nslot * i];
-      const uint32_t sgm = sgs[g];
-      const bool neg = (chimask >> g) & 1ull;
-      const ST f = FUSE_D ? (ST)op.isq[r] : (ST)1;
+      const unsigned long long pw = piw[op.hopg[k + op.nslot * i]];
       const T2* src = in + vix(it.tile, bv.nn, r, 0) + lane;
       T2 v[9];
       for (int lp = 0; lp < 9; ++lp) {
-        int p = pis[g * 9 + lp];
-        T2 x = src[p * TL];
-        ST fl = FUSE_D ? f * (ST)dds[lane * 9 + p] : f;
-        if (((sgm >> lp) & 1u) ^ (neg ? 1u : 0u)) fl = -fl;
-        v[lp].x = x.x * fl;
-        v[lp].y = x.y * fl;
+        int p = (int)((pw >> (4 * lp)) & 15ull);
+        v[lp] = flip_if(src[p * TL], (uint32_t)((pw >> (40 + lp)) & 1ull));
       }
-      const ST* Bk = B + (size_t)(k + 1) * 81;
-      for (int l = 0; l < 9; ++l)
-        for (int lp = 0; lp < 9; ++lp) {
-          ST bb = Bk[l * 9 + lp];
-          acc[l].x = fma_(bb, v[lp].x, acc[l].x);
-          acc[l].y = fma_(bb, v[lp].y, acc[l].y);
+      const ST* Bk = B + (size_t)(k + 1) * 9 * RW;
+      for (int l = 0; l < 9; ++l) {
+        const ST* row = Bk + l * RW;
+        for (int lp = 0; lp < 8; lp += 2) {
+          P2 bb = *(const P2*)(row + lp);
+          acc[l].x = fma_(bb.x, v[lp].x, acc[l].x);
+          acc[l].y = fma_(bb.x, v[lp].y, acc[l].y);
+          acc[l].x = fma_(bb.y, v[lp + 1].x, acc[l].x);
+          acc[l].y = fma_(bb.y, v[lp + 1].y, acc[l].y);
         }
+        acc[l].x = fma_(row[8], v[8].x, acc[l].x);
+        acc[l].y = fma_(row[8], v[8].y, acc[l].y);
+      }
     }
     if (!FINAL) {
       for (int l = 0; l < 9; ++l) stv(out + vix(it.tile, bv.nn, i, l) + lane, make_double2(acc[l].x, acc[l].y));
     } else {
-      // y_l = s sq (d_l t2_l + P_l(x0)),  P = c + e + X(z) (src/asr_augblk.f90:219-250), orbital by orbital
+      // y_l = s (d_l t2_l + P_l(U)),  P = c + e + X(z) (src/asr_augblk.f90:219-250), orbital by orbital
       const double* gb = bv.gblob + (size_t)(grp >= 0 ? grp : 0) * bv.GL.stride;
       const double2 z = bv.lane_z[L];
       const double2 s = bv.su[L];
       const bool withx = !(gflags & GF_X_ZERO);
-      const double sqi = op.sq[i], isqi = op.isq[i];
+      const double norb = op.sq[i] * op.sq[i];
       const int fs = (op.start[i] && gfrozen > 0) ? gfrozen : (int)op.frozen[i];
       const int nsm = op.nsmax, kap = op.ncl[i], l0 = op.lst[i], nk = op.nsc[kap];
       for (int l = 0; l < 9; ++l) {
         double2 ui = ld(in + vix(it.tile, bv.nn, i, l) + lane);
-        double2 x0 = cscale(ui, isqi);
         double2 pt;
         if (fs > 0) {
-          pt = cmul(praw(gb, bv.GL, PCEB, withx, z, fs, l), x0);
+          pt = cmul(praw(gb, bv.GL, PCEB, withx, z, fs, l), ui);
         } else {
-          pt = cmul(pweight(gb, bv.GL, PCEB, withx, z, nsm, kap, l0, l0, l), x0);
+          pt = cmul(pweight(gb, bv.GL, PCEB, withx, z, nsm, kap, l0, l0, l), ui);
           for (int k = 0; k < nk; ++k) {
             if (k == l0) continue;
             int r = op.flipr[k + nsm * i];
             if (r < 0) continue;
-            int g = op.flipg[k + nsm * i];
-            bool neg = (chimask >> g) & 1ull;
-            double fr = ((((uint32_t)sgs[g] >> l) & 1u) ^ (neg ? 1u : 0u)) ? -op.isq[r] : op.isq[r];
-            double2 xr = cscale(ld(in + vix(it.tile, bv.nn, r, pis[g * 9 + l]) + lane), fr);
+            const unsigned long long pw = piw[op.flipg[k + nsm * i]];
+            int p = (int)((pw >> (4 * l)) & 15ull);
+            double2 xr = flip_if(ld(in + vix(it.tile, bv.nn, r, p) + lane), (uint32_t)((pw >> (40 + l)) & 1ull));
             pt = cadd(pt, cmul(pweight(gb, bv.GL, PCEB, withx, z, nsm, kap, l0, k, l), xr));
           }
         }
-        double2 h = cscale(make_double2(acc[l].x, acc[l].y), dds[lane * 9 + l]);
-        double2 y = cmul(s, cscale(cadd(h, pt), sqi));
-        stv(out + vix(it.tile, bv.nn, i, l) + lane, y);
-        dot = cadd(dot, cmul(cmul(s, ui), y));
+        double2 y = cmul(s, cadd(make_double2(acc[l].x, acc[l].y), pt));
+        stv_cs(out + vix(it.tile, bv.nn, i, l) + lane, y);
+        dot = cadd(dot, cscale(cmul(cmul(s, ui), y), norb));
       }
     }
   }
@@ -255,10 +285,10 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
 }
 
 // ------------------------------------------------------------------------------------------------ random operators
-// out = R_p(in) (unscaled amplitude coordinates); norm: in is U (normalised coordinates)
+// out = R_p(in), amplitude coordinates, unscaled
 template <typename ST>
 __global__ void __launch_bounds__(WPB * TL) k_rand(OpView op, BatchView bv, int p, const typename St2<ST>::T* __restrict__ in,
-                                                   bool norm, typename St2<ST>::T* __restrict__ out, int npw) {
+                                                   typename St2<ST>::T* __restrict__ out, int npw) {
   NodeIter it;
   int bpt;
   if (!node_iter(bv, npw, it, bpt)) return;
@@ -272,18 +302,18 @@ __global__ void __launch_bounds__(WPB * TL) k_rand(OpView op, BatchView bv, int 
     int i = it.first + w + WPB * qn;
     if (i >= bv.nn) break;
     double2 xi[9], o[9];
-    double f = norm ? op.isq[i] : 1.0;
-    for (int l = 0; l < 9; ++l) xi[l] = cscale(ld(in + vix(it.tile, bv.nn, i, l) + lane), f);
-    rand_term(op, gi, gb, bv.GL, p, false, make_double2(0, 0), in, it.tile, i, lane, norm, o, xi);
+    for (int l = 0; l < 9; ++l) xi[l] = ld(in + vix(it.tile, bv.nn, i, l) + lane);
+    rand_term(op, gi, gb, bv.GL, p, false, make_double2(0, 0), in, it.tile, i, lane, o, xi);
     for (int l = 0; l < 9; ++l) stv(out + vix(it.tile, bv.nn, i, l) + lane, o[l]);
   }
 }
 
-// out = sgnAB (A + B) + C + H, A = D t2 (uniform: d o t2), B = R_pB(v1), C = R_(e+pb) + z pa on x0 (optional),
-// H = h1 (optional).  final: y = s sq out, partial dot U . y; else out is written unscaled (amplitude coordinates).
+// out = sgnAB (A + B) + C + H, A = D t2 (uniform: d o t2), B = R_pB(v1) (+ z pa if bx), C = R_(e+pb) + z pa on U
+// (optional), H = h1 (optional), amplitude coordinates.  final: y = s out and the partial dot sum norb (s U) . y; else
+// out is written unscaled.
 template <typename ST>
 __global__ void __launch_bounds__(WPB * TL) k_combine(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ t2,
-                                                      const typename St2<ST>::T* __restrict__ v1, bool v1norm, int pB, bool bx,
+                                                      const typename St2<ST>::T* __restrict__ v1, int pB, bool bx,
                                                       const typename St2<ST>::T* __restrict__ u, bool cterm,
                                                       const typename St2<ST>::T* __restrict__ h1, double sgnAB, bool final_,
                                                       typename St2<ST>::T* __restrict__ out, double2* part, int npw) {
@@ -307,31 +337,29 @@ __global__ void __launch_bounds__(WPB * TL) k_combine(OpView op, BatchView bv, c
         if (t2) {
           for (int l = 0; l < 9; ++l) xi[l] = ld(t2 + vix(it.tile, bv.nn, i, l) + lane);
           if (gi.flags & GF_D_UNIFORM) for (int l = 0; l < 9; ++l) acc[l] = cscale(xi[l], gi.dd[l]);
-          else rand_term(op, gi, gb, bv.GL, PD, false, z, t2, it.tile, i, lane, false, acc, xi);
+          else rand_term(op, gi, gb, bv.GL, PD, false, z, t2, it.tile, i, lane, acc, xi);
         } else {
           for (int l = 0; l < 9; ++l) acc[l] = make_double2(0, 0);
         }
         if (v1) {
-          double f = v1norm ? op.isq[i] : 1.0;
-          for (int l = 0; l < 9; ++l) xi[l] = cscale(ld(v1 + vix(it.tile, bv.nn, i, l) + lane), f);
-          rand_term(op, gi, gb, bv.GL, pB, bx, z, v1, it.tile, i, lane, v1norm, tmp, xi);
+          for (int l = 0; l < 9; ++l) xi[l] = ld(v1 + vix(it.tile, bv.nn, i, l) + lane);
+          rand_term(op, gi, gb, bv.GL, pB, bx, z, v1, it.tile, i, lane, tmp, xi);
           for (int l = 0; l < 9; ++l) acc[l] = cadd(acc[l], tmp[l]);
         }
         for (int l = 0; l < 9; ++l) acc[l] = cscale(acc[l], sgnAB);
         double2 ui[9];
         for (int l = 0; l < 9; ++l) ui[l] = ld(u + vix(it.tile, bv.nn, i, l) + lane);
         if (cterm) {
-          for (int l = 0; l < 9; ++l) xi[l] = cscale(ui[l], op.isq[i]);
-          rand_term(op, gi, gb, bv.GL, PEB, !(gi.flags & GF_X_ZERO), z, u, it.tile, i, lane, true, tmp, xi);
+          rand_term(op, gi, gb, bv.GL, PEB, !(gi.flags & GF_X_ZERO), z, u, it.tile, i, lane, tmp, ui);
           for (int l = 0; l < 9; ++l) acc[l] = cadd(acc[l], tmp[l]);
         }
         if (h1) for (int l = 0; l < 9; ++l) acc[l] = cadd(acc[l], ld(h1 + vix(it.tile, bv.nn, i, l) + lane));
         if (final_) {
-          double sqi = op.sq[i];
+          const double norb = op.sq[i] * op.sq[i];
           for (int l = 0; l < 9; ++l) {
-            double2 y = cmul(s, cscale(acc[l], sqi));
+            double2 y = cmul(s, acc[l]);
             stv(out + vix(it.tile, bv.nn, i, l) + lane, y);
-            dot = cadd(dot, cmul(cmul(s, ui[l]), y));
+            dot = cadd(dot, cscale(cmul(cmul(s, ui[l]), y), norb));
           }
         } else {
           for (int l = 0; l < 9; ++l) stv(out + vix(it.tile, bv.nn, i, l) + lane, acc[l]);
@@ -344,7 +372,8 @@ __global__ void __launch_bounds__(WPB * TL) k_combine(OpView op, BatchView bv, c
 
 // ------------------------------------------------------------------------------------------------ Lanczos update
 // w = y - a u - b up (u = su U, up = sup UP); projection onto the symmetric subspace (augcls_project_c,
-// src/asr_augcls.f90:329-348); lanes that left the chain are zeroed.  w overwrites y; partial dot w . w.
+// src/asr_augcls.f90:329-348; node-local, the same in amplitude coordinates); lanes that left the chain are zeroed.
+// w overwrites y; partial dot sum norb w . w.
 __device__ __forceinline__ void project_node(const OpView& op, int i, unsigned long long chimask, double2* x) {
   int s0 = op.stab_ptr[i], s1 = op.stab_ptr[i + 1];
   int ns = s1 - s0;
@@ -386,10 +415,12 @@ __global__ void __launch_bounds__(WPB * TL) k_lanczos_w(OpView op, BatchView bv,
     if (act) {
       for (int l = 0; l < 9; ++l) {
         size_t q = vix(it.tile, bv.nn, i, l) + lane;
-        x[l] = csub(csub(ld(y + q), cmul(as, ld(u + q))), cmul(bs, ld(up + q)));
+        x[l] = csub(csub(ld_cs(y + q), cmul(as, ld(u + q))), cmul(bs, ld_cs(up + q)));
       }
       if (bv.project) project_node(op, i, chim, x);
-      for (int l = 0; l < 9; ++l) dot = cadd(dot, cmul(x[l], x[l]));
+      double2 dn = make_double2(0, 0);
+      for (int l = 0; l < 9; ++l) dn = cadd(dn, cmul(x[l], x[l]));
+      dot = cadd(dot, cscale(dn, op.sq[i] * op.sq[i]));
     } else {
       for (int l = 0; l < 9; ++l) x[l] = make_double2(0, 0);
     }
@@ -546,11 +577,9 @@ struct Dev {
 };
 
 size_t smul_smem(const asr_op* op, size_t st_size) {
-  size_t b = (size_t)op->ntype * (op->nslot + 1) * 81 * st_size;
-  b += (op->nop * 9 + 1) & ~1;
-  b += op->nop * sizeof(uint16_t);
+  size_t b = (size_t)op->ntype * (op->nslot + 1) * 9 * RW * st_size;
   b = (b + 15) & ~(size_t)15;
-  b += TL * 9 * sizeof(double) + 16;
+  b += (size_t)op->nop * sizeof(unsigned long long);
   return b;
 }
 
@@ -572,19 +601,19 @@ int step_apply(asr_ctx* ctx, asr_op* op, const BatchView& bv, bool fused, bool a
   if (all_dunif) {
     k_smul<ST, true, false><<<grid, B, sm, s>>>(ov, bv, blk, U, T2, part, npw);
   } else {
-    k_rand<ST><<<grid, B, 0, s>>>(ov, bv, PD, U, true, T1, npw);
+    k_rand<ST><<<grid, B, 0, s>>>(ov, bv, PD, U, T1, npw);
     k_smul<ST, false, false><<<grid, B, sm, s>>>(ov, bv, blk, T1, T2, part, npw);
   }
-  if (!any_o) {   // y = s sq (D t2 + (c + e + X) x0)
-    k_combine<ST><<<grid, B, 0, s>>>(ov, bv, T2, U, true, PCEB, true, U, false, nullptr, 1.0, true, Y, part, npw);
+  if (!any_o) {   // y = s (D t2 + (c + e + X) U)
+    k_combine<ST><<<grid, B, 0, s>>>(ov, bv, T2, U, PCEB, true, U, false, nullptr, 1.0, true, Y, part, npw);
     return ASR_OK;
   }
-  // h1 = D t2 + C x0;  r1 = O h1;  h2 = D S D r1 + C r1;  y = s sq (h1 - h2 + (e + X) x0)
-  k_combine<ST><<<grid, B, 0, s>>>(ov, bv, T2, U, true, PC, false, U, false, nullptr, 1.0, false, H1, part, npw);
-  k_rand<ST><<<grid, B, 0, s>>>(ov, bv, PO, H1, false, R1, npw);
-  k_rand<ST><<<grid, B, 0, s>>>(ov, bv, PD, R1, false, T1, npw);   // t1 = D r1 (r1 is in amplitude coordinates)
+  // h1 = D t2 + C U;  r1 = O h1;  h2 = D S D r1 + C r1;  y = s (h1 - h2 + (e + X) U)
+  k_combine<ST><<<grid, B, 0, s>>>(ov, bv, T2, U, PC, false, U, false, nullptr, 1.0, false, H1, part, npw);
+  k_rand<ST><<<grid, B, 0, s>>>(ov, bv, PO, H1, R1, npw);
+  k_rand<ST><<<grid, B, 0, s>>>(ov, bv, PD, R1, T1, npw);
   k_smul<ST, false, false><<<grid, B, sm, s>>>(ov, bv, blk, T1, T2, part, npw);
-  k_combine<ST><<<grid, B, 0, s>>>(ov, bv, T2, R1, false, PC, false, U, true, H1, -1.0, true, Y, part, npw);
+  k_combine<ST><<<grid, B, 0, s>>>(ov, bv, T2, R1, PC, false, U, true, H1, -1.0, true, Y, part, npw);
   return ASR_OK;
 }
 
@@ -596,7 +625,16 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   typedef typename St2<ST>::T T2;
   cudaStream_t s = ctx->stream;
   const int nn = op->nn;
-  const int ntile_all = (nlane + TL - 1) / TL;
+  // tiles: the lanes of one group in chunks of 32 (a tile never holds two groups)
+  std::vector<std::vector<int>> tiles;
+  {
+    std::vector<std::vector<int>> per_group(ginfo.size());
+    for (int L = 0; L < nlane; ++L) per_group[lane_group[L]].push_back(L);
+    for (auto& lst : per_group)
+      for (size_t q = 0; q < lst.size(); q += TL)
+        tiles.emplace_back(lst.begin() + q, lst.begin() + std::min(lst.size(), q + (size_t)TL));
+  }
+  const int ntile_all = (int)tiles.size();
   int nlevmax = 0;
   bool any_o = false, all_dunif = true, fused = true;
   for (auto& g : ginfo) {
@@ -612,10 +650,14 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   const int nvec = 3 + (fused ? 0 : (any_o ? 4 : 2));
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
-  int tpb = opt.tiles_per_batch > 0 ? opt.tiles_per_batch : 8;
+  // 32-lane tiles per batch: larger batches amortise the per-level reductions and launch gaps (measured on the fcc
+  // ternary workload: FP64 best at 16 tiles, FP32 at 8 with 4 nodes per warp)
+  int tpb = opt.tiles_per_batch > 0 ? opt.tiles_per_batch : (std::is_same<ST, double>::value ? 16 : 8);
+  if (const char* e = getenv("ASR_TILES_PER_BATCH")) tpb = std::max(1, atoi(e));
   while (tpb > 1 && (size_t)tpb * nvec * vec_bytes > freeb / 2) tpb /= 2;
   tpb = std::min(tpb, ntile_all);
-  const int npw = std::max(1, opt.nodes_per_warp);
+  int npw = std::max(1, opt.nodes_per_warp);
+  if (const char* e = getenv("ASR_NODES_PER_WARP")) npw = std::max(1, atoi(e));
   const int npb = WPB * npw;
   const int bpt = (nn + npb - 1) / npb;
   // device state
@@ -626,10 +668,10 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   ASR_CUDA(cudaMemcpyAsync(d_gblob.p, gblob.data(), gblob.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   ASR_CUDA(cudaMemcpyAsync(d_ginfo.p, ginfo.data(), ginfo.size() * sizeof(GroupInfo), cudaMemcpyHostToDevice, s));
   const int nlp = tpb * TL;
-  Dev<int> d_lgroup, d_act, d_wact, d_m, d_tact, d_nfall;
+  Dev<int> d_lgroup, d_act, d_wact, d_m, d_tact, d_nfall, d_tgroup;
   Dev<double2> d_a, d_b, d_gprev, d_acur, d_bprev, d_su, d_sup, d_part, d_z;
   ASR_TRY(d_lgroup.alloc(nlp)); ASR_TRY(d_act.alloc(nlp)); ASR_TRY(d_wact.alloc(nlp)); ASR_TRY(d_m.alloc(nlp));
-  ASR_TRY(d_tact.alloc(tpb)); ASR_TRY(d_nfall.alloc(1));
+  ASR_TRY(d_tact.alloc(tpb)); ASR_TRY(d_nfall.alloc(1)); ASR_TRY(d_tgroup.alloc(tpb));
   ASR_TRY(d_a.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_b.alloc((size_t)nlp * NLMAX));
   ASR_TRY(d_gprev.alloc(nlp)); ASR_TRY(d_acur.alloc(nlp)); ASR_TRY(d_bprev.alloc(nlp)); ASR_TRY(d_su.alloc(nlp));
   ASR_TRY(d_sup.alloc(nlp)); ASR_TRY(d_part.alloc((size_t)tpb * bpt * TL)); ASR_TRY(d_z.alloc(nlp));
@@ -644,24 +686,28 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   ASR_TRY(d_lmap.alloc(nlp));
   ASR_TRY(d_m_all.alloc(nlane));
   ASR_CUDA(cudaMemsetAsync(d_m_all.p, 0, nlane * sizeof(int), s));
-  // tiles of 32 consecutive lanes, deepest first, so that every batch runs to one depth
+  // deepest tiles first, so that every batch runs to one depth
   std::vector<int> tdepth(ntile_all, 0), order(ntile_all);
-  for (int L = 0; L < nlane; ++L) tdepth[L / TL] = std::max(tdepth[L / TL], ginfo[lane_group[L]].nlev);
+  for (int t = 0; t < ntile_all; ++t) tdepth[t] = ginfo[lane_group[tiles[t][0]]].nlev;
   for (int t = 0; t < ntile_all; ++t) order[t] = t;
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return tdepth[x] > tdepth[y]; });
   std::vector<double2> one(nlp, make_double2(1.0, 0.0));
   for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
     const int nt = std::min(tpb, ntile_all - t0);
     int kmax = 0;
-    std::vector<int> tact(tpb, 0), ones(nlp, 0);
+    std::vector<int> tact(tpb, 0), ones(nlp, 0), tgroup(tpb, -1);
     for (int q = 0; q < nlp; ++q) {
       int bt = q / TL;
-      int L = bt < nt ? order[t0 + bt] * TL + q % TL : -1;
-      if (L >= nlane) L = -1;
+      int L = -1;
+      if (bt < nt) {
+        const std::vector<int>& tl = tiles[order[t0 + bt]];
+        if (q % TL < (int)tl.size()) L = tl[q % TL];
+      }
       lmap[q] = L;
       hgroup[q] = L >= 0 ? lane_group[L] : -1;
-      if (hgroup[q] >= 0) { kmax = std::max(kmax, ginfo[hgroup[q]].nlev); tact[bt] = 1; ones[q] = 1; }
+      if (hgroup[q] >= 0) { kmax = std::max(kmax, ginfo[hgroup[q]].nlev); tact[bt] = 1; ones[q] = 1; tgroup[bt] = hgroup[q]; }
     }
+    ASR_CUDA(cudaMemcpyAsync(d_tgroup.p, tgroup.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemcpyAsync(d_lgroup.p, hgroup.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemcpyAsync(d_lmap.p, lmap.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemcpyAsync(d_act.p, ones.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -676,8 +722,8 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
     ASR_CUDA(cudaMemcpyAsync(d_su.p, one.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
     k_gather_z<<<(nlp + 127) / 128, 128, 0, s>>>(nlp, d_lmap.p, d_lane_z, d_z.p);
     BatchView bv{nt, nn, op->nsmax, 0, opt.mode, opt.project, opt.tail, NLMAX, opt.depth_tol, d_gblob.p, GL, d_ginfo.p,
-                 d_lgroup.p, d_z.p, d_act.p, d_wact.p, d_m.p, d_a.p, d_b.p, d_gprev.p, d_acur.p, d_bprev.p, d_su.p, d_sup.p,
-                 d_tact.p, d_nfall.p};
+                 d_lgroup.p, d_tgroup.p, d_z.p, d_act.p, d_wact.p, d_m.p, d_a.p, d_b.p, d_gprev.p, d_acur.p, d_bprev.p, d_su.p,
+                 d_sup.p, d_tact.p, d_nfall.p};
     k_init<ST><<<std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256), 256, 0, s>>>(bv, V[1].p, V[0].p);
     ctx->launches += 2;
     const int gridb = nt * bpt;
@@ -743,22 +789,577 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   return ASR_OK;
 }
 
+// ================================================================================================ adjoint
+// Reverse mode through the chain (the derivative of the computed G, not of the exact resolvent), for the edc route
+// with o = 0 and a fixed depth.  Forward: u_1 = e, y_k = A u_k, a_k = u_k . y_k, w_k = y_k - a_k u_k - b_{k-1} u_{k-1},
+// w'_k = P w_k, b_k = sqrt(w'_k . w'_k), u_{k+1} = w'_k / b_k; G = cf(a, b).  With the bilinear form of the normalised
+// coordinates (amplitude coordinates weighted by the orbit size) A and P are symmetric on the symmetric subspace, and
+// every quantity is holomorphic in the parameters, so the adjoint recursion for the seeds abar_k, bbar_k is
+//   bbar_k -= (ubar_{k+1} . u_{k+1}) / b_k;  wbar = P (ubar_{k+1} / b_k + bbar_k u_{k+1})
+//   abar_k -= wbar . u_k;  bbar_{k-1} -= wbar . u_{k-1};  ybar = wbar + abar_k u_k
+//   ubar_k += A ybar + abar_k y_k - a_k wbar;  ubar_{k-1} -= b_{k-1} wbar;  theta_bar += ybar . (dA/dtheta) u_k.
+// For A = R_d S R_d + R_P (amplitude coordinates), ybar . dA u = ybar . dR_P u + ybar . dR_d (S R_d u) + (S R_d ybar) . dR_d u,
+// and dR_p / dpar(l, s) is the random operator with the weights mt(own, k', s, class) (local_weights,
+// src/asr_augcls.f90:362-377).  The Lanczos vectors are recomputed per segment from checkpoints every `stride` levels.
+
+constexpr int MAXSP = 8;        // species held in registers by the gradient kernel
+constexpr int GPW = 9;          // warps per gradient block: one per orbital
+
+// per-lane weighted dot: part = sum_i norb_i a_i . b_i (raw, unscaled vectors)
+template <typename ST>
+__global__ void __launch_bounds__(WPB * TL) k_dot(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ a,
+                                                  const typename St2<ST>::T* __restrict__ b, double2* part, int npw) {
+  NodeIter it;
+  int bpt;
+  if (!node_iter(bv, npw, it, bpt)) return;
+  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
+  double2 dot = make_double2(0, 0);
+  for (int qn = 0; qn < npw; ++qn) {
+    int i = it.first + w + WPB * qn;
+    if (i >= bv.nn) break;
+    double2 dn = make_double2(0, 0);
+    for (int l = 0; l < 9; ++l) {
+      size_t q = vix(it.tile, bv.nn, i, l) + lane;
+      dn = cadd(dn, cmul(ld(a + q), ld(b + q)));
+    }
+    dot = cadd(dot, cscale(dn, op.sq[i] * op.sq[i]));
+  }
+  block_reduce_store(dot, part, it.tile, bpt);
+}
+
+// wbar = P (c1 ubar_next + c2 X_next); partial dots wbar . X_k and wbar . X_{k-1}
+template <typename ST>
+__global__ void __launch_bounds__(WPB * TL) k_adj_w(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ ubn,
+                                                    const typename St2<ST>::T* __restrict__ xn, const typename St2<ST>::T* __restrict__ xk,
+                                                    const typename St2<ST>::T* __restrict__ xkm, const double2* c1, const double2* c2,
+                                                    typename St2<ST>::T* __restrict__ wb, double2* part1, double2* part2, int npw) {
+  NodeIter it;
+  int bpt;
+  if (!node_iter(bv, npw, it, bpt)) return;
+  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
+  const int L = it.tile * TL + lane;
+  const int grp = bv.lane_group[L];
+  const unsigned long long chim = grp >= 0 ? bv.ginfo[grp].chimask : 0ull;
+  const double2 a1 = c1[L], a2 = c2[L];
+  double2 d1 = make_double2(0, 0), d2 = make_double2(0, 0);
+  for (int qn = 0; qn < npw; ++qn) {
+    int i = it.first + w + WPB * qn;
+    if (i >= bv.nn) break;
+    double2 x[9];
+    for (int l = 0; l < 9; ++l) {
+      size_t q = vix(it.tile, bv.nn, i, l) + lane;
+      x[l] = cadd(cmul(a1, ld(ubn + q)), cmul(a2, ld(xn + q)));
+    }
+    if (bv.project) project_node(op, i, chim, x);
+    double2 e1 = make_double2(0, 0), e2 = make_double2(0, 0);
+    for (int l = 0; l < 9; ++l) {
+      size_t q = vix(it.tile, bv.nn, i, l) + lane;
+      stv(wb + q, x[l]);
+      e1 = cadd(e1, cmul(x[l], ld(xk + q)));
+      e2 = cadd(e2, cmul(x[l], ld(xkm + q)));
+    }
+    double nb = op.sq[i] * op.sq[i];
+    d1 = cadd(d1, cscale(e1, nb));
+    d2 = cadd(d2, cscale(e2, nb));
+  }
+  block_reduce_store(d1, part1, it.tile, bpt);
+  __syncthreads();
+  block_reduce_store(d2, part2, it.tile, bpt);
+}
+
+// ybar = wbar + c3 X_k;  ubar_{k-1} -= c4 wbar
+template <typename ST>
+__global__ void __launch_bounds__(WPB * TL) k_adj_y(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ wb,
+                                                    const typename St2<ST>::T* __restrict__ xk, const double2* c3, const double2* c4,
+                                                    typename St2<ST>::T* __restrict__ yb, typename St2<ST>::T* __restrict__ ubp, int npw) {
+  NodeIter it;
+  int bpt;
+  if (!node_iter(bv, npw, it, bpt)) return;
+  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
+  const int L = it.tile * TL + lane;
+  const double2 a3 = c3[L], a4 = c4[L];
+  for (int qn = 0; qn < npw; ++qn) {
+    int i = it.first + w + WPB * qn;
+    if (i >= bv.nn) break;
+    for (int l = 0; l < 9; ++l) {
+      size_t q = vix(it.tile, bv.nn, i, l) + lane;
+      double2 wv = ld(wb + q);
+      stv(yb + q, cadd(wv, cmul(a3, ld(xk + q))));
+      if (ubp) stv(ubp + q, csub(ld(ubp + q), cmul(a4, wv)));
+    }
+  }
+}
+
+// ubar_k += AY + c5 Y_k - c6 wbar
+template <typename ST>
+__global__ void __launch_bounds__(WPB * TL) k_adj_u(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ ay,
+                                                    const typename St2<ST>::T* __restrict__ yk, const typename St2<ST>::T* __restrict__ wb,
+                                                    const double2* c5, const double2* c6, typename St2<ST>::T* __restrict__ ubk, int npw) {
+  NodeIter it;
+  int bpt;
+  if (!node_iter(bv, npw, it, bpt)) return;
+  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
+  const int L = it.tile * TL + lane;
+  const double2 a5 = c5[L], a6 = c6[L];
+  for (int qn = 0; qn < npw; ++qn) {
+    int i = it.first + w + WPB * qn;
+    if (i >= bv.nn) break;
+    for (int l = 0; l < 9; ++l) {
+      size_t q = vix(it.tile, bv.nn, i, l) + lane;
+      double2 v = cadd(ld(ubk + q), ld(ay + q));
+      v = cadd(v, cmul(a5, ld(yk + q)));
+      v = csub(v, cmul(a6, ld(wb + q)));
+      stv(ubk + q, v);
+    }
+  }
+}
+
+// gradient partials of one reverse step: thread (orbital l = warp, lane); per block and kind (c-like, d, pa) the sums
+// over its nodes and the 32 lanes: gpart[((tile * gbpt + blk) * 3 + kind) * 9 * nsp + l * nsp + species]
+template <typename ST>
+__global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, const double* mt, const int* spc, int ldspc,
+                                                       const typename St2<ST>::T* __restrict__ yb,
+                                                       const typename St2<ST>::T* __restrict__ t2b,
+                                                       const typename St2<ST>::T* __restrict__ xk,
+                                                       const typename St2<ST>::T* __restrict__ t2k, const double2* sk, int nodes_per_block,
+                                                       double2* gpart) {
+  const int gbpt = (bv.nn + nodes_per_block - 1) / nodes_per_block;
+  const int tile = blockIdx.x / gbpt, blk = blockIdx.x % gbpt;
+  if (tile >= bv.ntile || !bv.tile_act[tile]) return;
+  const int l = threadIdx.x / TL, lane = threadIdx.x % TL;
+  const int L = tile * TL + lane;
+  const int grp = bv.tile_group[tile];
+  const int nsp = op.nsp, nsm = op.nsmax;
+  double2 g1[MAXSP], gd[MAXSP], gpa[MAXSP];
+  for (int q = 0; q < MAXSP; ++q) { g1[q] = make_double2(0, 0); gd[q] = g1[q]; gpa[q] = g1[q]; }
+  const bool live = bv.lane_group[L] >= 0 && grp >= 0;
+  if (live) {
+    const GroupInfo gi = bv.ginfo[grp];
+    const double2 s = sk[L], z = bv.lane_z[L];
+    const int i0 = blk * nodes_per_block, i1 = min(bv.nn, i0 + nodes_per_block);
+    for (int i = i0; i < i1; ++i) {
+      size_t q = vix(tile, bv.nn, i, l) + lane;
+      double2 ybv = ld(yb + q), tbv = ld(t2b + q);
+      double2 x = cmul(s, ld(xk + q)), t = cmul(s, ld(t2k + q));
+      double nb = op.sq[i] * op.sq[i];
+      int fs = frozen_of(op, gi, i);
+      if (fs > 0) {
+        double2 q1 = cscale(cmul(ybv, x), nb);
+        g1[fs - 1] = cadd(g1[fs - 1], q1);
+        gd[fs - 1] = cadd(gd[fs - 1], cscale(cadd(cmul(ybv, t), cmul(tbv, x)), nb));
+        gpa[fs - 1] = cadd(gpa[fs - 1], cmul(z, q1));
+        continue;
+      }
+      int kap = op.ncl[i], own = op.lst[i], nk = op.nsc[kap];
+      for (int kp = 0; kp < nk; ++kp) {
+        double2 lx, lt;
+        if (kp == own) { lx = x; lt = t; }
+        else {
+          int r = op.flipr[kp + nsm * i];
+          if (r < 0) continue;
+          int g = op.flipg[kp + nsm * i];
+          bool neg = (gi.chimask >> g) & 1ull;
+          double sgn = ((((uint32_t)op.sgm[g] >> l) & 1u) ^ (neg ? 1u : 0u)) ? -1.0 : 1.0;
+          size_t qr = vix(tile, bv.nn, r, op.pi[g * 9 + l]) + lane;
+          lx = cscale(cmul(s, ld(xk + qr)), sgn);
+          lt = cscale(cmul(s, ld(t2k + qr)), sgn);
+        }
+        double2 q1 = cscale(cmul(ybv, lx), nb);
+        double2 qd = cscale(cadd(cmul(ybv, lt), cmul(tbv, lx)), nb);
+        for (int sidx = 0; sidx < nk; ++sidx) {
+          double m = mt[own + nsm * (kp + nsm * (sidx + (size_t)nsm * kap))];
+          if (m == 0.0) continue;
+          int sp = spc[sidx + ldspc * kap] - 1;
+          g1[sp] = cadd(g1[sp], cscale(q1, m));
+          gd[sp] = cadd(gd[sp], cscale(qd, m));
+          gpa[sp] = cadd(gpa[sp], cmul(z, cscale(q1, m)));
+        }
+      }
+    }
+  }
+  // sum over the 32 lanes (one warp = one orbital), fixed order
+  for (int q = 0; q < nsp; ++q) {
+    for (int off = 16; off > 0; off >>= 1) {
+      g1[q].x += __shfl_xor_sync(0xffffffffu, g1[q].x, off);
+      g1[q].y += __shfl_xor_sync(0xffffffffu, g1[q].y, off);
+      gd[q].x += __shfl_xor_sync(0xffffffffu, gd[q].x, off);
+      gd[q].y += __shfl_xor_sync(0xffffffffu, gd[q].y, off);
+      gpa[q].x += __shfl_xor_sync(0xffffffffu, gpa[q].x, off);
+      gpa[q].y += __shfl_xor_sync(0xffffffffu, gpa[q].y, off);
+    }
+  }
+  if (lane == 0) {
+    double2* out = gpart + ((size_t)(tile * gbpt + blk) * 3) * 9 * nsp;
+    for (int q = 0; q < nsp; ++q) {
+      out[(0 * 9 + l) * nsp + q] = g1[q];
+      out[(1 * 9 + l) * nsp + q] = gd[q];
+      out[(2 * 9 + l) * nsp + q] = gpa[q];
+    }
+  }
+}
+
+// gacc[tile][3][9][nsp] += sum over the blocks of the step's partials (fixed order)
+__global__ void k_adj_gsum(int ntile, int gbpt, int ng, const int* tile_act, const double2* gpart, double2* gacc) {
+  int tile = blockIdx.x;
+  if (tile >= ntile || !tile_act[tile]) return;
+  for (int e = threadIdx.x; e < ng; e += blockDim.x) {
+    double2 sum = make_double2(0, 0);
+    for (int b = 0; b < gbpt; ++b) sum = cadd(sum, gpart[(size_t)(tile * gbpt + b) * ng + e]);
+    gacc[(size_t)tile * ng + e] = cadd(gacc[(size_t)tile * ng + e], sum);
+  }
+}
+
+// per-lane sum of partials: out[L] = sum_q part[(tile * bpt + q) * TL + lane]
+__global__ void k_lane_sum(int ntile, int bpt, const int* tile_act, const double2* part, double2* out) {
+  int tile = blockIdx.x, lane = threadIdx.x;
+  if (tile >= ntile) return;
+  double2 sum = make_double2(0, 0);
+  if (tile_act[tile])
+    for (int q = 0; q < bpt; ++q) sum = cadd(sum, part[((size_t)tile * bpt + q) * TL + lane]);
+  out[tile * TL + lane] = sum;
+}
+
+// scalars of reverse step k for every lane (state arrays indexed [lane][NLMAX], k 1-based):
+//   phase 0: coefficients of wbar from d1 = ubar_{k+1} . X_{k+1} (raw)
+//   phase 1: abar', bbar_{k-1} update from d2 = wbar . X_k, d3 = wbar . X_{k-1} (raw)
+struct AdjScal {
+  const double2* a;       // forward a_k
+  const double2* b;       // forward b_k
+  const int* m;           // depth per lane
+  double2* abar;
+  double2* bbar;
+  double2 *s_next, *s_k, *s_prev;   // scales of X_{k+1}, X_k, X_{k-1}
+  double2 *c1, *c2, *c3, *c4, *c5, *c6;
+  const double2 *d1, *d2, *d3;
+};
+__device__ __forceinline__ double2 scale_of(const AdjScal& S, int L, int k) {   // s_k: u_k = s_k X_k
+  if (k <= 1) return make_double2(k == 1 ? 1.0 : 0.0, 0.0);
+  double2 b = S.b[(size_t)L * NLMAX + k - 2];
+  if (cabs2(b) == 0.0 || k > S.m[L]) return make_double2(0, 0);
+  return cdiv(make_double2(1.0, 0.0), b);
+}
+__global__ void k_adj_scal(AdjScal S, int nlane, const int* lane_group, int k, int phase) {
+  int L = blockIdx.x * blockDim.x + threadIdx.x;
+  if (L >= nlane) return;
+  const double2 zero = make_double2(0, 0);
+  if (lane_group[L] < 0 || k > S.m[L]) {
+    if (phase == 0) { S.c1[L] = zero; S.c2[L] = zero; S.s_next[L] = zero; S.s_k[L] = zero; S.s_prev[L] = zero; }
+    else { S.c3[L] = zero; S.c4[L] = zero; S.c5[L] = zero; S.c6[L] = zero; }
+    return;
+  }
+  const size_t o = (size_t)L * NLMAX;
+  if (phase == 0) {
+    double2 sn = k < S.m[L] ? scale_of(S, L, k + 1) : zero;
+    S.s_next[L] = sn;
+    S.s_k[L] = scale_of(S, L, k);
+    S.s_prev[L] = scale_of(S, L, k - 1);
+    if (k < S.m[L]) {
+      double2 bk = S.b[o + k - 1];
+      double2 ib = cdiv(make_double2(1.0, 0.0), bk);
+      double2 d1 = cmul(sn, S.d1[L]);                           // ubar_{k+1} . u_{k+1}
+      double2 bb = csub(S.bbar[o + k - 1], cmul(d1, ib));
+      S.bbar[o + k - 1] = bb;
+      S.c1[L] = ib;                                              // wbar' = ubar_{k+1} / b_k + bbar_k u_{k+1}
+      S.c2[L] = cmul(bb, sn);
+    } else {
+      S.c1[L] = zero;
+      S.c2[L] = zero;
+    }
+  } else {
+    double2 sk = S.s_k[L], sp = S.s_prev[L];
+    double2 ab = csub(S.abar[o + k - 1], cmul(sk, S.d2[L]));   // abar_k -= wbar . u_k
+    S.abar[o + k - 1] = ab;
+    if (k > 1) S.bbar[o + k - 2] = csub(S.bbar[o + k - 2], cmul(sp, S.d3[L]));   // bbar_{k-1} -= wbar . u_{k-1}
+    S.c3[L] = cmul(ab, sk);                                      // ybar = wbar + abar u_k
+    S.c4[L] = k > 1 ? S.b[o + k - 2] : zero;                     // ubar_{k-1} -= b_{k-1} wbar
+    S.c5[L] = ab;                                                // ubar_k += A ybar + abar y_k - a_k wbar
+    S.c6[L] = S.a[o + k - 1];
+  }
+}
+
+// forward recompute of one level: acur = a_k, bprev = b_{k-1}, su = s_k, sup = s_{k-1}, wact = k < m
+__global__ void k_set_fwd(BatchView bv, AdjScal S, int nlane, int k) {
+  int L = blockIdx.x * blockDim.x + threadIdx.x;
+  if (L >= nlane) return;
+  const size_t o = (size_t)L * NLMAX;
+  bool live = bv.lane_group[L] >= 0 && k <= S.m[L];
+  bv.acur[L] = live ? S.a[o + k - 1] : make_double2(0, 0);
+  bv.bprev[L] = (live && k > 1) ? S.b[o + k - 2] : make_double2(0, 0);
+  bv.su[L] = live ? scale_of(S, L, k) : make_double2(0, 0);
+  bv.sup[L] = live ? scale_of(S, L, k - 1) : make_double2(0, 0);
+  bv.lane_wact[L] = (live && k < S.m[L]) ? 1 : 0;
+}
+
+// t2 = S R_d x (unscaled), general or with d folded into the blocks
+template <typename ST>
+void apply_SD(asr_op* op, const BatchView& bv, bool dunif, const typename St2<ST>::T* x, typename St2<ST>::T* tmp,
+              typename St2<ST>::T* t2, double2* part, int npw, int grid, cudaStream_t s) {
+  OpView ov = op->view();
+  const ST* blk = std::is_same<ST, double>::value ? (const ST*)op->d_blocks : (const ST*)op->d_blocks_f;
+  size_t sm = smul_smem(op, sizeof(ST));
+  if (dunif) {
+    k_smul<ST, true, false><<<grid, WPB * TL, sm, s>>>(ov, bv, blk, x, t2, part, npw);
+  } else {
+    k_rand<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, PD, x, tmp, npw);
+    k_smul<ST, false, false><<<grid, WPB * TL, sm, s>>>(ov, bv, blk, tmp, t2, part, npw);
+  }
+}
+
+template <typename ST>
+int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+                  const GroupLayout& GL, const std::vector<int>& lane_group, const std::vector<double2>& lane_z,
+                  const std::vector<double2>& lane_w, int tail, int project, int stride, std::vector<double2>& g_out,
+                  std::vector<double2>& grad_out /* [group][3][9][nsp] */) {
+  typedef typename St2<ST>::T T2;
+  cudaStream_t s = ctx->stream;
+  const int nn = op->nn, nsp = op->nsp, nlane = (int)lane_group.size();
+  if (nsp > MAXSP) { set_error("adjoint: at most %d species", MAXSP); return ASR_EINVAL; }
+  bool dunif = true;
+  int mmax = 0;
+  for (auto& g : ginfo) {
+    if (!(g.flags & GF_O_ZERO)) { set_error("adjoint: o must be zero (H = E_nu + h)"); return ASR_EINVAL; }
+    if (!(g.flags & GF_D_UNIFORM)) dunif = false;
+    mmax = std::max(mmax, g.nlev);
+  }
+  if (mmax > NLMAX) { set_error("adjoint: depth above %d", NLMAX); return ASR_EINVAL; }
+  const int c = std::max(1, stride > 0 ? stride : (int)std::ceil(std::sqrt((double)mmax)));
+  const int nseg = (mmax + c - 1) / c;
+  // tiles: one group each
+  std::vector<std::vector<int>> tiles;
+  {
+    std::vector<std::vector<int>> per_group(ginfo.size());
+    for (int L = 0; L < nlane; ++L) per_group[lane_group[L]].push_back(L);
+    for (auto& lst : per_group)
+      for (size_t q = 0; q < lst.size(); q += TL)
+        tiles.emplace_back(lst.begin() + q, lst.begin() + std::min(lst.size(), q + (size_t)TL));
+  }
+  const int ntile_all = (int)tiles.size();
+  // memory: forward 3 + checkpoints 2 nseg + segment (c + 2) X + c Y + c T2 + adjoint 7 (+1 temporary) vectors per tile
+  const size_t vec_bytes = (size_t)nn * 9 * TL * sizeof(T2);
+  const int nvec = 3 + 2 * nseg + (c + 2) + 2 * c + 8;
+  size_t freeb = 0, totb = 0;
+  cudaMemGetInfo(&freeb, &totb);
+  int tpb = 4;
+  if (const char* e = getenv("ASR_TILES_PER_BATCH")) tpb = std::max(1, atoi(e));
+  while (tpb > 1 && (size_t)tpb * nvec * vec_bytes > freeb / 2) tpb /= 2;
+  if ((size_t)nvec * vec_bytes > freeb) { set_error("adjoint: %d vectors of %zu bytes do not fit", nvec, vec_bytes); return ASR_ENOMEM; }
+  tpb = std::min(tpb, ntile_all);
+  const int npw = 4, npb = WPB * npw, bpt = (nn + npb - 1) / npb;
+  const int gnpb = 64, gbpt = (nn + gnpb - 1) / gnpb, ngd = 3 * 9 * nsp;
+  const int nlp = tpb * TL;
+  Dev<double> d_gblob, d_mt;
+  Dev<GroupInfo> d_ginfo;
+  Dev<int> d_spc;
+  ASR_TRY(d_gblob.alloc(gblob.size())); ASR_TRY(d_ginfo.alloc(ginfo.size()));
+  ASR_TRY(d_mt.alloc(op->mt.size())); ASR_TRY(d_spc.alloc(op->spc.size()));
+  ASR_CUDA(cudaMemcpyAsync(d_gblob.p, gblob.data(), gblob.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_ginfo.p, ginfo.data(), ginfo.size() * sizeof(GroupInfo), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_mt.p, op->mt.data(), op->mt.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_spc.p, op->spc.data(), op->spc.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  Dev<int> d_lgroup, d_act, d_wact, d_m, d_tact, d_nfall, d_tgroup;
+  Dev<double2> d_a, d_b, d_abar, d_bbar, d_gprev, d_acur, d_bprev, d_su, d_sup, d_part, d_part2, d_z, d_gpart, d_gacc;
+  Dev<double2> d_sn, d_sk, d_sp, d_c[6], d_d1, d_d2, d_d3, d_one;
+  ASR_TRY(d_lgroup.alloc(nlp)); ASR_TRY(d_act.alloc(nlp)); ASR_TRY(d_wact.alloc(nlp)); ASR_TRY(d_m.alloc(nlp));
+  ASR_TRY(d_tact.alloc(tpb)); ASR_TRY(d_nfall.alloc(1)); ASR_TRY(d_tgroup.alloc(tpb));
+  ASR_TRY(d_a.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_b.alloc((size_t)nlp * NLMAX));
+  ASR_TRY(d_abar.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_bbar.alloc((size_t)nlp * NLMAX));
+  ASR_TRY(d_gprev.alloc(nlp)); ASR_TRY(d_acur.alloc(nlp)); ASR_TRY(d_bprev.alloc(nlp)); ASR_TRY(d_su.alloc(nlp));
+  ASR_TRY(d_sup.alloc(nlp)); ASR_TRY(d_part.alloc((size_t)tpb * bpt * TL)); ASR_TRY(d_part2.alloc((size_t)tpb * bpt * TL));
+  ASR_TRY(d_z.alloc(nlp)); ASR_TRY(d_gpart.alloc((size_t)tpb * gbpt * ngd)); ASR_TRY(d_gacc.alloc((size_t)tpb * ngd));
+  ASR_TRY(d_sn.alloc(nlp)); ASR_TRY(d_sk.alloc(nlp)); ASR_TRY(d_sp.alloc(nlp));
+  for (int q = 0; q < 6; ++q) ASR_TRY(d_c[q].alloc(nlp));
+  ASR_TRY(d_d1.alloc(nlp)); ASR_TRY(d_d2.alloc(nlp)); ASR_TRY(d_d3.alloc(nlp)); ASR_TRY(d_one.alloc(nlp));
+  const size_t vlen = (size_t)tpb * nn * 9 * TL;
+  std::vector<Dev<T2>> V(nvec);
+  for (int q = 0; q < nvec; ++q) ASR_TRY(V[q].alloc(vlen));
+  T2* FW[3] = {V[0].p, V[1].p, V[2].p};
+  auto CK = [&](int j, int which) { return V[3 + 2 * j + which].p; };          // checkpoint j: X_{k0-1}, X_{k0}
+  const int xs0 = 3 + 2 * nseg;
+  auto XS = [&](int q) { return V[xs0 + q].p; };                               // X_{k0-1+q}, q = 0 .. c+1
+  auto YS = [&](int q) { return V[xs0 + c + 2 + q].p; };
+  auto TS = [&](int q) { return V[xs0 + 2 * c + 2 + q].p; };
+  const int ab0 = xs0 + 3 * c + 2;
+  T2* UB[3] = {V[ab0].p, V[ab0 + 1].p, V[ab0 + 2].p};
+  T2* WB = V[ab0 + 3].p;
+  T2* YB = V[ab0 + 4].p;
+  T2* T2B = V[ab0 + 5].p;
+  T2* AY = V[ab0 + 6].p;
+  T2* TMP = V[ab0 + 7].p;
+  g_out.assign(nlane, make_double2(0, 0));
+  grad_out.assign(ginfo.size() * (size_t)ngd, make_double2(0, 0));
+  std::vector<double2> ones(nlp, make_double2(1.0, 0.0));
+  ASR_CUDA(cudaMemcpyAsync(d_one.p, ones.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
+  std::vector<int> hgroup(nlp), lmap(nlp), hm(nlp);
+  std::vector<double2> hz(nlp), ha((size_t)nlp * NLMAX), hb((size_t)nlp * NLMAX), habar((size_t)nlp * NLMAX), hbbar((size_t)nlp * NLMAX);
+  std::vector<double2> hgacc((size_t)tpb * ngd);
+  OpView ov = op->view();
+  for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
+    const int nt = std::min(tpb, ntile_all - t0);
+    std::vector<int> tact(tpb, 0), act(nlp, 0), tgroup(tpb, -1);
+    for (int q = 0; q < nlp; ++q) {
+      int bt = q / TL, L = -1;
+      if (bt < nt && q % TL < (int)tiles[t0 + bt].size()) L = tiles[t0 + bt][q % TL];
+      lmap[q] = L;
+      hgroup[q] = L >= 0 ? lane_group[L] : -1;
+      hz[q] = L >= 0 ? lane_z[L] : make_double2(0, 0);
+      if (L >= 0) { tact[bt] = 1; act[q] = 1; tgroup[bt] = hgroup[q]; }
+    }
+    ASR_CUDA(cudaMemcpyAsync(d_lgroup.p, hgroup.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_tgroup.p, tgroup.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_act.p, act.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_tact.p, tact.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_z.p, hz.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_su.p, ones.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemsetAsync(d_wact.p, 0, nlp * sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_m.p, 0, nlp * sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_a.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_b.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_gprev.p, 0, nlp * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_bprev.p, 0, nlp * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_sup.p, 0, nlp * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_nfall.p, 0, sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_gacc.p, 0, (size_t)tpb * ngd * sizeof(double2), s));
+    BatchView bv{nt, nn, op->nsmax, 0, ASR_MODE_EDC, project, tail, NLMAX, 0.0, d_gblob.p, GL, d_ginfo.p, d_lgroup.p, d_tgroup.p,
+                 d_z.p, d_act.p, d_wact.p, d_m.p, d_a.p, d_b.p, d_gprev.p, d_acur.p, d_bprev.p, d_su.p, d_sup.p, d_tact.p,
+                 d_nfall.p};
+    const int grid = nt * bpt;
+    int kmax = 0;
+    for (int q = 0; q < nlp; ++q) if (hgroup[q] >= 0) kmax = std::max(kmax, ginfo[hgroup[q]].nlev);
+    // ---- forward with checkpoints (X_{k0-1}, X_{k0}) at k0 = 1 + j c
+    k_init<ST><<<std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256), 256, 0, s>>>(bv, FW[1], FW[0]);
+    const size_t cpy = (size_t)nt * nn * 9 * TL * sizeof(T2);
+    ASR_CUDA(cudaMemcpyAsync(CK(0, 0), FW[0], cpy, cudaMemcpyDeviceToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(CK(0, 1), FW[1], cpy, cudaMemcpyDeviceToDevice, s));
+    for (int k = 1; k <= kmax; ++k) {
+      T2* U = FW[k % 3];
+      T2* UP = FW[(k + 2) % 3];
+      T2* Y = FW[(k + 1) % 3];
+      apply_SD<ST>(op, bv, dunif, U, TMP, AY, d_part.p, npw, grid, s);
+      k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, AY, U, PCEB, true, U, false, nullptr, 1.0, true, Y, d_part.p, npw);
+      k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+      k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, Y, U, UP, d_part.p, npw);
+      k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
+      if (k % c == 0 && k / c < nseg) {   // X_k and X_{k+1} start segment k / c
+        ASR_CUDA(cudaMemcpyAsync(CK(k / c, 0), U, cpy, cudaMemcpyDeviceToDevice, s));
+        ASR_CUDA(cudaMemcpyAsync(CK(k / c, 1), Y, cpy, cudaMemcpyDeviceToDevice, s));
+      }
+    }
+    ASR_CUDA(cudaGetLastError());
+    // the forward retired finished tiles; the recomputation and the reverse sweep visit every tile of the batch
+    ASR_CUDA(cudaMemcpyAsync(d_tact.p, tact.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
+    // ---- fraction adjoint on the host: G and the seeds abar, bbar
+    ASR_CUDA(cudaMemcpyAsync(hm.data(), d_m.p, nlp * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaMemcpyAsync(ha.data(), d_a.p, ha.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaMemcpyAsync(hb.data(), d_b.p, hb.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaStreamSynchronize(s));
+    std::fill(habar.begin(), habar.end(), make_double2(0, 0));
+    std::fill(hbbar.begin(), hbbar.end(), make_double2(0, 0));
+    {
+      std::vector<double2> w1(NLMAX), w2(NLMAX), w3(NLMAX), w4(NLMAX), w5(NLMAX);
+      for (int q = 0; q < nlp; ++q) {
+        int L = lmap[q];
+        if (L < 0 || hm[q] < 1) continue;
+        g_out[L] = cf_species_adjoint(&ha[(size_t)q * NLMAX], &hb[(size_t)q * NLMAX], hm[q], lane_z[L], tail, lane_w[L],
+                                      &habar[(size_t)q * NLMAX], &hbbar[(size_t)q * NLMAX], w1.data(), w2.data(), w3.data(),
+                                      w4.data(), w5.data());
+      }
+    }
+    ASR_CUDA(cudaMemcpyAsync(d_abar.p, habar.data(), habar.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_bbar.p, hbbar.data(), hbbar.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+    AdjScal S{d_a.p, d_b.p, d_m.p, d_abar.p, d_bbar.p, d_sn.p, d_sk.p, d_sp.p, d_c[0].p, d_c[1].p, d_c[2].p, d_c[3].p, d_c[4].p,
+              d_c[5].p, d_d1.p, d_d2.p, d_d3.p};
+    // adjoint BatchView: unit scales for applying A to ybar
+    BatchView bva = bv;
+    bva.su = d_one.p;
+    for (int q = 0; q < 3; ++q) ASR_CUDA(cudaMemsetAsync(UB[q], 0, cpy, s));
+    for (int j = nseg - 1; j >= 0; --j) {
+      const int k0 = 1 + j * c, k1 = std::min(kmax, k0 + c - 1);
+      if (k0 > kmax) continue;
+      // recompute X_{k0-1} .. X_{k1+1}, Y_k, T2_k
+      ASR_CUDA(cudaMemcpyAsync(XS(0), CK(j, 0), cpy, cudaMemcpyDeviceToDevice, s));
+      ASR_CUDA(cudaMemcpyAsync(XS(1), CK(j, 1), cpy, cudaMemcpyDeviceToDevice, s));
+      for (int k = k0; k <= k1; ++k) {
+        int q = k - k0;
+        k_set_fwd<<<(nlp + 127) / 128, 128, 0, s>>>(bv, S, nlp, k);
+        apply_SD<ST>(op, bv, dunif, XS(q + 1), TMP, TS(q), d_part.p, npw, grid, s);
+        k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TS(q), XS(q + 1), PCEB, true, XS(q + 1), false, nullptr, 1.0, true, YS(q),
+                                                d_part.p, npw);
+        ASR_CUDA(cudaMemcpyAsync(XS(q + 2), YS(q), cpy, cudaMemcpyDeviceToDevice, s));
+        k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, XS(q + 2), XS(q + 1), XS(q), d_part.p, npw);
+      }
+      // reverse k = k1 .. k0
+      for (int k = k1; k >= k0; --k) {
+        int q = k - k0;
+        T2* ubn = UB[(k + 1) % 3];
+        T2* ubk = UB[k % 3];
+        T2* ubp = UB[(k + 2) % 3];
+        k_dot<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, ubn, XS(q + 2), d_part.p, npw);
+        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d1.p);
+        k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 0);
+        k_adj_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, ubn, XS(q + 2), XS(q + 1), XS(q), d_c[0].p, d_c[1].p, WB, d_part.p, d_part2.p,
+                                              npw);
+        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d2.p);
+        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_d3.p);
+        k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 1);
+        k_adj_y<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, WB, XS(q + 1), d_c[2].p, d_c[3].p, YB, k > 1 ? ubp : nullptr, npw);
+        // A ybar (unit scale) and t2bar = S R_d ybar
+        apply_SD<ST>(op, bva, dunif, YB, TMP, T2B, d_part.p, npw, grid, s);
+        k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, T2B, YB, PCEB, true, YB, false, nullptr, 1.0, true, AY, d_part.p, npw);
+        k_adj_u<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, AY, YS(q), WB, d_c[4].p, d_c[5].p, ubk, npw);
+        k_adj_grad<ST><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, YB, T2B, XS(q + 1), TS(q), d_sk.p, gnpb,
+                                                      d_gpart.p);
+        k_adj_gsum<<<nt, 128, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
+        ASR_CUDA(cudaMemsetAsync(ubn, 0, cpy, s));   // becomes ubar_{k-2}
+      }
+    }
+    ASR_CUDA(cudaGetLastError());
+    ASR_CUDA(cudaMemcpyAsync(hgacc.data(), d_gacc.p, (size_t)tpb * ngd * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaStreamSynchronize(s));
+    ASR_CUDA(cudaGetLastError());
+    for (int bt = 0; bt < nt; ++bt) {
+      int gq = tgroup[bt];
+      if (gq < 0) continue;
+      for (int e = 0; e < ngd; ++e) grad_out[(size_t)gq * ngd + e] = cadd(grad_out[(size_t)gq * ngd + e], hgacc[(size_t)bt * ngd + e]);
+    }
+    const int nsd = dunif ? 1 : 2;   // launches of one S application
+    ctx->launches += 1 + (int64_t)kmax * ((4 + nsd) + (3 + nsd) + (12 + nsd));
+  }
+  return ASR_OK;
+}
+
 }  // namespace
+
+// the operator kernels stage up to 96 KB of bond blocks in shared memory (set once per device)
+static void smem_attrs() {
+  static bool done[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || done[dev]) return;
+  cudaFuncSetAttribute(k_smul<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  done[dev] = true;
+}
+
+int run_adjoint(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+                const GroupLayout& GL, const std::vector<int>& lane_group, const std::vector<double2>& lane_z,
+                const std::vector<double2>& lane_w, int tail, int project, int stride, int precision, std::vector<double2>& g_out,
+                std::vector<double2>& grad_out) {
+  smem_attrs();
+  if (smul_smem(op, sizeof(double)) > 96 * 1024) { set_error("adjoint: bond tables above 96 KB of shared memory"); return ASR_EINVAL; }
+  if (precision == ASR_FP32)
+    return run_adjoint_t<float>(ctx, op, ginfo, gblob, GL, lane_group, lane_z, lane_w, tail, project, stride, g_out, grad_out);
+  return run_adjoint_t<double>(ctx, op, ginfo, gblob, GL, lane_group, lane_z, lane_w, tail, project, stride, g_out, grad_out);
+}
 
 int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
               const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
               const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
               std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out) {
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaFuncSetAttribute(k_smul<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_smul<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_smul<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_smul<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_smul<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    cudaFuncSetAttribute(k_smul<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-    attr_done = true;
-  }
+  smem_attrs();
   if (smul_smem(op, sizeof(double)) > 96 * 1024) { set_error("chains: bond tables above 96 KB of shared memory"); return ASR_EINVAL; }
   if (opt.precision == ASR_FP32)
     return run_lanes_t<float>(ctx, op, ginfo, gblob, GL, lane_group, d_lane_z, nlane, opt, d_g_out, a_out, b_out, m_out, nfall_out,
@@ -774,13 +1375,18 @@ int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   const int nn = op->nn;
   const int nt = (nvec + TL - 1) / TL;
   const size_t nel = (size_t)nt * nn * 9 * TL;
+  // normalised coordinates in and out; the kernels work in amplitude coordinates (x / sqrt(orbit size))
+  std::vector<double> sqv(nn);
+  ASR_CUDA(cudaMemcpyAsync(sqv.data(), op->d_sq, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
   std::vector<double2> hx(nel, make_double2(0, 0));
   for (int v = 0; v < nvec; ++v)
     for (int i = 0; i < nn; ++i)
       for (int l = 0; l < 9; ++l) {
         size_t src = (size_t)v * 9 * nn + 9 * (size_t)i + l;
         size_t dst = (((size_t)(v / TL) * nn + i) * 9 + l) * TL + v % TL;
-        hx[dst] = complex_in ? make_double2(x_host[2 * src], x_host[2 * src + 1]) : make_double2(x_host[src], 0.0);
+        double f = what == APPLY_PROJECT ? 1.0 : 1.0 / sqv[i];
+        hx[dst] = complex_in ? make_double2(f * x_host[2 * src], f * x_host[2 * src + 1]) : make_double2(f * x_host[src], 0.0);
       }
   Dev<double> d_gblob;
   Dev<GroupInfo> d_ginfo;
@@ -790,12 +1396,14 @@ int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   ASR_CUDA(cudaMemcpyAsync(d_ginfo.p, ginfo.data(), ginfo.size() * sizeof(GroupInfo), cudaMemcpyHostToDevice, s));
   const int nlp = nt * TL;
   const int npw = 4, npb = WPB * npw, bpt = (nn + npb - 1) / npb;
-  std::vector<int> hgroup(nlp), ones(nlp, 1), tact(nt, 1);
+  std::vector<int> hgroup(nlp), ones(nlp, 1), tact(nt, 1), tgroup(nt, 0);
   for (int q = 0; q < nlp; ++q) hgroup[q] = q < nvec ? 0 : -1;
   std::vector<double2> hz(nlp, make_double2(0.0, what == APPLY_RAND_Z ? 1.0 : 0.0)), hsu(nlp, make_double2(1.0, 0.0));
-  Dev<int> d_lgroup, d_act, d_tact;
+  Dev<int> d_lgroup, d_act, d_tact, d_tgroup;
   Dev<double2> d_z, d_su, d_part, V[6];
   ASR_TRY(d_lgroup.alloc(nlp)); ASR_TRY(d_act.alloc(nlp)); ASR_TRY(d_tact.alloc(nt)); ASR_TRY(d_z.alloc(nlp));
+  ASR_TRY(d_tgroup.alloc(nt));
+  ASR_CUDA(cudaMemcpyAsync(d_tgroup.p, tgroup.data(), nt * sizeof(int), cudaMemcpyHostToDevice, s));
   ASR_TRY(d_su.alloc(nlp)); ASR_TRY(d_part.alloc((size_t)nt * bpt * TL));
   for (int q = 0; q < 6; ++q) ASR_TRY(V[q].alloc(nel));
   ASR_CUDA(cudaMemcpyAsync(V[0].p, hx.data(), nel * sizeof(double2), cudaMemcpyHostToDevice, s));
@@ -806,7 +1414,7 @@ int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   ASR_CUDA(cudaMemcpyAsync(d_su.p, hsu.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
   BatchView bv{};
   bv.ntile = nt; bv.nn = nn; bv.nsm = op->nsmax; bv.mode = ASR_MODE_EDC; bv.project = 1; bv.gblob = d_gblob.p; bv.GL = GL;
-  bv.ginfo = d_ginfo.p; bv.lane_group = d_lgroup.p; bv.lane_z = d_z.p; bv.lane_act = d_act.p; bv.lane_wact = d_act.p;
+  bv.ginfo = d_ginfo.p; bv.lane_group = d_lgroup.p; bv.tile_group = d_tgroup.p; bv.lane_z = d_z.p; bv.lane_act = d_act.p; bv.lane_wact = d_act.p;
   bv.su = d_su.p; bv.sup = d_su.p; bv.tile_act = d_tact.p;
   const int grid = nt * bpt;
   OpView ov = op->view();
@@ -817,8 +1425,8 @@ int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     ASR_TRY(step_apply<double>(ctx, op, bv, fused, any_o, dunif, V[0].p, V[1].p, V[2].p, V[3].p, V[4].p, V[5].p, d_part.p, npw,
                                grid));
   } else if (what == APPLY_RAND_Z) {
-    // w = sq X(x / sq) with X = z pa + pb, z = i: the complex parameter par = pb + i pa
-    k_combine<double><<<grid, WPB * TL, 0, s>>>(ov, bv, nullptr, V[0].p, true, PB, true, V[0].p, false, nullptr, 1.0, true, V[1].p,
+    // w = X x with X = z pa + pb, z = i: the complex parameter par = pb + i pa
+    k_combine<double><<<grid, WPB * TL, 0, s>>>(ov, bv, nullptr, V[0].p, PB, true, V[0].p, false, nullptr, 1.0, true, V[1].p,
                                                 d_part.p, npw);
   } else {
     k_project<double><<<grid, WPB * TL, 0, s>>>(ov, bv, V[0].p, npw);
@@ -834,6 +1442,7 @@ int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
       for (int l = 0; l < 9; ++l) {
         size_t dst = (size_t)v * 9 * nn + 9 * (size_t)i + l;
         double2 val = hy[(((size_t)(v / TL) * nn + i) * 9 + l) * TL + v % TL];
+        if (what != APPLY_PROJECT) val = cscale(val, sqv[i]);
         if (complex_in || what != APPLY_H) { y_host[2 * dst] = val.x; y_host[2 * dst + 1] = val.y; }
         else y_host[dst] = val.x;
       }

@@ -38,6 +38,7 @@ struct BatchView {
   GroupLayout GL;
   const GroupInfo* ginfo;
   const int* lane_group;   // -1: idle lane
+  const int* tile_group;   // the group of every lane of the tile (tiles hold one group)
   const double2* lane_z;
   int* lane_act;           // 1 active
   int* lane_wact;          // 1: the lane computes w / b this step
@@ -68,6 +69,12 @@ int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
               const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
               const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
               std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out);
+
+// reverse mode: G per lane and the gradients sum_lanes w_L dG_L/dpar per group, kinds (c | e | pb), d, pa, each (9, nsp)
+int run_adjoint(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+                const GroupLayout& GL, const std::vector<int>& lane_group, const std::vector<double2>& lane_z,
+                const std::vector<double2>& lane_w, int tail, int project, int stride, int precision, std::vector<double2>& g_out,
+                std::vector<double2>& grad_out);
 
 // y = H x style applications of the operator's own parameters on nvec vectors (normalised coordinates)
 int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,

@@ -126,6 +126,18 @@ int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
                        int mode, double depth_tol, int tail, int precision, int project, void* g_dev, double* a, double* b,
                        int* mused);
 
+/* Reverse mode of the batched energy-dependent chains (edc route, o = 0, fixed depth nlev per group): g(nz, ngroup) as
+ * asr_chains_run, and grad(9, nsp, 3, ngroup) complex = sum_j w(j, q) dG(j, q)/dpar for the parameter arrays of group q:
+ * kind 0 the diagonal c (the same derivative applies to e and pb, which enter only as c + e + pb), kind 1 d, kind 2 pa.
+ * w(nz, ngroup) complex seeds.  The entries are symmetrised over the orbits of the orbitals under the operator's point
+ * group (the group-reduced operator represents only parameters constant on each orbit): derivatives along every
+ * group-invariant direction (per l, per orbit) are exact.  The Lanczos vectors are kept every `stride` levels
+ * (0: ceil(sqrt(depth))) and recomputed
+ * in between.  Tails none, hull, avg2.  No counterpart in the reference (gradients of the chain with respect to the
+ * species parameters of src/asr_edc.f90:41-71). */
+int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz,
+                       const double* w, int tail, int precision, int project, int stride, double* g, double* grad);
+
 /* cf_species (src/asr_chain.f90:67-167) for nchain complex chains a, b (ld, nchain), depth m(nchain), at the energies
  * z(nz, nchain): g(nz, nchain).  edges (optional, (2, nz, nchain)) returns the tail (centre, quarter width). */
 int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain, const double* z, int nz,
