@@ -29,7 +29,7 @@ EXPORTS = ["asr_version", "asr_last_error", "asr_ctx_create", "asr_ctx_destroy",
            "asr_op_free", "asr_op_dims", "asr_op_export_tables", "asr_op_set_params", "asr_op_freeze_site", "asr_op_unfreeze",
            "asr_op_set_start", "asr_op_set_chi", "asr_op_set_class_conc", "asr_op_apply", "asr_op_rand_c", "asr_op_project_c",
            "asr_chains_run", "asr_chains_run_dev", "asr_cf_eval", "asr_cf_adjoint",
-    "asr_chains_adjoint", "asr_supercell_build", "asr_supercell_free",
+    "asr_chains_adjoint", "asr_cf_eval_noalloc", "asr_supercell_build", "asr_supercell_free",
            "asr_supercell_apply", "asr_kpm_moments", "asr_kpm_dos", "asr_sro_layout", "asr_gauss_legendre", "asr_contour_nodes",
            "asr_contour_nodes_closed", "asr_contour_nodes_fermi", "asr_contour_moment"]
 

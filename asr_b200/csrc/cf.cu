@@ -55,3 +55,91 @@ __global__ void k_real_green(const double* a, const double* b, const int* n, int
 }
 
 }  // namespace asrb
+
+// ------------------------------------------------------------------------------------------------ asr_cf_eval_noalloc
+// The same fractions as asr_cf_eval, staged through one file-scope device array instead of cudaMalloc'd buffers.  It is
+// meant for callers that may not allocate device memory: a host that evaluates fractions between chain batches while
+// other streams are busy (cudaMalloc and cudaFree synchronise the device), or a process whose device memory is owned by
+// another allocator (a framework's caching allocator, a fixed memory budget).  The operands must fit in the scratch:
+//   32 ld nchain (a, b) + 32 nz nchain (z, g) + 4 nchain (m) + 4 (fallback counter) bytes, each part rounded up to
+//   256 bytes, at most ASR_CF_NOALLOC_BYTES (8 MiB) per device.
+// Only the fallback counter has to start at zero; it is cleared on the stream before every launch.  The scratch is one
+// per device: two calls that overlap in time on the same device (other host threads, other streams) race on it.
+#include <mutex>
+
+#include "../../include/asr_b200.h"
+
+namespace asrb {
+namespace {
+
+constexpr int kMaxDevices = 64;
+__device__ __align__(256) unsigned char g_cf_scratch[ASR_CF_NOALLOC_BYTES];
+std::mutex g_cf_mu;
+unsigned char* g_cf_ptr[kMaxDevices] = {};
+
+size_t up256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// device address of the scratch on the current device, resolved once per device (the device must be current)
+int cf_scratch(int dev, unsigned char** out) {
+  if (dev < 0 || dev >= kMaxDevices) { set_error("asr_cf_eval_noalloc: device %d out of range", dev); return ASR_EINVAL; }
+  std::lock_guard<std::mutex> lk(g_cf_mu);
+  if (!g_cf_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t rc = cudaGetSymbolAddress(&p, g_cf_scratch);
+    if (rc != cudaSuccess || !p) {
+      set_error("asr_cf_eval_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev, cudaGetErrorString(rc));
+      return ASR_ECUDA;
+    }
+    g_cf_ptr[dev] = (unsigned char*)p;
+  }
+  *out = g_cf_ptr[dev];
+  return ASR_OK;
+}
+
+}  // namespace
+}  // namespace asrb
+
+extern "C" int asr_cf_eval_noalloc(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain,
+                                   const double* z, int nz, int tail, double* g, int64_t* nfall) {
+  using namespace asrb;
+  if (!ctx || !a || !b || !m || !z || !g || ld < 1 || nchain < 1 || nz < 1 || tail < 0 || tail > 3) {
+    set_error("asr_cf_eval_noalloc: bad argument");
+    return ASR_EINVAL;
+  }
+  for (int c = 0; c < nchain; ++c)
+    if (m[c] < 1 || m[c] > ld || m[c] > CF_NMAX) { set_error("asr_cf_eval_noalloc: depth of chain %d out of range", c + 1); return ASR_EINVAL; }
+  const size_t nab = (size_t)ld * nchain, nzz = (size_t)nz * nchain;
+  const size_t o_b = up256(nab * sizeof(double2)), o_z = o_b + up256(nab * sizeof(double2));
+  const size_t o_g = o_z + up256(nzz * sizeof(double2)), o_m = o_g + up256(nzz * sizeof(double2));
+  const size_t o_nf = o_m + up256((size_t)nchain * sizeof(int)), total = o_nf + up256(sizeof(int));
+  if (total > (size_t)ASR_CF_NOALLOC_BYTES) {
+    set_error("asr_cf_eval_noalloc: the operands need %zu bytes, above the %zu-byte static scratch (split the chains)", total,
+              (size_t)ASR_CF_NOALLOC_BYTES);
+    return ASR_EINVAL;
+  }
+  ASR_CUDA(cudaSetDevice(ctx->device));
+  unsigned char* base = nullptr;
+  ASR_TRY(cf_scratch(ctx->device, &base));
+  cudaStream_t s = ctx->stream;
+  double2* d_a = (double2*)base;
+  double2* d_b = (double2*)(base + o_b);
+  double2* d_z = (double2*)(base + o_z);
+  double2* d_g = (double2*)(base + o_g);
+  int* d_m = (int*)(base + o_m);
+  int* d_nf = (int*)(base + o_nf);
+  ASR_CUDA(cudaMemcpyAsync(d_a, a, nab * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_b, b, nab * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_z, z, nzz * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_m, m, nchain * sizeof(int), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(int), s));
+  k_cf_eval<<<(unsigned)((nzz + 127) / 128), 128, 0, s>>>(d_a, d_b, d_m, ld, nchain, d_z, nz, tail, d_g, nullptr, d_nf);
+  ASR_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  int nf = 0;
+  ASR_CUDA(cudaMemcpyAsync(g, d_g, nzz * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(&nf, d_nf, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  if (nfall) *nfall = nf;
+  ctx->nfall += nf;
+  return ASR_OK;
+}

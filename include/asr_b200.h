@@ -143,6 +143,16 @@ int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
 int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain, const double* z, int nz,
                 int tail, double* g, double* edges, int64_t* nfall);
 
+/* asr_cf_eval without device allocation (no edges), for callers that may not call cudaMalloc / cudaFree (they
+ * synchronise the device, or device memory belongs to another allocator).  No counterpart in the reference.  The
+ * operands go through one static device array of ASR_CF_NOALLOC_BYTES per device; calls whose operands need more
+ * (32 ld nchain + 32 nz nchain + 4 nchain + 4 bytes, each part rounded up to 256) return ASR_EINVAL.  The first call on
+ * a device resolves the array's address; make it before capturing the context's stream.  Calls that overlap in time
+ * on one device share the array and race: serialise them. */
+#define ASR_CF_NOALLOC_BYTES (8u << 20)
+int asr_cf_eval_noalloc(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain, const double* z,
+                        int nz, int tail, double* g, int64_t* nfall);
+
 /* reverse mode of cf_species for one chain (host): abar(m), bbar(m) complex receive w dG/da_k and w dG/db_k; g = G.
  * Tails none, hull, avg2 (the bp fixed point has no derivative here).  No counterpart in the reference. */
 int asr_cf_adjoint(const double* a, const double* b, int m, double zr, double zi, int tail, double wr, double wi, double* abar,
