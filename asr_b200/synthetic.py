@@ -248,3 +248,41 @@ def cubic_case(kind: str, l: int, nsp: int, conc, seed: int, group: str = "d2h",
     mdl = ClassModel.single_class(nsp, conc, block, block0)
     return dict(graph=g, coord=coord, bvec=bvec, cls=cls, perm=np.asfortranarray(perm, dtype=np.int32),
                 dmat=np.asfortranarray(dmat), model=mdl)
+
+
+# L2_1 (Heusler-like) decoration of bcc: four fcc sublattices.  Sites of the bcc grid have i, j, k all even or all odd
+# (half-lattice units); even sites split by (i + j + k) / 2 mod 2, odd sites by (i + j + k - 3) / 2 mod 2.
+HEUSLER_SHIFT = ((0, 0, 0), (2, 0, 0), (1, 1, 1), (3, 1, 1))   # a site of sublattice 1..4 relative to sublattice 1
+
+
+def heusler_sublattice(coord: np.ndarray) -> np.ndarray:
+    """Sublattice 1..4 of every bcc site (3, n)."""
+    s = coord.sum(axis=0)
+    odd = (coord[0] % 2).astype(np.int64)
+    half = np.where(odd == 1, (s - 3) // 2, s // 2) % 2
+    return (1 + 2 * odd + half).astype(np.int32)
+
+
+def heusler_case(l: int = 4, seed: int = 3, sublattice: int = 1, maxlevel: int = 3, maxrank: int = 1):
+    """L2_1 four-sublattice bcc cell with sublattices 1-3 ordered (species 1, 2, 3) and sublattice 4 disordered
+    (species 4 and 5 at 0.6 / 0.4, Cr0.6Fe0.4-like); NN + NNN Slater-Koster blocks.  The site classes are shifted so
+    that site 1 (the origin, the start of the recursion) lies on ``sublattice``; the group is the class-preserving
+    diagonal subgroup (D2 here: all nine orbitals one dimensional)."""
+    if l % 2:
+        raise ValueError("heusler_case: l must be even for a periodic L2_1 decoration")
+    g, coord, bvec = lat.periodic_graph_shells("bcc", l, 4)
+    shift = np.asarray(HEUSLER_SHIFT[sublattice - 1], dtype=np.int64)[:, None]
+    cls = heusler_sublattice(coord + shift)
+    perm, mats = lat.d2h_ops(coord, 2 * l, cls)
+    dmat = lat.orbital_rep(mats)
+    block, block0 = sk_blocks(bvec, seed)
+    nsc = np.array([1, 1, 1, 2], dtype=np.int32)
+    spc = np.asfortranarray(np.array([[1, 0], [2, 0], [3, 0], [4, 5]], dtype=np.int32).T)
+    conc = np.asfortranarray(np.array([[1.0, 0.0], [1.0, 0.0], [1.0, 0.0], [0.6, 0.4]]).T)
+    mdl = ClassModel(nsp=5, nsc=nsc, spc=spc, conc=conc, block=np.asfortranarray(block.reshape(9, 9, -1, 1)),
+                     block0=np.asfortranarray(block0.reshape(9, 9, 1)))
+    fl = np.ones(g.n, np.int32)
+    fl[0] = 0
+    return dict(graph=g, coord=coord, bvec=bvec, cls=cls, perm=np.asfortranarray(perm, dtype=np.int32),
+                dmat=np.asfortranarray(dmat), model=mdl, maxlevel=maxlevel, maxrank=maxrank, flippable=fl,
+                sublattice=sublattice)

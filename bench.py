@@ -25,6 +25,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NZ_SLICE = 192
+# DRAM bytes (read + write) per launch of the step kernel from one ncu capture of a 16-tile launch, and the algorithmic
+# bytes of that launch (profiles/k_smul_fcc_ternary_edc.md); traffic is scaled to the bench's mean launch
+NCU_STEP_TRAFFIC = {"fp64": (6.14e9, 16 * 20969 * (2 * 4608.0 + 18 * 5 + 3 * 5 + 20))}
 
 
 def parse():
@@ -37,6 +40,8 @@ def parse():
     p.add_argument("--nz-slice", type=int, default=NZ_SLICE)
     p.add_argument("--cpu-sample", type=int, default=1, help="run the bounded CPU baseline sample (1) or skip it (0)")
     p.add_argument("--e2e", type=int, default=1, help="time the host-buffer C-ABI path too (1) or skip it (0)")
+    p.add_argument("--legs", type=int, default=1,
+                   help="also measure the mixed-precision leg with its DOS error and the adjoint leg (1) or not (0)")
     return p.parse_args()
 
 
@@ -166,6 +171,86 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def fp64_peak_tflops(torch):
+    """Measured FP64 matrix throughput of this GPU (cuBLAS DGEMM 8192^3, best of 3), the denominator of the FP64
+    fraction of the chain step."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = a @ b
+    best = 1e30
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    return 2.0 * n ** 3 / (best / 1000.0) / 1e12
+
+
+def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
+    """The mixed-precision leg (FP32 matvec and vectors, FP64 coefficients and fractions) with its DOS and charge error
+    against the FP64 run, and the adjoint leg (forward plus reverse sweep) on the contour energies."""
+    import torch
+    nzs = args.nz_slice
+    depth = np.array([g["nlev"] for g in groups])
+    out = {}
+    step(0, "fp32")
+    torch.cuda.synchronize()
+    nsteps = max(1, min(args.steps, 3))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for it in range(nsteps):
+        step(args.warmup + it, "fp32")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms32 = e0.elapsed_time(e1)
+    mixed = {"value": int(depth.sum()) * nzs * nsteps * world / (ms32 / 1000.0), "unit": "chain-steps/s", "steps": nsteps}
+    # error against FP64: DOS -Im G / pi on 192 real-axis energies, and the contour charge M_0 over the 48 contour nodes
+    zr = z_all[48:48 + 192]
+    g64 = A.chains_run(op, specs, zr, "edc", 0.0, "hull", "fp64")["g"]
+    g32 = A.chains_run(op, specs, zr, "edc", 0.0, "hull", "fp32")["g"]
+    dos64, dos32 = -g64.imag / np.pi, -g32.imag / np.pi
+    mixed["dos_error"] = float(np.max(np.abs(dos32 - dos64)) / np.max(np.abs(dos64)))
+    ebot, ef = -1.2, 0.3
+    x, wgl = np.polynomial.legendre.leggauss(48)
+    th = 0.5 * np.pi * (1.0 - x)
+    zc = z_all[:48]
+    wc = 0.5 * np.pi * wgl * 0.5j * (ef - ebot) * np.exp(1j * th)   # dz along the semicircle
+    c64 = A.chains_run(op, specs, zc, "edc", 0.0, "hull", "fp64")["g"]
+    c32 = A.chains_run(op, specs, zc, "edc", 0.0, "hull", "fp32")["g"]
+    q64 = -np.imag(np.sum(wc[:, None] * c64, axis=0)) / np.pi
+    q32 = -np.imag(np.sum(wc[:, None] * c32, axis=0)) / np.pi
+    mixed["charge_error"] = float(np.max(np.abs(q32 - q64)))
+    mixed["error_basis"] = ("max |DOS32 - DOS64| / max DOS64 over 54 groups x 192 real-axis energies; max |M0_32 - M0_64| "
+                            "of the 48-node contour charge per group")
+    out["mixed"] = mixed
+    # adjoint: forward + reverse sweep of all groups over the 48 contour energies, seeds = contour charge weights
+    w = np.repeat(wc[:, None], len(specs), axis=1)
+    A.chains_adjoint(op, specs, zc[:8], w[:8], "hull", "fp64", True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    _, grad = A.chains_adjoint(op, specs, zc, w, "hull", "fp64", True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    msa = e0.elapsed_time(e1)
+    e0.record(stream)
+    A.chains_run(op, specs, zc, "edc", 0.0, "hull", "fp64")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    msf = e0.elapsed_time(e1)
+    steps_adj = int(depth.sum()) * zc.shape[0]
+    out["adjoint"] = {"value": steps_adj / (msa / 1000.0), "unit": "chain-steps/s (forward + reverse, checkpoints every "
+                      "sqrt(depth) levels)", "forward_same_energies": steps_adj / (msf / 1000.0),
+                      "adjoint_over_forward_time": msa / msf, "energies": int(zc.shape[0]), "groups": len(specs),
+                      "gradient_norm": float(np.linalg.norm(grad))}
+    out["fp64_peak_tflops"] = fp64_peak_tflops(torch)
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -205,9 +290,9 @@ def main():
         start = ((it * world + rank) * nzs) % (nall - nzs + 1)
         return start
 
-    def step(it):
+    def step(it, precision=args.precision):
         s0 = slice_of(it)
-        A.chains_run_device(op, specs, z_dev[s0:s0 + nzs].data_ptr(), g_dev.data_ptr(), nzs, "edc", 0.0, "hull", args.precision)
+        A.chains_run_device(op, specs, z_dev[s0:s0 + nzs].data_ptr(), g_dev.data_ptr(), nzs, "edc", 0.0, "hull", precision)
         if world > 1:
             out = torch.empty(world * g_dev.numel(), dtype=g_dev.dtype, device="cuda")
             dist.all_gather_into_tensor(out, g_dev)
@@ -259,6 +344,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_e2e = float(t.item())
     e2e = total_steps / (ms_e2e / 1000.0)
+    legs = run_legs(args, A, op, specs, groups, z_all, step, stream, world) if args.legs else None
     nsp = 3
     h2d = nzs * 16 + len(specs) * 6 * 9 * nsp * 8
     d2h = len(specs) * nzs * (16 + 4)
@@ -274,6 +360,10 @@ def main():
         achieved = (ks["bytes"] / max(ks["launches"], 1)) / (per_launch_ms / 1000.0) / 1e9
         tflops = (ks["flops"] / max(ks["launches"], 1)) / (per_launch_ms / 1000.0) / 1e12
         cpu = cpu_baseline(case, fl, groups, z_all) if args.cpu_sample else None
+        traffic = None
+        if args.precision in NCU_STEP_TRAFFIC:
+            meas, alg = NCU_STEP_TRAFFIC[args.precision]
+            traffic = meas * (ks["bytes"] / max(ks["launches"], 1)) / alg
         line = {
             "metric": "chain-steps/s (batched energy-dependent chains, fcc ternary, 54 groups, depths 16-28)",
             "value": value, "unit": "chain-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -288,10 +378,13 @@ def main():
                        "precision": args.precision},
             "e2e": {"value": e2e, "unit": "chain-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "traffic": None, "kernel": "chain step operator (k_smul, fused S + diagonal + dot)",
+                         "traffic": traffic, "kernel": "chain step operator (k_smul, fused S + diagonal + dot)",
                          "per_launch_ms": per_launch_ms, "launches": ks["launches"], "fp64_tflops": tflops,
-                         "share_of_step": ks["ms"] / ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
+                         "share_of_step": ks["ms"] / ms, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)",
+                         "fp64_frac": (tflops / legs["fp64_peak_tflops"]) if legs else None,
+                         "fp64_peak_source": "cuBLAS DGEMM 8192^3 measured in this run"},
             "cpu_baseline": cpu,
+            "legs": legs,
             "gpu_launches": int(launches),
             "clocks": clocks,
         }
