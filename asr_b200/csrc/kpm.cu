@@ -24,6 +24,7 @@ struct asr_supercell {
   int* d_nbr = nullptr;          // (ns, n) 0-based
   uint8_t* d_spc = nullptr;      // (n) 0-based species
   double* d_par = nullptr;       // c, d, o, e: 4 x (9, nsp)
+  std::vector<double> par_h;     // host copy of the same
   double* d_blocks = nullptr;    // [1 + ns][l][l']
   float* d_blocks_f = nullptr;
 };
@@ -127,6 +128,127 @@ __global__ void __launch_bounds__(KSITES * KV) k_cheb(ScView S, const ST* __rest
     for (int r = 1; r < KSITES; ++r) { rt += red[r][v][0]; tt += red[r][v][1]; tp += red[r][v][2]; }
     double* out = part + ((size_t)blockIdx.x * KV + v) * 3;
     out[0] = rt; out[1] = tt; out[2] = tp;
+  }
+}
+
+// acc += B[l][.] . x for one padded block row (12 entries, the last 3 zero): vector loads from shared memory.  The
+// loads are volatile so that they stay next to their use: hoisting all 27 rows of a block ahead of the multiplies
+// (what the compiler does otherwise) costs 80 registers a thread and halves the occupancy.
+__device__ __forceinline__ float4 lds_f4(const float* p) {
+  float4 r;
+  unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ld.volatile.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w) : "r"(a));
+  return r;
+}
+__device__ __forceinline__ double2 lds_d2(const double* p) {
+  double2 r;
+  unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ld.volatile.shared.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "r"(a));
+  return r;
+}
+__device__ __forceinline__ float row9(const float* __restrict__ row, const float* x, float acc) {
+  float4 a = lds_f4(row), b = lds_f4(row + 4), c = lds_f4(row + 8);
+  acc = fmaf(a.x, x[0], acc); acc = fmaf(a.y, x[1], acc); acc = fmaf(a.z, x[2], acc); acc = fmaf(a.w, x[3], acc);
+  acc = fmaf(b.x, x[4], acc); acc = fmaf(b.y, x[5], acc); acc = fmaf(b.z, x[6], acc); acc = fmaf(b.w, x[7], acc);
+  return fmaf(c.x, x[8], acc);
+}
+__device__ __forceinline__ double row9(const double* __restrict__ row, const double* x, double acc) {
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    double2 a = lds_d2(row + 2 * q);
+    acc = fma(a.x, x[2 * q], acc);
+    if (q < 4) acc = fma(a.y, x[2 * q + 1], acc);
+  }
+  return acc;
+}
+constexpr int KRW = 12;   // padded block row (16-byte aligned)
+
+// Chebyshev step for o = 0 on d-scaled vectors u = d o t (per site and orbital, d of the site's species): with
+// h t = c t + d S (d t), the recurrence t' = 2 (H t - cen t) / sc - t_old becomes
+//   u' = 2 ((c + e - cen) o u + d^2 o S u) / sc - u_old,
+// so the gathered neighbour rows need neither their species nor a scaling.  Partial dots of t (weights 1/d^2, 1/d):
+// part[blk][v] = (r . t', t' . t', t' . t).  The next slot's neighbour index and row are loaded while the current slot
+// is multiplied.
+struct UCoef {
+  const double* cc;   // (c + e - cen) per (orbital, species)
+  const double* d2;   // d^2
+  const double* w2;   // 1 / d^2
+  const double* w1;   // 1 / d
+};
+
+template <typename ST, bool WANT_R>
+__global__ void __launch_bounds__(KSITES * KV, sizeof(ST) == 8 ? 3 : 0) k_cheb_u(ScView S, const ST* __restrict__ blocks, const double* __restrict__ coef,
+                                                        const ST* __restrict__ u, const ST* __restrict__ uold,
+                                                        ST* __restrict__ unew, double isc, bool first, uint64_t seed, int v0,
+                                                        double* part) {
+  extern __shared__ unsigned char sm_raw[];
+  const int np = 9 * S.nsp;
+  double* cs = (double*)sm_raw;                 // cc | d2 | w2 | w1
+  ST* Bs = (ST*)(cs + 4 * np);                  // [1 + ns][9][KRW]
+  for (int q = threadIdx.x; q < 4 * np; q += blockDim.x) cs[q] = coef[q];
+  for (int q = threadIdx.x; q < (S.ns + 1) * 9 * KRW; q += blockDim.x) {
+    int c = q % KRW, r = q / KRW;
+    Bs[q] = c < 9 ? blocks[r * 9 + c] : (ST)0;
+  }
+  __syncthreads();
+  const int v = threadIdx.x % KV, row = threadIdx.x / KV;
+  double rt = 0.0, tt = 0.0, tp = 0.0;
+  for (int i = blockIdx.x * KSITES + row; i < S.n; i += gridDim.x * KSITES) {
+    ST acc[9], xa[9], xb[9], uo[9];
+    for (int l = 0; l < 9; ++l) acc[l] = (ST)0;
+    const ST* ui = u + (size_t)i * 9 * KV + v;
+    for (int l = 0; l < 9; ++l) uo[l] = ui[l * KV];
+    const int* nb = S.nbr + (size_t)S.ns * i;
+    int jn = S.ns > 0 ? nb[0] : 0;
+    if (S.ns > 0) { const ST* src = u + (size_t)jn * 9 * KV + v; for (int l = 0; l < 9; ++l) xa[l] = src[l * KV]; }
+    // on-site block
+    for (int l = 0; l < 9; ++l) acc[l] = row9(Bs + l * KRW, uo, acc[l]);
+#pragma unroll 1
+    for (int k = 0; k < S.ns; ++k) {
+      if (k + 1 < S.ns) {
+        jn = nb[k + 1];
+        const ST* src = u + (size_t)jn * 9 * KV + v;
+        for (int l = 0; l < 9; ++l) xb[l] = src[l * KV];
+      }
+      const ST* Bk = Bs + (size_t)(k + 1) * 9 * KRW;
+      for (int l = 0; l < 9; ++l) acc[l] = row9(Bk + l * KRW, xa, acc[l]);
+      for (int l = 0; l < 9; ++l) xa[l] = xb[l];
+    }
+    const int si = S.spc[i];
+    ST* uni = unew + (size_t)i * 9 * KV + v;
+    const ST* uoi = first ? nullptr : uold + (size_t)i * 9 * KV + v;
+    for (int l = 0; l < 9; ++l) {
+      const int q = l + 9 * si;
+      double y = cs[q] * (double)uo[l] + cs[np + q] * (double)acc[l];
+      double un = first ? y * isc : 2.0 * y * isc - (double)uoi[l * KV];
+      ST us = (ST)un;
+      uni[l * KV] = us;
+      double ur = (double)us;
+      tt += cs[2 * np + q] * ur * ur;
+      tp += cs[2 * np + q] * ur * (double)uo[l];
+      if (WANT_R) rt += rademacher(seed, (uint64_t)(v0 + v), (uint64_t)i * 9 + l) * ur * cs[3 * np + q];
+    }
+  }
+  __shared__ double red[KSITES][KV][3];
+  red[row][v][0] = rt; red[row][v][1] = tt; red[row][v][2] = tp;
+  __syncthreads();
+  if (row == 0) {
+    for (int r = 1; r < KSITES; ++r) { rt += red[r][v][0]; tt += red[r][v][1]; tp += red[r][v][2]; }
+    double* out = part + ((size_t)blockIdx.x * KV + v) * 3;
+    out[0] = rt; out[1] = tt; out[2] = tp;
+  }
+}
+
+// u_0 = d o r (d of each site's species)
+template <typename ST>
+__global__ void k_rademacher_init_scaled(ScView S, uint64_t seed, int v0, ST* t) {
+  size_t tot = (size_t)S.n * 9 * KV;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (size_t)gridDim.x * blockDim.x) {
+    int v = (int)(q % KV);
+    size_t e = q / KV;   // site * 9 + l
+    int site = (int)(e / 9), l = (int)(e % 9);
+    double d = S.par[9 * S.nsp + l + 9 * S.spc[site]];
+    t[q] = (ST)(d * rademacher(seed, (uint64_t)(v0 + v), (uint64_t)e));
   }
 }
 
@@ -240,16 +362,44 @@ int kpm_run(asr_ctx* ctx, asr_supercell* sc, double cen, double scl, int nmom, i
   const double isc = 1.0 / scl;
   const double dim = 9.0 * n;
   std::vector<double> hred((size_t)nsteps * KV * 3);
+  // coefficients of the d-scaled recurrence (o = 0): c + e - cen, d^2, 1/d^2, 1/d per (orbital, species)
+  DevBuf<double> ucoef;
+  const size_t smem_u = 4 * 9 * sc->nsp * sizeof(double) + (size_t)(sc->ns + 1) * 9 * KRW * sizeof(ST);
+  bool dpos = true;
+  if (!general) {
+    const int np = 9 * sc->nsp;
+    std::vector<double> hc(4 * (size_t)np);
+    for (int q = 0; q < np; ++q) {
+      double c = sc->par_h[q], d = sc->par_h[np + q], e = sc->par_h[3 * np + q];
+      if (d == 0.0) dpos = false;
+      hc[q] = c + e - cen;
+      hc[np + q] = d * d;
+      hc[2 * np + q] = d != 0.0 ? 1.0 / (d * d) : 0.0;
+      hc[3 * np + q] = d != 0.0 ? 1.0 / d : 0.0;
+    }
+    if (dpos) {
+      ASR_TRY(ucoef.alloc(hc.size()));
+      ASR_CUDA(cudaMemcpyAsync(ucoef.p, hc.data(), hc.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+  }
+  const bool scaled = !general && dpos;
   for (int vb = 0; vb < nvec; vb += KV) {
     const int nv = std::min(KV, nvec - vb);
-    k_rademacher_init<ST><<<ctx->num_sms * 8, 256, 0, s>>>(n, seed, v0 + vb, T0.p);
+    if (scaled) k_rademacher_init_scaled<ST><<<ctx->num_sms * 8, 256, 0, s>>>(S, seed, v0 + vb, T0.p);
+    else k_rademacher_init<ST><<<ctx->num_sms * 8, 256, 0, s>>>(n, seed, v0 + vb, T0.p);
     ST *ta = T0.p, *tb = T1.p, *tc = T2.p;   // t_{k-1}, t_k, t_{k+1}
     // step 0: t_1 = (H t_0 - cen t_0) / sc
     for (int k = 0; k < nsteps; ++k) {
       const ST* tin = (k == 0) ? ta : tb;
       const ST* told = (k == 0) ? nullptr : ta;
       ST* tout = (k == 0) ? tb : tc;
-      if (!general) {
+      if (scaled) {
+        // <r|t> is needed for every step without doubling, and for mu_1 (step 0) with it
+        if (!doubling || k == 0)
+          k_cheb_u<ST, true><<<grid, KSITES * KV, smem_u, s>>>(S, blocks, ucoef.p, tin, told, tout, isc, k == 0, seed, v0 + vb, part.p);
+        else
+          k_cheb_u<ST, false><<<grid, KSITES * KV, smem_u, s>>>(S, blocks, ucoef.p, tin, told, tout, isc, k == 0, seed, v0 + vb, part.p);
+      } else if (!general) {
         k_cheb<ST><<<grid, KSITES * KV, smem, s>>>(S, blocks, tin, told, tout, cen, isc, k == 0, !sc->e_zero, seed, v0 + vb, part.p);
       } else {
         k_h<ST><<<grid, KSITES * KV, smem, s>>>(S, blocks, tin, false, W1.p);
@@ -342,6 +492,7 @@ int asr_supercell_build(asr_ctx* ctx, int nsite, int nslot, const int* nbr, cons
   cudaMemcpyAsync(sc->d_nbr, nb.data(), nb.size() * sizeof(int), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(sc->d_spc, sp.data(), nsite, cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(sc->d_par, par.data(), par.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+  sc->par_h = par;
   cudaMemcpyAsync(sc->d_blocks, B.data(), B.size() * sizeof(double), cudaMemcpyHostToDevice, s);
   cudaMemcpyAsync(sc->d_blocks_f, Bf.data(), Bf.size() * sizeof(float), cudaMemcpyHostToDevice, s);
   ASR_CUDA(cudaStreamSynchronize(s));

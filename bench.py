@@ -190,6 +190,83 @@ def fp64_peak_tflops(torch):
     return 2.0 * n ** 3 / (best / 1000.0) / 1e12
 
 
+def kpm_leg(torch):
+    """KPM on the explicit supercell: fcc 40^3 conventional cells (256,000 sites, 12 NN + 6 NNN slots), species
+    Fe/Ni/Cr-like 0.66 / 0.14 / 0.20 placed by seeded Metropolis swaps towards alpha_1 = -0.10, h = c + d S d; 2048
+    Chebyshev moments over 64 Rademacher vectors (two moments per matvec), FP32 matvec and vectors with FP64 moments,
+    timed, against the FP64 run (moment and Jackson-DOS error)."""
+    from asr_b200 import kpm, synthetic as S
+    t0 = time.perf_counter()
+    nbr, spc, bvec, aout = kpm.fcc_supercell(40, [0.66, 0.14, 0.20], -0.10, seed=4, sweeps=4)
+    block, block0 = S.sk_blocks(bvec, 4)
+    c, d, o, e = S.plain_params(S.draw_species(3, 4))
+    sc = kpm.Supercell(nbr, spc, c, d, o, e, block, block0)
+    setup_s = time.perf_counter() - t0
+    # spectral bound: |H| <= max|c| + max d^2 sum_slots |B_k|_inf + |B_0|_inf
+    bn = sum(np.max(np.sum(np.abs(block[:, :, k]), axis=1)) for k in range(block.shape[2]))
+    bound = np.max(np.abs(c)) + np.max(d) ** 2 * (bn + np.max(np.sum(np.abs(block0), axis=1)))
+    cen, scl = 0.0, 1.05 * bound
+    nmom, nvec = 2048, 64
+    out = {"sites": int(sc.n), "rows": int(sc.dim), "moments": nmom, "vectors": nvec, "setup_s": setup_s,
+           "alpha1_achieved": float(aout[0, 1])}
+    sc.kpm_moments(cen, scl, 64, nvec, seed=5, precision="fp32")
+    torch.cuda.synchronize()
+    for prec in ("fp32", "fp64"):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        mu = sc.kpm_moments(cen, scl, nmom, nvec, seed=5, precision=prec)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[prec] = {"ms": ms, "matvec_rows_per_s": (nmom // 2) * nvec * sc.dim / (ms / 1000.0),
+                     "tflops": (nmom // 2) * nvec * sc.n * 2.0 * 81 * (1 + sc.ns) / (ms / 1000.0) / 1e12}
+        out["mu_" + prec] = mu
+    m32, m64 = out.pop("mu_fp32"), out.pop("mu_fp64")
+    egrid = np.linspace(cen - 0.99 * scl, cen + 0.99 * scl, 2000)
+    r32, r64 = kpm.kpm_dos(m32, cen, scl, egrid), kpm.kpm_dos(m64, cen, scl, egrid)
+    out["moment_error"] = float(np.max(np.abs(m32 - m64)))
+    out["dos_error"] = float(np.max(np.abs(r32 - r64)) / np.max(np.abs(r64)))
+    # algorithmic bytes per vector and Chebyshev step: 3 FP32 streams x 36 B + 1 B species per site
+    out["fp32"]["hbm_gbs_algorithmic"] = (nmom // 2) * nvec * sc.n * (3 * 36 + 1) / (out["fp32"]["ms"] / 1000.0) / 1e9
+    sc.free()
+    return out
+
+
+def plain_leg(torch):
+    """The CPU-runnable plain configuration: bcc A0.5B0.5 on one site class, D2h, levels 4, rank 1, 9 real chains of
+    depth 12 (one per start orbital), Beer-Pettifor tail, G at 2000 real energies (Im z = 0.005): device time of the
+    whole call and its DOS against the oracle's lanczos + terminated_green on the same operator."""
+    import asr_b200 as A
+    from asr_b200 import synthetic as S
+    from oracle import oracle as O
+    case = S.cubic_case("bcc", 4, 2, [0.5, 0.5], seed=0, group="d2h")
+    fl = np.ones(case["graph"].n, np.int32)
+    op = A.build_augcls_operator(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, 4, maxrank=1,
+                                 flippable=fl)
+    c, d, o, e = S.plain_params(S.draw_species(2, 0))
+    specs = [A.ChainSpec(c=c, d=d, o=o, e=e, start_orb=l0, nlev=12) for l0 in range(1, 10)]
+    z = np.linspace(-1.5, 1.0, 2000) + 0.005j
+    A.chains_run(op, specs, z, mode="plain", tail="bp")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    g = A.chains_run(op, specs, z, mode="plain", tail="bp")["g"]
+    ms = (time.perf_counter() - t0) * 1000.0
+    oop = O.OracleOp(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, 4, 1, fl)
+    oop.set_params(c, d, o, e)
+    t0 = time.perf_counter()
+    err = 0.0
+    for l0 in range(1, 10):
+        oop.set_start(l0)
+        v0 = np.zeros(oop.dim)
+        v0[l0 - 1] = 1.0
+        ao, bo, no = oop.lanczos(v0, 12)
+        go, _ = O.terminated_green(ao, bo, no, z, "beer-pettifor")
+        err = max(err, float(np.max(np.abs(g[:, l0 - 1].imag - go.imag)) / np.pi))
+    ms_cpu = (time.perf_counter() - t0) * 1000.0
+    return {"nodes": int(op.nn), "chains": 9, "depth": 12, "energies": 2000, "ms": ms, "oracle_ms_1thread": ms_cpu,
+            "dos_abs_error_vs_oracle": err}
+
+
 def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
     """The mixed-precision leg (FP32 matvec and vectors, FP64 coefficients and fractions) with its DOS and charge error
     against the FP64 run, and the adjoint leg (forward plus reverse sweep) on the contour energies."""
@@ -248,6 +325,8 @@ def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
                       "adjoint_over_forward_time": msa / msf, "energies": int(zc.shape[0]), "groups": len(specs),
                       "gradient_norm": float(np.linalg.norm(grad))}
     out["fp64_peak_tflops"] = fp64_peak_tflops(torch)
+    out["kpm"] = kpm_leg(torch)
+    out["plain"] = plain_leg(torch)
     return out
 
 
