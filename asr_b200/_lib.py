@@ -29,7 +29,7 @@ EXPORTS = ["asr_version", "asr_last_error", "asr_ctx_create", "asr_ctx_destroy",
            "asr_op_free", "asr_op_dims", "asr_op_export_tables", "asr_op_set_params", "asr_op_freeze_site", "asr_op_unfreeze",
            "asr_op_set_start", "asr_op_set_chi", "asr_op_set_class_conc", "asr_op_apply", "asr_op_rand_c", "asr_op_project_c",
            "asr_chains_run", "asr_chains_run_dev", "asr_cf_eval", "asr_cf_adjoint",
-    "asr_chains_adjoint", "asr_cf_eval_noalloc", "asr_supercell_build", "asr_supercell_free",
+    "asr_chains_adjoint", "asr_cf_eval_noalloc", "asr_ed3_blocks", "asr_supercell_build", "asr_supercell_free",
            "asr_supercell_apply", "asr_kpm_moments", "asr_kpm_dos", "asr_sro_layout", "asr_gauss_legendre", "asr_contour_nodes",
            "asr_contour_nodes_closed", "asr_contour_nodes_fermi", "asr_contour_moment"]
 
@@ -37,6 +37,12 @@ EXPORTS = ["asr_version", "asr_last_error", "asr_ctx_create", "asr_ctx_destroy",
 class ChainGroup(C.Structure):
     """asr_chain_group of include/asr_b200.h."""
     _fields_ = [("c", d_p), ("d", d_p), ("o", d_p), ("e", d_p), ("pa", d_p), ("pb", d_p), ("frozen_sp", C.c_int),
+                ("start_orb", C.c_int), ("nlev", C.c_int), ("reserved", C.c_int)]
+
+
+class Ed3Group(C.Structure):
+    """asr_ed3_group of include/asr_b200.h."""
+    _fields_ = [("g", d_p), ("d", d_p), ("dc", d_p), ("dl", d_p), ("enu", d_p), ("o", d_p), ("p", d_p), ("central", C.c_int),
                 ("start_orb", C.c_int), ("nlev", C.c_int), ("reserved", C.c_int)]
 
 
@@ -84,6 +90,11 @@ def lib():
                                      C.c_int, vp, d_p, d_p, i_p]
     L.asr_cf_eval.argtypes = [vp, d_p, d_p, i_p, C.c_int, C.c_int, d_p, C.c_int, C.c_int, d_p, d_p, i64_p]
     L.asr_cf_adjoint.argtypes = [d_p, d_p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_double, C.c_double, d_p, d_p, d_p]
+    L.asr_cf_eval_noalloc.argtypes = [vp, d_p, d_p, i_p, C.c_int, C.c_int, d_p, C.c_int, C.c_int, d_p, i64_p]
+    L.asr_chains_adjoint.argtypes = [vp, vp, C.POINTER(ChainGroup), C.c_int, d_p, C.c_int, d_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     d_p, d_p]
+    L.asr_ed3_blocks.argtypes = [vp, vp, C.POINTER(Ed3Group), C.c_int, d_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, d_p,
+                                 i_p, d_p, d_p, d_p]
     L.asr_supercell_build.argtypes = [vp, C.c_int, C.c_int, i_p, i_p, C.c_int, d_p, d_p, d_p, d_p, d_p, d_p, C.POINTER(vp)]
     L.asr_supercell_free.argtypes = [vp]
     L.asr_supercell_apply.argtypes = [vp, d_p, d_p, C.c_int]

@@ -100,6 +100,36 @@ def chains_adjoint(op: AugclsOp, specs, z, w, tail: str = "hull", precision: str
     return g.T, grad
 
 
+def ed3_blocks(op: AugclsOp, groups, z, depth_tol: float = 0.0, tail: str = "hull", precision: str = "fp64",
+               project: bool = True, coefs: bool = False):
+    """``ed3_blocks`` (src/asr_ed3.f90:242-265) for every group at every energy.  groups: dicts with g, d, o, p, dl, enu
+    ((9, nsp) each), dc (9), central, start_orb, nlev (``synthetic.ed3_params`` builds them).  Returns dict(bk=(4, nz, ngroup)
+    complex: G_11, (hG)_11, (hGh)_11, q1 mismatch; m=(2, nz, ngroup) depths of the |a> and |v> chains; a, b, c =
+    (nlevmax, 2, nz, ngroup) if coefs)."""
+    z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
+    nz, ng = z.shape[0], len(groups)
+    arr = (_lib.Ed3Group * ng)()
+    keep = []
+    for q, gr in enumerate(groups):
+        vals = {}
+        for k in ("g", "d", "dc", "dl", "enu", "o", "p"):
+            a = _f64(gr[k])
+            keep.append(a)
+            vals[k] = _pd(a)
+        arr[q] = _lib.Ed3Group(vals["g"], vals["d"], vals["dc"], vals["dl"], vals["enu"], vals["o"], vals["p"], int(gr["central"]),
+                               int(gr["start_orb"]), int(gr["nlev"]), 0)
+    nlevmax = max(int(gr["nlev"]) for gr in groups)
+    bk = np.zeros((ng, nz, 4), np.complex128)
+    m = np.zeros((ng, nz, 2), np.int32)
+    cf = [np.zeros((ng, nz, 2, nlevmax), np.complex128) for _ in range(3)] if coefs else [None] * 3
+    check(lib().asr_ed3_blocks(op.ctx.h, op.h, arr, ng, _pd(z), nz, float(depth_tol), _lib.TAILS[tail], PREC[precision],
+                               int(bool(project)), _pd(bk), _pi(m), *[_pd(x) if x is not None else None for x in cf]))
+    out = dict(bk=bk.transpose(2, 1, 0), m=m.transpose(2, 1, 0))
+    if coefs:
+        out["a"], out["b"], out["c"] = (x.transpose(3, 2, 1, 0) for x in cf)
+    return out
+
+
 def chains_run_device(op: AugclsOp, specs, z_dev, g_dev, nz: int, mode: str = "edc", depth_tol: float = 0.0, tail: str = "hull",
                       precision: str = "fp64", project: bool = True):
     """Device-resident form: z_dev / g_dev are device pointers (ints, e.g. torch tensor data_ptr()) of complex128 arrays;

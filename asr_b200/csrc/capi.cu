@@ -88,6 +88,9 @@ bool all_zero(const double* p, int n) {
 }
 
 // one group: parameters -> blob + info
+int make_group_slots(const asr_op* op, const GroupLayout& GL, const double* const* P, int frozen_sp, int l0, int nlev,
+                     const double* chi_override, double* blob, GroupInfo& gi);
+
 int make_group(const asr_op* op, const GroupLayout& GL, const double* c, const double* d, const double* o, const double* e,
                const double* pa, const double* pb, int frozen_sp, int l0, int nlev, const double* chi_override, double* blob,
                GroupInfo& gi) {
@@ -98,6 +101,13 @@ int make_group(const asr_op* op, const GroupLayout& GL, const double* c, const d
   P[PA] = pa ? pa : zero.data(); P[PB] = pb ? pb : zero.data();
   for (int q = 0; q < np; ++q) { ceb[q] = P[PC][q] + P[PE][q] + P[PB][q]; eb[q] = P[PE][q] + P[PB][q]; }
   P[PCEB] = ceb.data(); P[PEB] = eb.data();
+  return make_group_slots(op, GL, P, frozen_sp, l0, nlev, chi_override, blob, gi);
+}
+
+// weights and flags of a group from the raw parameter arrays of every blob slot (9, nsp each)
+int make_group_slots(const asr_op* op, const GroupLayout& GL, const double* const* P, int frozen_sp, int l0, int nlev,
+                     const double* chi_override, double* blob, GroupInfo& gi) {
+  const int np = 9 * op->nsp;
   for (int p = 0; p < NPAR; ++p) {
     weights(op, P[p], blob + GL.w(p));
     for (int q = 0; q < np; ++q) blob[GL.raw(p) + q] = P[p][q];
@@ -649,6 +659,83 @@ static int chains_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups
     ctx->nchain += ngroup;
   }
   ctx->nlev += nsteps;
+  ctx->nfall += nfall;
+  return ASR_OK;
+}
+
+int asr_ed3_blocks(asr_ctx* ctx, asr_op* op, const asr_ed3_group* groups, int ngroup, const double* z, int nz, double depth_tol,
+                   int tail, int precision, int project, double* bk, int* mused, double* a, double* b, double* c) {
+  if (!ctx || !op || !groups || ngroup < 1 || nz < 1 || !z || !bk) { set_error("asr_ed3_blocks: bad argument"); return ASR_EINVAL; }
+  if (tail < 0 || tail > 3) { set_error("asr_ed3_blocks: unknown tail"); return ASR_EINVAL; }
+  ASR_TRY(set_device(ctx));
+  const int nsp = op->nsp, np = 9 * nsp;
+  GroupLayout GL = layout(op);
+  std::vector<double> blob((size_t)GL.stride * ngroup, 0.0), oc(ngroup);
+  std::vector<GroupInfo> gi(ngroup);
+  int nlevmax = 0;
+  for (int q = 0; q < ngroup; ++q) {
+    const asr_ed3_group& G = groups[q];
+    if (!G.g || !G.d || !G.dc || !G.del || !G.enu || !G.o || !G.p) { set_error("asr_ed3_blocks: group %d incomplete", q + 1); return ASR_EINVAL; }
+    if (G.nlev < 1 || G.nlev > NLMAX) { set_error("asr_ed3_blocks: depth %d out of range 1..%d", G.nlev, NLMAX); return ASR_EINVAL; }
+    if (G.central < 1 || G.central > nsp) { set_error("asr_ed3_blocks: central species out of range"); return ASR_EINVAL; }
+    if (G.start_orb < 1 || G.start_orb > 9) { set_error("asr_ed3_blocks: start orbital out of range"); return ASR_EINVAL; }
+    // ed3_coefs (:91-107) as z-linear coefficients (the cf of ed3_blocks_blk, :281-288): et = z ea + eb, u = z ua + ub,
+    // Qt = z qa + qb
+    std::vector<double> ea(np), eb(np), ua(np), ub(np), qa(np), qb(np);
+    for (int sp = 0; sp < nsp; ++sp)
+      for (int l = 0; l < 9; ++l) {
+        int k = l + 9 * sp;
+        double r = G.dc[l] / G.del[k];
+        ea[k] = r; eb[k] = -r * G.enu[k];
+        ua[k] = G.o[k]; ub[k] = -G.o[k] * G.enu[k];
+        qa[k] = -G.p[k] / r; qb[k] = (G.o[k] + G.p[k] * G.enu[k]) / r;
+      }
+    const double* P[NPAR];
+    P[PC] = G.g; P[PD] = G.d; P[PO] = ea.data(); P[PE] = eb.data(); P[PA] = ua.data(); P[PB] = ub.data();
+    P[PCEB] = qa.data(); P[PEB] = qb.data();
+    ASR_TRY(make_group_slots(op, GL, P, G.central, G.start_orb, G.nlev, nullptr, blob.data() + (size_t)GL.stride * q, gi[q]));
+    oc[q] = G.o[(G.start_orb - 1) + 9 * (size_t)(G.central - 1)];
+    nlevmax = std::max(nlevmax, G.nlev);
+  }
+  const int nlane = 2 * ngroup * nz;
+  std::vector<int> lg(nlane), lk(nlane);
+  std::vector<double2> lz(nlane);
+  for (int q = 0; q < ngroup; ++q)
+    for (int j = 0; j < nz; ++j)
+      for (int kd = 0; kd < 2; ++kd) {
+        size_t L = 2 * ((size_t)q * nz + j) + kd;
+        lg[L] = q; lk[L] = kd; lz[L] = make_double2(z[2 * j], z[2 * j + 1]);
+      }
+  std::vector<double2> g, f, ha, hb, hc;
+  std::vector<double> na, nv;
+  std::vector<int> m;
+  int64_t nfall = 0;
+  int rc = run_ed3(ctx, op, gi, blob, GL, oc, lg, lk, lz, depth_tol, tail, project, precision, g, f, na, nv, m, a ? &ha : nullptr,
+                   b ? &hb : nullptr, c ? &hc : nullptr, &nfall);
+  if (rc != ASR_OK) return rc;
+  for (int q = 0; q < ngroup; ++q)
+    for (int j = 0; j < nz; ++j) {
+      size_t LA = 2 * ((size_t)q * nz + j), LV = LA + 1;
+      double2 q0 = cscale(g[LA], na[LA] * na[LA]), q1a = cscale(f[LA], na[LA]);
+      double2 q2 = cscale(g[LV], nv[LV] * nv[LV]), q1b = cscale(f[LV], nv[LV]);
+      double2 fm = cscale(cadd(q1a, q1b), 0.5);
+      double o = oc[q];
+      double2 out[4] = {cadd(csub(q0, cscale(fm, 2.0 * o)), cscale(q2, o * o)), csub(fm, cscale(q2, o)), q2, csub(q1a, q1b)};
+      for (int k = 0; k < 4; ++k) {
+        size_t dst = 2 * (4 * ((size_t)j + (size_t)nz * q) + k);
+        bk[dst] = out[k].x;
+        bk[dst + 1] = out[k].y;
+      }
+      if (mused) { mused[2 * (j + (size_t)nz * q)] = m[LA]; mused[2 * (j + (size_t)nz * q) + 1] = m[LV]; }
+      for (int kd = 0; kd < 2; ++kd)
+        for (int k = 0; k < nlevmax; ++k) {
+          size_t src = (LA + kd) * NLMAX + k, dst = 2 * ((LA + kd) * nlevmax + k);
+          if (a) { a[dst] = ha[src].x; a[dst + 1] = ha[src].y; }
+          if (b) { b[dst] = hb[src].x; b[dst + 1] = hb[src].y; }
+          if (c) { c[dst] = hc[src].x; c[dst + 1] = hc[src].y; }
+        }
+    }
+  ctx->nchain += nlane;
   ctx->nfall += nfall;
   return ASR_OK;
 }

@@ -24,15 +24,15 @@ __host__ __device__ inline int cs_tridiag_eig(int n, double2* d, double2* e) {
     for (;;) {
       int m;
       for (m = l; m < n - 1; ++m) {
-        double dd = cabs2(d[m]) + cabs2(d[m + 1]);
-        if (cabs2(e[m]) <= DBL_EPSILON * dd || cabs2(e[m]) == 0.0) break;
+        double dd = cmag(d[m]) + cmag(d[m + 1]);
+        if (cmag(e[m]) <= DBL_EPSILON * dd || cmag(e[m]) == 0.0) break;
       }
       if (m == l) break;
       if (++iter > 60) return 1;
       double2 g = cdiv(csub(d[l + 1], d[l]), cscale(e[l], 2.0));
       double2 r = csqrt_p(cadd(cmul(g, g), make_double2(1.0, 0.0)));
       double2 gp = cadd(g, r), gm = csub(g, r);
-      double2 den = cabs2(gp) >= cabs2(gm) ? gp : gm;
+      double2 den = cmag(gp) >= cmag(gm) ? gp : gm;
       g = cadd(csub(d[m], d[l]), cdiv(e[l], den));
       double2 s = make_double2(1.0, 0.0), c = make_double2(1.0, 0.0), p = make_double2(0.0, 0.0);
       bool early = false;
@@ -40,7 +40,7 @@ __host__ __device__ inline int cs_tridiag_eig(int n, double2* d, double2* e) {
         double2 f = cmul(s, e[i]), b = cmul(c, e[i]);
         r = csqrt_p(cadd(cmul(f, f), cmul(g, g)));
         e[i + 1] = r;
-        if (cabs2(r) == 0.0) {
+        if (cmag(r) == 0.0) {
           d[i + 1] = csub(d[i + 1], p);
           e[m] = make_double2(0.0, 0.0);
           early = true;
@@ -80,10 +80,10 @@ __host__ __device__ inline int chain_extremes(const double2* a, const double2* b
   return 0;
 }
 
-// cf_species: g11 of the chain (a, b) of depth m at z with the tail (0 none, 1 hull, 2 bp, 3 avg2).  wd, we: work (m).
-__host__ __device__ inline double2 cf_species_dev(const double2* a, const double2* b, int m, double2 z, int tail, double2* wd,
-                                                  double2* we, int* nfall, double2* edges) {
-  double2 aa, bb;
+// tail parameters (aa, bb) of cf_species (src/asr_chain.f90:80-101): hull extremes, Beer-Pettifor fixed point, avg2 or
+// none.  wd, we: work (m).
+__host__ __device__ inline void cf_tail_dev(const double2* a, const double2* b, int m, int tail, double2* wd, double2* we,
+                                            int* nfall, double2& aa, double2& bb) {
   bool ok = false;
   double2 lo, hi;
   if (m >= 2 && tail != 0) ok = chain_extremes(a, b, m, a[m - 1], wd, we, lo, hi) == 0;
@@ -97,7 +97,7 @@ __host__ __device__ inline double2 cf_species_dev(const double2* a, const double
         if (chain_extremes(a, b, m, cadd(a[m - 1], bb), wd, we, l1, h1)) { if (nfall) ++*nfall; done = true; break; }
         if (chain_extremes(a, b, m, csub(a[m - 1], bb), wd, we, l2, h2)) { if (nfall) ++*nfall; done = true; break; }
         double2 an = cscale(cadd(h1, l2), 0.5), bn = cscale(csub(h1, l2), 0.25);
-        if (cabs2(csub(an, aa)) + cabs2(csub(bn, bb)) < 1.0e-12 * (1.0 + cabs2(bn))) { aa = an; bb = bn; done = true; break; }
+        if (cmag(csub(an, aa)) + cmag(csub(bn, bb)) < 1.0e-12 * (1.0 + cmag(bn))) { aa = an; bb = bn; done = true; break; }
         aa = an;
         bb = bn;
       }
@@ -117,19 +117,53 @@ __host__ __device__ inline double2 cf_species_dev(const double2* a, const double
     bb = csqrt_p(cscale(cadd(cmul(b[m - 2], b[m - 2]), cmul(b[m - 3], b[m - 3])), 0.5));
   }
   if (tail == 0) { aa = make_double2(0.0, 0.0); bb = make_double2(0.0, 0.0); }
-  if (edges) { edges[0] = aa; edges[1] = bb; }
-  double2 d = csub(z, aa), tl;
-  if (cabs2(bb) < 1.0e-14) tl = make_double2(0.0, 0.0);
-  else {
+}
+
+// the square-root terminator of the tail (aa, bb) at z, on the branch with |bb g| minimal (src/asr_chain.f90:103-110)
+__host__ __device__ inline double2 cf_tail_term(double2 z, double2 aa, double2 bb) {
+  double2 d = csub(z, aa), tl = make_double2(0.0, 0.0);
+  if (cmag(bb) >= 1.0e-14) {   // |bb| < 1e-14: no tail
     double2 bb2 = cmul(bb, bb);
     double2 s = csqrt_p(csub(cmul(d, d), cscale(bb2, 4.0)));
     double2 g1 = cdiv(csub(d, s), cscale(bb2, 2.0)), g2 = cdiv(cadd(d, s), cscale(bb2, 2.0));
-    tl = cabs2(cmul(bb, g1)) <= cabs2(cmul(bb, g2)) ? cmul(bb2, g1) : cmul(bb2, g2);
+    tl = cmag(cmul(bb, g1)) <= cmag(cmul(bb, g2)) ? cmul(bb2, g1) : cmul(bb2, g2);
   }
+  return tl;
+}
+
+// cf_species: g11 of the chain (a, b) of depth m at z with the tail (0 none, 1 hull, 2 bp, 3 avg2).  wd, we: work (m).
+__host__ __device__ inline double2 cf_species_dev(const double2* a, const double2* b, int m, double2 z, int tail, double2* wd,
+                                                  double2* we, int* nfall, double2* edges) {
+  double2 aa, bb;
+  cf_tail_dev(a, b, m, tail, wd, we, nfall, aa, bb);
+  if (edges) { edges[0] = aa; edges[1] = bb; }
+  double2 tl = cf_tail_term(z, aa, bb);
   double2 one = make_double2(1.0, 0.0);
   double2 gt = cdiv(one, csub(csub(z, a[m - 1]), tl));
   for (int j = m - 2; j >= 0; --j) gt = cdiv(one, csub(csub(z, a[j]), cmul(cmul(b[j], b[j]), gt)));
   return gt;
+}
+
+// cf_species with the projection f = sum_k c_k prod_{j<k} (b_j gt_{j+1}) gt_1 (src/asr_chain.f90:111-122); closed: the exact
+// fraction without tail (cf_closed, src/asr_ed3.f90:221-236).  gt: work (m); wd, we: work (m).
+__host__ __device__ inline double2 cf_species_f_dev(const double2* a, const double2* b, const double2* c, int m, double2 z, int tail,
+                                                    bool closed, double2* gt, double2* wd, double2* we, int* nfall, double2& f) {
+  double2 tl = make_double2(0.0, 0.0);
+  if (!closed) {
+    double2 aa, bb;
+    cf_tail_dev(a, b, m, tail, wd, we, nfall, aa, bb);
+    tl = cf_tail_term(z, aa, bb);
+  }
+  double2 one = make_double2(1.0, 0.0);
+  gt[m - 1] = cdiv(one, csub(csub(z, a[m - 1]), tl));
+  for (int j = m - 2; j >= 0; --j) gt[j] = cdiv(one, csub(csub(z, a[j]), cmul(cmul(b[j], b[j]), gt[j + 1])));
+  f = make_double2(0.0, 0.0);
+  double2 prod = gt[0];
+  for (int k = 0; k < m; ++k) {
+    f = cadd(f, cmul(c[k], prod));
+    if (k < m - 1) prod = cmul(prod, cmul(b[k], gt[k + 1]));
+  }
+  return gt[0];
 }
 
 // ---- real chains (plain mode)
@@ -190,7 +224,7 @@ __host__ __device__ inline double2 terminated_green_dev(const double* a, const d
     double2 s = csqrt_p(csub(cmul(w, w), make_double2(4.0 * binf * binf, 0.0)));
     double d2 = 2.0 * binf * binf;
     double2 g1 = cscale(csub(w, s), 1.0 / d2), g2 = cscale(cadd(w, s), 1.0 / d2);
-    double2 g = cabs2(g1) <= cabs2(g2) ? g1 : g2;
+    double2 g = cmag(g1) <= cmag(g2) ? g1 : g2;
     tl = cscale(g, binf * binf);
   }
   double2 one = make_double2(1.0, 0.0);
@@ -209,14 +243,14 @@ __host__ __device__ inline int tridiag_solve_shift(int m, const double2* a, cons
   // (T - lam) x = rhs, Thomas algorithm on the complex symmetric tridiagonal (no pivoting; lam is perturbed off the
   // eigenvalue by the caller)
   double2 dd = csub(a[0], lam);
-  if (cabs2(dd) == 0.0) dd = make_double2(1e-300, 0.0);
+  if (cmag(dd) == 0.0) dd = make_double2(1e-300, 0.0);
   wd[0] = dd;
   x[0] = rhs[0];
   for (int j = 1; j < m; ++j) {
     double2 l = cdiv(b[j - 1], wd[j - 1]);
     we[j - 1] = l;
     double2 d = csub(csub(a[j], lam), cmul(l, b[j - 1]));
-    if (cabs2(d) == 0.0) d = make_double2(1e-300, 0.0);
+    if (cmag(d) == 0.0) d = make_double2(1e-300, 0.0);
     wd[j] = d;
     x[j] = csub(rhs[j], cmul(l, x[j - 1]));
   }
@@ -229,13 +263,13 @@ __host__ __device__ inline void eig_grad(int m, const double2* a, const double2*
                                          double2* bbar, double2* v, double2* t, double2* wd, double2* we) {
   // eigenvector by two steps of inverse iteration at a shift next to lam, then dlam/da_j = v_j^2 / (v.v)
   double sc = 0.0;
-  for (int j = 0; j < m; ++j) sc = fmax(sc, cabs2(a[j]) + (j < m - 1 ? cabs2(b[j]) : 0.0));
+  for (int j = 0; j < m; ++j) sc = fmax(sc, cmag(a[j]) + (j < m - 1 ? cmag(b[j]) : 0.0));
   double2 mu = cadd(lam, make_double2(1e-10 * (sc + 1.0), 1e-10 * (sc + 1.0)));
   for (int j = 0; j < m; ++j) t[j] = make_double2(1.0 / sqrt((double)m), 0.0);
   for (int it = 0; it < 3; ++it) {
     tridiag_solve_shift(m, a, b, mu, t, v, wd, we);
     double nr = 0.0;
-    for (int j = 0; j < m; ++j) nr = fmax(nr, cabs2(v[j]));
+    for (int j = 0; j < m; ++j) nr = fmax(nr, cmag(v[j]));
     for (int j = 0; j < m; ++j) t[j] = cscale(v[j], 1.0 / nr);
   }
   double2 vv = make_double2(0.0, 0.0);
@@ -267,12 +301,12 @@ __host__ __device__ inline double2 cf_species_adjoint(const double2* a, const do
   }
   double2 d = csub(z, aa), tl = make_double2(0, 0), sroot = make_double2(0, 0);
   double sig = 0.0;
-  bool has_tail = cabs2(bb) >= 1.0e-14;
+  bool has_tail = cmag(bb) >= 1.0e-14;
   if (has_tail) {
     double2 bb2 = cmul(bb, bb);
     sroot = csqrt_p(csub(cmul(d, d), cscale(bb2, 4.0)));
     double2 g1 = cdiv(csub(d, sroot), cscale(bb2, 2.0)), g2 = cdiv(cadd(d, sroot), cscale(bb2, 2.0));
-    if (cabs2(cmul(bb, g1)) <= cabs2(cmul(bb, g2))) { tl = cmul(bb2, g1); sig = 1.0; }
+    if (cmag(cmul(bb, g1)) <= cmag(cmul(bb, g2))) { tl = cmul(bb2, g1); sig = 1.0; }
     else { tl = cmul(bb2, g2); sig = -1.0; }
   }
   double2 one = make_double2(1.0, 0.0);

@@ -55,22 +55,23 @@ __device__ __forceinline__ size_t vix(int tile, int nn, int node, int l) {
   return (((size_t)tile * nn + node) * 9 + l) * TL;
 }
 
-// complex weight of the diagonal term p (+ X(z) if withx) for (l, own, flip) of class kap
-__device__ __forceinline__ double2 pweight(const double* gb, const GroupLayout& GL, int p, bool withx, double2 z, int nsm,
+// complex weight W_p + z W_pz (pz < 0: none) of the diagonal term for (l, own, flip) of class kap; the edc route's
+// X(z) = z pa + pb enters as pz = PA
+__device__ __forceinline__ double2 pweight(const double* gb, const GroupLayout& GL, int p, int pz, double2 z, int nsm,
                                            int kap, int own, int flip, int l) {
   int q = ((kap * nsm + own) * nsm + flip) * 9 + l;
   double w = p >= 0 ? __ldg(gb + GL.w(p) + q) : 0.0;
-  if (withx) {
-    double wa = __ldg(gb + GL.w(PA) + q);
+  if (pz >= 0) {
+    double wa = __ldg(gb + GL.w(pz) + q);
     return make_double2(w + z.x * wa, z.y * wa);
   }
   return make_double2(w, 0.0);
 }
-__device__ __forceinline__ double2 praw(const double* gb, const GroupLayout& GL, int p, bool withx, double2 z, int sp, int l) {
+__device__ __forceinline__ double2 praw(const double* gb, const GroupLayout& GL, int p, int pz, double2 z, int sp, int l) {
   int q = (sp - 1) * 9 + l;
   double w = p >= 0 ? __ldg(gb + GL.raw(p) + q) : 0.0;
-  if (withx) {
-    double wa = __ldg(gb + GL.raw(PA) + q);
+  if (pz >= 0) {
+    double wa = __ldg(gb + GL.raw(pz) + q);
     return make_double2(w + z.x * wa, z.y * wa);
   }
   return make_double2(w, 0.0);
@@ -83,16 +84,16 @@ __device__ __forceinline__ int frozen_of(const OpView& op, const GroupInfo& gi, 
 // vector v (unscaled, amplitude coordinates); xi_own: the node's own values of v.
 template <typename T2>
 __device__ __forceinline__ void rand_term(const OpView& op, const GroupInfo& gi, const double* gb, const GroupLayout& GL, int p,
-                                          bool withx, double2 z, const T2* v, int tile, int i, int lane, double2* out,
+                                          int pz, double2 z, const T2* v, int tile, int i, int lane, double2* out,
                                           const double2* xi_own) {
   int fs = frozen_of(op, gi, i);
   if (fs > 0) {
-    for (int l = 0; l < 9; ++l) out[l] = cmul(praw(gb, GL, p, withx, z, fs, l), xi_own[l]);
+    for (int l = 0; l < 9; ++l) out[l] = cmul(praw(gb, GL, p, pz, z, fs, l), xi_own[l]);
     return;
   }
   const int nsm = op.nsmax;
   int kap = op.ncl[i], l0 = op.lst[i];
-  for (int l = 0; l < 9; ++l) out[l] = cmul(pweight(gb, GL, p, withx, z, nsm, kap, l0, l0, l), xi_own[l]);
+  for (int l = 0; l < 9; ++l) out[l] = cmul(pweight(gb, GL, p, pz, z, nsm, kap, l0, l0, l), xi_own[l]);
   int nk = op.nsc[kap];
   for (int k = 0; k < nk; ++k) {
     if (k == l0) continue;
@@ -105,7 +106,7 @@ __device__ __forceinline__ void rand_term(const OpView& op, const GroupInfo& gi,
       int pl = op.pi[g * 9 + l];
       double2 x = ld(v + vix(tile, op.nn, r, pl) + lane);
       double sgn = (((sgm >> l) & 1u) ^ (neg ? 1u : 0u)) ? -1.0 : 1.0;
-      out[l] = cadd(out[l], cmul(pweight(gb, GL, p, withx, z, nsm, kap, l0, k, l), cscale(x, sgn)));
+      out[l] = cadd(out[l], cmul(pweight(gb, GL, p, pz, z, nsm, kap, l0, k, l), cscale(x, sgn)));
     }
   }
 }
@@ -262,9 +263,9 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
         double2 ui = ld(in + vix(it.tile, bv.nn, i, l) + lane);
         double2 pt;
         if (fs > 0) {
-          pt = cmul(praw(gb, bv.GL, PCEB, withx, z, fs, l), ui);
+          pt = cmul(praw(gb, bv.GL, PCEB, withx ? PA : -1, z, fs, l), ui);
         } else {
-          pt = cmul(pweight(gb, bv.GL, PCEB, withx, z, nsm, kap, l0, l0, l), ui);
+          pt = cmul(pweight(gb, bv.GL, PCEB, withx ? PA : -1, z, nsm, kap, l0, l0, l), ui);
           for (int k = 0; k < nk; ++k) {
             if (k == l0) continue;
             int r = op.flipr[k + nsm * i];
@@ -272,7 +273,7 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
             const unsigned long long pw = piw[op.flipg[k + nsm * i]];
             int p = (int)((pw >> (4 * l)) & 15ull);
             double2 xr = flip_if(ld(in + vix(it.tile, bv.nn, r, p) + lane), (uint32_t)((pw >> (40 + l)) & 1ull));
-            pt = cadd(pt, cmul(pweight(gb, bv.GL, PCEB, withx, z, nsm, kap, l0, k, l), xr));
+            pt = cadd(pt, cmul(pweight(gb, bv.GL, PCEB, withx ? PA : -1, z, nsm, kap, l0, k, l), xr));
           }
         }
         double2 y = cmul(s, cadd(make_double2(acc[l].x, acc[l].y), pt));
@@ -303,7 +304,7 @@ __global__ void __launch_bounds__(WPB * TL) k_rand(OpView op, BatchView bv, int 
     if (i >= bv.nn) break;
     double2 xi[9], o[9];
     for (int l = 0; l < 9; ++l) xi[l] = ld(in + vix(it.tile, bv.nn, i, l) + lane);
-    rand_term(op, gi, gb, bv.GL, p, false, make_double2(0, 0), in, it.tile, i, lane, o, xi);
+    rand_term(op, gi, gb, bv.GL, p, -1, make_double2(0, 0), in, it.tile, i, lane, o, xi);
     for (int l = 0; l < 9; ++l) stv(out + vix(it.tile, bv.nn, i, l) + lane, o[l]);
   }
 }
@@ -337,20 +338,20 @@ __global__ void __launch_bounds__(WPB * TL) k_combine(OpView op, BatchView bv, c
         if (t2) {
           for (int l = 0; l < 9; ++l) xi[l] = ld(t2 + vix(it.tile, bv.nn, i, l) + lane);
           if (gi.flags & GF_D_UNIFORM) for (int l = 0; l < 9; ++l) acc[l] = cscale(xi[l], gi.dd[l]);
-          else rand_term(op, gi, gb, bv.GL, PD, false, z, t2, it.tile, i, lane, acc, xi);
+          else rand_term(op, gi, gb, bv.GL, PD, -1, z, t2, it.tile, i, lane, acc, xi);
         } else {
           for (int l = 0; l < 9; ++l) acc[l] = make_double2(0, 0);
         }
         if (v1) {
           for (int l = 0; l < 9; ++l) xi[l] = ld(v1 + vix(it.tile, bv.nn, i, l) + lane);
-          rand_term(op, gi, gb, bv.GL, pB, bx, z, v1, it.tile, i, lane, tmp, xi);
+          rand_term(op, gi, gb, bv.GL, pB, bx ? PA : -1, z, v1, it.tile, i, lane, tmp, xi);
           for (int l = 0; l < 9; ++l) acc[l] = cadd(acc[l], tmp[l]);
         }
         for (int l = 0; l < 9; ++l) acc[l] = cscale(acc[l], sgnAB);
         double2 ui[9];
         for (int l = 0; l < 9; ++l) ui[l] = ld(u + vix(it.tile, bv.nn, i, l) + lane);
         if (cterm) {
-          rand_term(op, gi, gb, bv.GL, PEB, !(gi.flags & GF_X_ZERO), z, u, it.tile, i, lane, tmp, ui);
+          rand_term(op, gi, gb, bv.GL, PEB, (gi.flags & GF_X_ZERO) ? -1 : PA, z, u, it.tile, i, lane, tmp, ui);
           for (int l = 0; l < 9; ++l) acc[l] = cadd(acc[l], tmp[l]);
         }
         if (h1) for (int l = 0; l < 9; ++l) acc[l] = cadd(acc[l], ld(h1 + vix(it.tile, bv.nn, i, l) + lane));
@@ -475,7 +476,7 @@ __global__ void k_reduce_a(BatchView bv, const double2* part, int bpt, int k) {
     double2 gtry = cf_species_dev(bv.acoef + (size_t)L * NLMAX, bv.bcoef + (size_t)L * NLMAX, k, bv.lane_z[L], bv.tail, wd, we,
                                   &nf, nullptr);
     if (nf) atomicAdd(bv.nfall, nf);
-    if (k > 8 && cabs2(csub(gtry, bv.gprev[L])) <= bv.depth_tol * cabs2(gtry)) go = false;
+    if (k > 8 && cmag(csub(gtry, bv.gprev[L])) <= bv.depth_tol * cmag(gtry)) go = false;   // :123-125
     bv.gprev[L] = gtry;
   }
   if (go) bv.lane_wact[L] = 1;
@@ -494,8 +495,9 @@ __global__ void k_reduce_b(BatchView bv, const double2* part, int bpt, int k, do
     for (int q = 0; q < bpt; ++q) ww = cadd(ww, part[((size_t)tile * bpt + q) * TL + lane]);
     double2 b = bv.mode == ASR_MODE_PLAIN ? make_double2(sqrt(ww.x), 0.0) : csqrt_p(ww);
     bv.bcoef[(size_t)L * NLMAX + k - 1] = b;
-    bool ok = bv.mode == ASR_MODE_PLAIN ? (b.x >= btol) : (cabs2(b) >= btol);
+    bool ok = bv.mode == ASR_MODE_PLAIN ? (b.x >= btol) : (cmag(b) >= btol);   // |b| < 1e-12 ends the chain
     if (!bv.lane_act[L]) ok = false;   // plain chain at its last level: b_n stored, chain done
+    else if (!ok && bv.lane_closed) bv.lane_closed[L] = 1;   // the Krylov space is exhausted
     if (ok) {
       bv.sup[L] = bv.su[L];
       bv.su[L] = cdiv(make_double2(1.0, 0.0), b);
@@ -1035,7 +1037,7 @@ struct AdjScal {
 __device__ __forceinline__ double2 scale_of(const AdjScal& S, int L, int k) {   // s_k: u_k = s_k X_k
   if (k <= 1) return make_double2(k == 1 ? 1.0 : 0.0, 0.0);
   double2 b = S.b[(size_t)L * NLMAX + k - 2];
-  if (cabs2(b) == 0.0 || k > S.m[L]) return make_double2(0, 0);
+  if (cmag(b) == 0.0 || k > S.m[L]) return make_double2(0, 0);
   return cdiv(make_double2(1.0, 0.0), b);
 }
 __global__ void k_adj_scal(AdjScal S, int nlane, const int* lane_group, int k, int phase) {
@@ -1327,6 +1329,410 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   return ASR_OK;
 }
 
+// ================================================================================================ route ed3
+// src/asr_ed3.f90: chains on H_eff = z - K'(z), K' = et - h' + u h' + h' u - h' Qt h', h' = g + d S d, with
+// et = z ea + eb, u = z ua + ub, Qt = z qa + qb per (orbital, species) in the blob slots
+//   PC = g, PD = d, PO = ea, PE = eb, PA = ua, PB = ub, PCEB = qa, PEB = qb.
+// Two chains per (group, energy): kind 0 from |a>/|a| with projection vector |v>, kind 1 from |v>/|v| with |a>, where
+// |v> = h'|e> (projected) and |a> = |e> + o_c |v>.  Lanes L = 2 (group-energy index) + kind.
+enum { E3_G = PC, E3_D = PD, E3_EA = PO, E3_EB = PE, E3_UA = PA, E3_UB = PB, E3_QA = PCEB, E3_QB = PEB };
+
+// T3 = R_u(U) - R_Qt(T1)
+template <typename ST>
+__global__ void __launch_bounds__(WPB * TL) k_ed3_t3(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ U,
+                                                     const typename St2<ST>::T* __restrict__ T1, typename St2<ST>::T* __restrict__ T3,
+                                                     int npw) {
+  NodeIter it;
+  int bpt;
+  if (!node_iter(bv, npw, it, bpt)) return;
+  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
+  const int L = it.tile * TL + lane;
+  const int grp = bv.lane_group[L];
+  if (grp < 0) return;
+  const GroupInfo gi = bv.ginfo[grp];
+  const double* gb = bv.gblob + (size_t)grp * bv.GL.stride;
+  const double2 z = bv.lane_z[L];
+  for (int qn = 0; qn < npw; ++qn) {
+    int i = it.first + w + WPB * qn;
+    if (i >= bv.nn) break;
+    double2 xu[9], xt[9], o1[9], o2[9];
+    for (int l = 0; l < 9; ++l) {
+      size_t q = vix(it.tile, bv.nn, i, l) + lane;
+      xu[l] = ld(U + q);
+      xt[l] = ld(T1 + q);
+    }
+    rand_term(op, gi, gb, bv.GL, E3_UB, E3_UA, z, U, it.tile, i, lane, o1, xu);
+    rand_term(op, gi, gb, bv.GL, E3_QB, E3_QA, z, T1, it.tile, i, lane, o2, xt);
+    for (int l = 0; l < 9; ++l) stv(T3 + vix(it.tile, bv.nn, i, l) + lane, csub(o1[l], o2[l]));
+  }
+}
+
+// Y = s (z U - K'U) with K'U = R_et(U) - T1 + R_u(T1) + h'(T3), h'(T3) = R_g(T3) + d o T3a (T3a = S d T3); partials
+// a = sum norb (s U) . Y and c = sum norb TV . (s U)
+template <typename ST>
+__global__ void __launch_bounds__(WPB * TL) k_ed3_w(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ U,
+                                                    const typename St2<ST>::T* __restrict__ T1,
+                                                    const typename St2<ST>::T* __restrict__ T3,
+                                                    const typename St2<ST>::T* __restrict__ T3a,
+                                                    const typename St2<ST>::T* __restrict__ TV, typename St2<ST>::T* __restrict__ Y,
+                                                    double2* part_a, double2* part_c, int npw) {
+  NodeIter it;
+  int bpt;
+  if (!node_iter(bv, npw, it, bpt)) return;
+  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
+  const int L = it.tile * TL + lane;
+  const int grp = bv.lane_group[L];
+  double2 da = make_double2(0, 0), dc = make_double2(0, 0);
+  if (grp >= 0) {
+    const GroupInfo gi = bv.ginfo[grp];
+    const double* gb = bv.gblob + (size_t)grp * bv.GL.stride;
+    const double2 z = bv.lane_z[L], s = bv.su[L];
+    for (int qn = 0; qn < npw; ++qn) {
+      int i = it.first + w + WPB * qn;
+      if (i >= bv.nn) break;
+      double2 xu[9], xt1[9], xt3[9], r1[9], r2[9], r3[9], r4[9];
+      for (int l = 0; l < 9; ++l) {
+        size_t q = vix(it.tile, bv.nn, i, l) + lane;
+        xu[l] = ld(U + q);
+        xt1[l] = ld(T1 + q);
+        xt3[l] = ld(T3 + q);
+      }
+      rand_term(op, gi, gb, bv.GL, E3_EB, E3_EA, z, U, it.tile, i, lane, r1, xu);     // et U
+      rand_term(op, gi, gb, bv.GL, E3_UB, E3_UA, z, T1, it.tile, i, lane, r2, xt1);   // u T1
+      rand_term(op, gi, gb, bv.GL, E3_G, -1, z, T3, it.tile, i, lane, r3, xt3);       // g T3
+      if (gi.flags & GF_D_UNIFORM) {
+        for (int l = 0; l < 9; ++l) r4[l] = cscale(ld(T3a + vix(it.tile, bv.nn, i, l) + lane), gi.dd[l]);
+      } else {
+        double2 xa[9];
+        for (int l = 0; l < 9; ++l) xa[l] = ld(T3a + vix(it.tile, bv.nn, i, l) + lane);
+        rand_term(op, gi, gb, bv.GL, E3_D, -1, z, T3a, it.tile, i, lane, r4, xa);
+      }
+      const double norb = op.sq[i] * op.sq[i];
+      double2 en = make_double2(0, 0), ec = make_double2(0, 0);
+      for (int l = 0; l < 9; ++l) {
+        size_t q = vix(it.tile, bv.nn, i, l) + lane;
+        double2 kx = cadd(csub(r1[l], xt1[l]), cadd(r2[l], cadd(r3[l], r4[l])));
+        double2 y = cmul(s, csub(cmul(z, xu[l]), kx));
+        stv(Y + q, y);
+        double2 su_ = cmul(s, xu[l]);
+        en = cadd(en, cmul(su_, y));
+        ec = cadd(ec, cmul(ld(TV + q), su_));
+      }
+      da = cadd(da, cscale(en, norb));
+      dc = cadd(dc, cscale(ec, norb));
+    }
+  }
+  block_reduce_store(da, part_a, it.tile, bpt);
+  __syncthreads();
+  block_reduce_store(dc, part_c, it.tile, bpt);
+}
+
+// a_k, c_k and the depth test of src/asr_ed3.f90:173-179 (g and the projection f)
+__global__ void k_ed3_reduce_a(BatchView bv, const double2* part_a, const double2* part_c, int bpt, int k, double2* ccoef,
+                               double2* fprev, const double* tnorm) {
+  int tile = blockIdx.x, lane = threadIdx.x;
+  if (tile >= bv.ntile || !bv.tile_act[tile]) return;
+  int L = tile * TL + lane;
+  int grp = bv.lane_group[L];
+  bv.lane_wact[L] = 0;
+  if (grp < 0 || !bv.lane_act[L]) return;
+  double2 a = make_double2(0, 0), c = make_double2(0, 0);
+  for (int q = 0; q < bpt; ++q) {
+    a = cadd(a, part_a[((size_t)tile * bpt + q) * TL + lane]);
+    c = cadd(c, part_c[((size_t)tile * bpt + q) * TL + lane]);
+  }
+  bv.acur[L] = a;
+  bv.acoef[(size_t)L * NLMAX + k - 1] = a;
+  ccoef[(size_t)L * NLMAX + k - 1] = c;
+  bv.lane_m[L] = k;
+  int nlev = bv.ginfo[grp].nlev;
+  bool go = k < nlev;
+  if (go && bv.depth_tol > 0.0 && k >= 8 && k % 4 == 0) {
+    double2 gt[NLMAX], wd[NLMAX], we[NLMAX], f;
+    int nf = 0;
+    double2 g = cf_species_f_dev(bv.acoef + (size_t)L * NLMAX, bv.bcoef + (size_t)L * NLMAX, ccoef + (size_t)L * NLMAX, k,
+                                 bv.lane_z[L], bv.tail, false, gt, wd, we, &nf, f);
+    if (nf) atomicAdd(bv.nfall, nf);
+    if (k > 8) {
+      double ag = cmag(g), af = cmag(f);
+      if (cmag(csub(g, bv.gprev[L])) <= bv.depth_tol * ag && cmag(csub(f, fprev[L])) <= bv.depth_tol * fmax(af, tnorm[L] * ag))
+        go = false;
+    }
+    bv.gprev[L] = g;
+    fprev[L] = f;
+  }
+  if (go) bv.lane_wact[L] = 1;
+  else bv.lane_act[L] = 0;
+}
+
+// |v>.|v> and |a>.|a> (|a> = |e> + o_c |v>, |e> the start orbital at node 0) per lane: two partial arrays
+template <typename ST>
+__global__ void __launch_bounds__(WPB * TL) k_ed3_dots(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ VV,
+                                                       const double* oc, double2* part_v, double2* part_a, int npw) {
+  NodeIter it;
+  int bpt;
+  if (!node_iter(bv, npw, it, bpt)) return;
+  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
+  const int L = it.tile * TL + lane;
+  const int grp = bv.lane_group[L];
+  double2 dv = make_double2(0, 0), da = make_double2(0, 0);
+  if (grp >= 0) {
+    const int l0 = bv.ginfo[grp].l0 - 1;
+    const double o = oc[grp];
+    for (int qn = 0; qn < npw; ++qn) {
+      int i = it.first + w + WPB * qn;
+      if (i >= bv.nn) break;
+      double2 ev = make_double2(0, 0), ea = make_double2(0, 0);
+      for (int l = 0; l < 9; ++l) {
+        double2 v = ld(VV + vix(it.tile, bv.nn, i, l) + lane);
+        double2 a = cscale(v, o);
+        if (i == 0 && l == l0) a.x += 1.0;
+        ev = cadd(ev, cmul(v, v));
+        ea = cadd(ea, cmul(a, a));
+      }
+      double nb = op.sq[i] * op.sq[i];
+      dv = cadd(dv, cscale(ev, nb));
+      da = cadd(da, cscale(ea, nb));
+    }
+  }
+  block_reduce_store(dv, part_v, it.tile, bpt);
+  __syncthreads();
+  block_reduce_store(da, part_a, it.tile, bpt);
+}
+
+// start vectors: kind 0: U = |a> / na, TV = |v>; kind 1: U = |v> / nv, TV = |a>; UP = 0
+template <typename ST>
+__global__ void k_ed3_start(BatchView bv, const typename St2<ST>::T* __restrict__ VV, const double* oc, const int* kind,
+                            const double* na, const double* nv, typename St2<ST>::T* U, typename St2<ST>::T* UP,
+                            typename St2<ST>::T* TV) {
+  size_t n = (size_t)bv.ntile * bv.nn * 9 * TL;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    int lane = (int)(q % TL);
+    size_t rest = q / TL;
+    int l = (int)(rest % 9);
+    size_t nt = rest / 9;
+    int node = (int)(nt % bv.nn);
+    int tile = (int)(nt / bv.nn);
+    int L = tile * TL + lane;
+    int grp = bv.lane_group[L];
+    double2 u = make_double2(0, 0), t = make_double2(0, 0);
+    if (grp >= 0) {
+      double2 v = ld(VV + q);
+      double2 a = cscale(v, oc[grp]);
+      if (node == 0 && l == bv.ginfo[grp].l0 - 1) a.x += 1.0;
+      if (kind[L] == 0) { u = cscale(a, 1.0 / na[L]); t = v; }
+      else { u = cscale(v, 1.0 / nv[L]); t = a; }
+    }
+    stv(U + q, u);
+    stv(UP + q, make_double2(0, 0));
+    stv(TV + q, t);
+  }
+}
+
+// final fractions of every lane: g and the projection f (cf_species or, for a closed chain, cf_closed)
+__global__ void k_ed3_final(BatchView bv, int nlane, const int* lmap, const double2* ccoef, const int* closed, double2* g,
+                            double2* f) {
+  int L = blockIdx.x * blockDim.x + threadIdx.x;
+  if (L >= nlane) return;
+  int dst = lmap[L];
+  if (bv.lane_group[L] < 0 || dst < 0) return;
+  int m = bv.lane_m[L];
+  double2 gt[NLMAX], wd[NLMAX], we[NLMAX], ff = make_double2(0, 0), gg = make_double2(0, 0);
+  int nf = 0;
+  if (m > 0)
+    gg = cf_species_f_dev(bv.acoef + (size_t)L * NLMAX, bv.bcoef + (size_t)L * NLMAX, ccoef + (size_t)L * NLMAX, m, bv.lane_z[L],
+                          bv.tail, closed[L] != 0, gt, wd, we, &nf, ff);
+  if (nf) atomicAdd(bv.nfall, nf);
+  g[dst] = gg;
+  f[dst] = ff;
+}
+
+template <typename ST>
+int run_ed3_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+              const GroupLayout& GL, const std::vector<double>& oc, const std::vector<int>& lane_group,
+              const std::vector<int>& lane_kind, const std::vector<double2>& lane_z, double depth_tol, int tail, int project,
+              std::vector<double2>& g_out, std::vector<double2>& f_out, std::vector<double>& na_out, std::vector<double>& nv_out,
+              std::vector<int>& m_out, std::vector<double2>* a_out, std::vector<double2>* b_out, std::vector<double2>* c_out,
+              int64_t* nfall_out) {
+  typedef typename St2<ST>::T T2;
+  cudaStream_t s = ctx->stream;
+  const int nn = op->nn, nlane = (int)lane_group.size();
+  bool dunif = true;
+  for (auto& g : ginfo) {
+    if (!(g.flags & GF_D_UNIFORM)) dunif = false;
+    if (g.nlev > NLMAX) { set_error("ed3: depth %d above %d", g.nlev, NLMAX); return ASR_EINVAL; }
+  }
+  std::vector<std::vector<int>> tiles;
+  {
+    std::vector<std::vector<int>> per_group(ginfo.size());
+    for (int L = 0; L < nlane; ++L) per_group[lane_group[L]].push_back(L);
+    for (auto& lst : per_group)
+      for (size_t q = 0; q < lst.size(); q += TL)
+        tiles.emplace_back(lst.begin() + q, lst.begin() + std::min(lst.size(), q + (size_t)TL));
+  }
+  const int ntile_all = (int)tiles.size();
+  const size_t vec_bytes = (size_t)nn * 9 * TL * sizeof(T2);
+  const int nvec = 8;   // U, UP, Y (rotating), T1, T3, Sa (S d x), TMP (d x), TV
+  size_t freeb = 0, totb = 0;
+  cudaMemGetInfo(&freeb, &totb);
+  int tpb = std::is_same<ST, double>::value ? 16 : 8;
+  while (tpb > 1 && (size_t)tpb * nvec * vec_bytes > freeb / 2) tpb /= 2;
+  if ((size_t)nvec * vec_bytes > freeb) { set_error("ed3: %d vectors of %zu bytes do not fit", nvec, vec_bytes); return ASR_ENOMEM; }
+  tpb = std::min(tpb, ntile_all);
+  const int npw = 4, npb = WPB * npw, bpt = (nn + npb - 1) / npb;
+  const int nlp = tpb * TL;
+  Dev<double> d_gblob, d_oc, d_na, d_nv, d_tn;
+  Dev<GroupInfo> d_ginfo;
+  ASR_TRY(d_gblob.alloc(gblob.size())); ASR_TRY(d_ginfo.alloc(ginfo.size())); ASR_TRY(d_oc.alloc(oc.size()));
+  ASR_CUDA(cudaMemcpyAsync(d_gblob.p, gblob.data(), gblob.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_ginfo.p, ginfo.data(), ginfo.size() * sizeof(GroupInfo), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_oc.p, oc.data(), oc.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  ASR_TRY(d_na.alloc(nlp)); ASR_TRY(d_nv.alloc(nlp)); ASR_TRY(d_tn.alloc(nlp));
+  Dev<int> d_lgroup, d_act, d_wact, d_m, d_tact, d_nfall, d_tgroup, d_kind, d_closed, d_lmap;
+  Dev<double2> d_a, d_b, d_c, d_gprev, d_fprev, d_acur, d_bprev, d_su, d_sup, d_part, d_part2, d_z, d_g, d_f, d_sv, d_sa;
+  ASR_TRY(d_lgroup.alloc(nlp)); ASR_TRY(d_act.alloc(nlp)); ASR_TRY(d_wact.alloc(nlp)); ASR_TRY(d_m.alloc(nlp));
+  ASR_TRY(d_tact.alloc(tpb)); ASR_TRY(d_nfall.alloc(1)); ASR_TRY(d_tgroup.alloc(tpb)); ASR_TRY(d_kind.alloc(nlp));
+  ASR_TRY(d_closed.alloc(nlp)); ASR_TRY(d_lmap.alloc(nlp));
+  ASR_TRY(d_a.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_b.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_c.alloc((size_t)nlp * NLMAX));
+  ASR_TRY(d_gprev.alloc(nlp)); ASR_TRY(d_fprev.alloc(nlp)); ASR_TRY(d_acur.alloc(nlp)); ASR_TRY(d_bprev.alloc(nlp));
+  ASR_TRY(d_su.alloc(nlp)); ASR_TRY(d_sup.alloc(nlp)); ASR_TRY(d_z.alloc(nlp)); ASR_TRY(d_g.alloc(nlane)); ASR_TRY(d_f.alloc(nlane));
+  ASR_TRY(d_part.alloc((size_t)tpb * bpt * TL)); ASR_TRY(d_part2.alloc((size_t)tpb * bpt * TL));
+  ASR_TRY(d_sv.alloc(nlp)); ASR_TRY(d_sa.alloc(nlp));
+  const size_t vlen = (size_t)tpb * nn * 9 * TL;
+  std::vector<Dev<T2>> V(nvec);
+  for (int q = 0; q < nvec; ++q) ASR_TRY(V[q].alloc(vlen));
+  T2 *T1 = V[3].p, *T3 = V[4].p, *SA = V[5].p, *TMP = V[6].p, *TV = V[7].p;
+  OpView ov = op->view();
+  const ST* blk = std::is_same<ST, double>::value ? (const ST*)op->d_blocks : (const ST*)op->d_blocks_f;
+  const size_t sm = smul_smem(op, sizeof(ST));
+  g_out.assign(nlane, make_double2(0, 0));
+  f_out.assign(nlane, make_double2(0, 0));
+  na_out.assign(nlane, 0.0);
+  nv_out.assign(nlane, 0.0);
+  m_out.assign(nlane, 0);
+  if (a_out) a_out->assign((size_t)nlane * NLMAX, make_double2(0, 0));
+  if (b_out) b_out->assign((size_t)nlane * NLMAX, make_double2(0, 0));
+  if (c_out) c_out->assign((size_t)nlane * NLMAX, make_double2(0, 0));
+  std::vector<int> hgroup(nlp), lmap(nlp), hkind(nlp), hm(nlp);
+  std::vector<double2> hz(nlp), hab((size_t)nlp * NLMAX);
+  std::vector<double> hna(nlp), hnv(nlp);
+  std::vector<double2> ones(nlp, make_double2(1.0, 0.0));
+  ASR_CUDA(cudaMemsetAsync(d_nfall.p, 0, sizeof(int), s));
+  // apply h' = g + d S d to x (raw): Sa = S d x (TMP for a species-dependent d), out = R_g x + d o Sa
+  auto apply_hp = [&](const BatchView& bv, int grid, T2* x, T2* out) -> int {
+    apply_SD<ST>(op, bv, dunif, x, TMP, SA, d_part.p, npw, grid, s);
+    k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, SA, x, E3_G, false, x, false, nullptr, 1.0, false, out, d_part.p, npw);
+    return ASR_OK;
+  };
+  for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
+    const int nt = std::min(tpb, ntile_all - t0);
+    std::vector<int> tact(tpb, 0), act(nlp, 0), tgroup(tpb, -1);
+    for (int q = 0; q < nlp; ++q) {
+      int bt = q / TL, L = -1;
+      if (bt < nt && q % TL < (int)tiles[t0 + bt].size()) L = tiles[t0 + bt][q % TL];
+      lmap[q] = L;
+      hgroup[q] = L >= 0 ? lane_group[L] : -1;
+      hkind[q] = L >= 0 ? lane_kind[L] : 0;
+      hz[q] = L >= 0 ? lane_z[L] : make_double2(0, 0);
+      if (L >= 0) { tact[bt] = 1; act[q] = 1; tgroup[bt] = hgroup[q]; }
+    }
+    ASR_CUDA(cudaMemcpyAsync(d_lgroup.p, hgroup.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_tgroup.p, tgroup.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_kind.p, hkind.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_lmap.p, lmap.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_act.p, act.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_tact.p, tact.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_z.p, hz.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_su.p, ones.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemsetAsync(d_wact.p, 0, nlp * sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_m.p, 0, nlp * sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_closed.p, 0, nlp * sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_a.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_b.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_c.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_gprev.p, 0, nlp * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_fprev.p, 0, nlp * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_bprev.p, 0, nlp * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_sup.p, 0, nlp * sizeof(double2), s));
+    BatchView bv{nt, nn, op->nsmax, 0, ASR_MODE_EDC, project, tail, NLMAX, depth_tol, d_gblob.p, GL, d_ginfo.p, d_lgroup.p,
+                 d_tgroup.p, d_z.p, d_act.p, d_wact.p, d_m.p, d_a.p, d_b.p, d_gprev.p, d_acur.p, d_bprev.p, d_su.p, d_sup.p,
+                 d_tact.p, d_nfall.p, d_closed.p};
+    const int grid = nt * bpt;
+    const unsigned egrid = (unsigned)std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256);
+    int kmax = 0;
+    for (int q = 0; q < nlp; ++q) if (hgroup[q] >= 0) kmax = std::max(kmax, ginfo[hgroup[q]].nlev);
+    // ---- start vectors (ed3_start, src/asr_ed3.f90:135-144): |v> = h'|e> (projected), |a> = |e> + o_c |v>
+    k_init<ST><<<egrid, 256, 0, s>>>(bv, V[1].p, V[0].p);
+    ASR_TRY(apply_hp(bv, grid, V[1].p, T1));
+    if (project) k_project<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, T1, npw);
+    k_ed3_dots<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, T1, d_oc.p, d_part.p, d_part2.p, npw);
+    k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_sv.p);
+    k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_sa.p);
+    std::vector<double2> hsv(nlp), hsa(nlp);
+    ASR_CUDA(cudaMemcpyAsync(hsv.data(), d_sv.p, nlp * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaMemcpyAsync(hsa.data(), d_sa.p, nlp * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaStreamSynchronize(s));
+    std::vector<double> htn(nlp, 0.0);
+    for (int q = 0; q < nlp; ++q) {
+      hna[q] = hnv[q] = 1.0;
+      if (hgroup[q] < 0) continue;
+      double nv = std::sqrt(hsv[q].x), na = std::sqrt(hsa[q].x);   // sqrt(real(v.v)), as the reference
+      if (!(nv >= 1.0e-14) || !(na >= 1.0e-14)) { set_error("ed3_start: zero start vector (group %d)", hgroup[q] + 1); return ASR_EINVAL; }
+      hna[q] = na;
+      hnv[q] = nv;
+      htn[q] = hkind[q] == 0 ? nv : na;
+    }
+    ASR_CUDA(cudaMemcpyAsync(d_na.p, hna.data(), nlp * sizeof(double), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_nv.p, hnv.data(), nlp * sizeof(double), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_tn.p, htn.data(), nlp * sizeof(double), cudaMemcpyHostToDevice, s));
+    // V[0] = U_1 (scale 1), V[2] = U_0 = 0; T1 holds |v> until the start vectors are written
+    k_ed3_start<ST><<<egrid, 256, 0, s>>>(bv, T1, d_oc.p, d_kind.p, d_na.p, d_nv.p, V[1].p, V[0].p, TV);
+    // ---- the chains (chain, src/asr_ed3.f90:147-218)
+    for (int k = 1; k <= kmax; ++k) {
+      T2* U = V[k % 3].p;
+      T2* UP = V[(k + 2) % 3].p;
+      T2* Y = V[(k + 1) % 3].p;
+      ASR_TRY(apply_hp(bv, grid, U, T1));                                              // t1 = h'u
+      k_ed3_t3<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, U, T1, T3, npw);                  // t3 = u u - Qt t1
+      apply_SD<ST>(op, bv, dunif, T3, TMP, SA, d_part.p, npw, grid, s);               // S d t3
+      k_ed3_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, U, T1, T3, SA, TV, Y, d_part.p, d_part2.p, npw);
+      k_ed3_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, d_part2.p, bpt, k, d_c.p, d_fprev.p, d_tn.p);
+      k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, Y, U, UP, d_part.p, npw);
+      k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
+    }
+    ASR_CUDA(cudaGetLastError());
+    ctx->launches += 8 + (int64_t)kmax * (dunif ? 8 : 10);
+    k_ed3_final<<<(nlp + 127) / 128, 128, 0, s>>>(bv, nlp, d_lmap.p, d_c.p, d_closed.p, d_g.p, d_f.p);
+    ASR_CUDA(cudaMemcpyAsync(hm.data(), d_m.p, nlp * sizeof(int), cudaMemcpyDeviceToHost, s));
+    for (int which = 0; which < 3; ++which) {
+      std::vector<double2>* dst = which == 0 ? a_out : which == 1 ? b_out : c_out;
+      if (!dst) continue;
+      const double2* src = which == 0 ? d_a.p : which == 1 ? d_b.p : d_c.p;
+      ASR_CUDA(cudaMemcpyAsync(hab.data(), src, hab.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
+      ASR_CUDA(cudaStreamSynchronize(s));
+      for (int q = 0; q < nlp; ++q)
+        if (lmap[q] >= 0)
+          std::copy(hab.begin() + (size_t)q * NLMAX, hab.begin() + (size_t)(q + 1) * NLMAX, dst->begin() + (size_t)lmap[q] * NLMAX);
+    }
+    ASR_CUDA(cudaStreamSynchronize(s));
+    for (int q = 0; q < nlp; ++q) {
+      int L = lmap[q];
+      if (L < 0) continue;
+      m_out[L] = hm[q];
+      na_out[L] = hna[q];
+      nv_out[L] = hnv[q];
+    }
+  }
+  ASR_CUDA(cudaMemcpyAsync(g_out.data(), d_g.p, nlane * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(f_out.data(), d_f.p, nlane * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  int nf = 0;
+  ASR_CUDA(cudaMemcpyAsync(&nf, d_nfall.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  ASR_CUDA(cudaGetLastError());
+  if (nfall_out) *nfall_out = nf;
+  return ASR_OK;
+}
+
 }  // namespace
 
 // the operator kernels stage up to 96 KB of bond blocks in shared memory (set once per device)
@@ -1353,6 +1759,21 @@ int run_adjoint(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   if (precision == ASR_FP32)
     return run_adjoint_t<float>(ctx, op, ginfo, gblob, GL, lane_group, lane_z, lane_w, tail, project, stride, g_out, grad_out);
   return run_adjoint_t<double>(ctx, op, ginfo, gblob, GL, lane_group, lane_z, lane_w, tail, project, stride, g_out, grad_out);
+}
+
+int run_ed3(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+            const GroupLayout& GL, const std::vector<double>& oc, const std::vector<int>& lane_group,
+            const std::vector<int>& lane_kind, const std::vector<double2>& lane_z, double depth_tol, int tail, int project,
+            int precision, std::vector<double2>& g_out, std::vector<double2>& f_out, std::vector<double>& na_out,
+            std::vector<double>& nv_out, std::vector<int>& m_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
+            std::vector<double2>* c_out, int64_t* nfall_out) {
+  smem_attrs();
+  if (smul_smem(op, sizeof(double)) > 96 * 1024) { set_error("ed3: bond tables above 96 KB of shared memory"); return ASR_EINVAL; }
+  if (precision == ASR_FP32)
+    return run_ed3_t<float>(ctx, op, ginfo, gblob, GL, oc, lane_group, lane_kind, lane_z, depth_tol, tail, project, g_out, f_out,
+                            na_out, nv_out, m_out, a_out, b_out, c_out, nfall_out);
+  return run_ed3_t<double>(ctx, op, ginfo, gblob, GL, oc, lane_group, lane_kind, lane_z, depth_tol, tail, project, g_out, f_out,
+                           na_out, nv_out, m_out, a_out, b_out, c_out, nfall_out);
 }
 
 int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,

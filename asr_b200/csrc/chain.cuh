@@ -52,6 +52,7 @@ struct BatchView {
   double2* sup;            // scale of the previous vector
   int* tile_act;           // tile has an active lane
   int* nfall;
+  int* lane_closed;        // optional: 1 where |b| < 1e-12 ended the chain
 };
 
 struct RunOptions {
@@ -69,6 +70,15 @@ int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
               const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
               const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
               std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out);
+
+// route ed3: two chains per (group, energy) (lane kind 0: from |a>, 1: from |v>); per lane g, the projection f, the start
+// norms |a|, |v| and the depth
+int run_ed3(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+            const GroupLayout& GL, const std::vector<double>& oc, const std::vector<int>& lane_group,
+            const std::vector<int>& lane_kind, const std::vector<double2>& lane_z, double depth_tol, int tail, int project,
+            int precision, std::vector<double2>& g_out, std::vector<double2>& f_out, std::vector<double>& na_out,
+            std::vector<double>& nv_out, std::vector<int>& m_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
+            std::vector<double2>* c_out, int64_t* nfall_out);
 
 // reverse mode: G per lane and the gradients sum_lanes w_L dG_L/dpar per group, kinds (c | e | pb), d, pa, each (9, nsp)
 int run_adjoint(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,

@@ -47,7 +47,8 @@ __host__ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __host__ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __host__ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __host__ __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
-__host__ __device__ __forceinline__ double cabs2(double2 a) { return hypot(a.x, a.y); }
+// modulus |a|
+__host__ __device__ __forceinline__ double cmag(double2 a) { return hypot(a.x, a.y); }
 // Smith's algorithm for complex division (R. L. Smith, CACM 5 (1962) 435)
 __host__ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
   if (fabs(b.x) >= fabs(b.y)) {

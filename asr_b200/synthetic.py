@@ -226,6 +226,21 @@ def edc_params(sp: SpeciesParams, central: int):
     return dict(c=cc, d=dd, o=o, e=e, pa=pa, pb=pb, dc=dc, dl=np.asfortranarray(de), enu=np.asfortranarray(en))
 
 
+def ed3_params(sp: SpeciesParams, central: int, o=None, p=None):
+    """Route ed3 (``ed3_setup``, src/asr_edc.f90's sibling src/asr_ed3.f90:57-79) for central species ``central``: with
+    D_s = Delta_l,s, g_s = (D_c / D_s) c_l,s (c as C - E_nu), d = d_l of the central species in the role of D_c^1/2 (as
+    in the edc mapping), and the alpha-representation o_s, p_s per (species, l) (``o``, ``p`` (nsp, 3); default 0).
+    Returns the group dict of ``chains.ed3_blocks`` (start_orb and nlev to be added)."""
+    nsp = sp.c.shape[0]
+    o = np.zeros((nsp, 3)) if o is None else np.asarray(o, float)
+    p = np.zeros((nsp, 3)) if p is None else np.asarray(p, float)
+    c, d, de, en = (sp.per_orbital(x) for x in (sp.c, sp.d, sp.delta, sp.enu))
+    dc = de[:, central - 1].copy()
+    return dict(g=np.asfortranarray(dc[:, None] / de * c), d=np.asfortranarray(np.repeat(d[:, central - 1:central], nsp, axis=1)),
+                dc=dc, dl=np.asfortranarray(de), enu=np.asfortranarray(en), o=sp.per_orbital(o), p=sp.per_orbital(p),
+                central=central)
+
+
 def cubic_case(kind: str, l: int, nsp: int, conc, seed: int, group: str = "d2h", r2max: int | None = None):
     """A one-class cubic alloy: graph, group (perm, dmat), model with Slater-Koster blocks.
 

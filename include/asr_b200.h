@@ -126,6 +126,22 @@ int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
                        int mode, double depth_tol, int tail, int precision, int project, void* g_dev, double* a, double* b,
                        int* mused);
 
+/* ---- route ed3 (src/asr_ed3.f90): chains on z - K'(z), K' = et - h' + u h' + h' u - h' Qt h', h' = g + d S d ---------- */
+typedef struct asr_ed3_group {
+  const double *g, *d;                    /* (9, nsp): h' of ed3_setup (:57-79): g = (D_c / D_s)(C - E_nu), d = D_c^1/2 */
+  const double *dc, *del, *enu, *o, *p;   /* ed3_t (:24-28): D_c (9); D_s, E_nu,s, o_s, p_s (9, nsp) */
+  int central;                            /* species frozen on the start site */
+  int start_orb;                          /* 1..9, one dimensional under the group */
+  int nlev;                               /* chain depth */
+  int reserved;
+} asr_ed3_group;
+/* ed3_blocks (src/asr_ed3.f90:242-265) of every group at every energy: bk(4, nz, ngroup) complex = G_11, (hG)_11,
+ * (hGh)_11 and q1 of the |a> chain minus q1 of the |v> chain; mused(2, nz, ngroup) the depths of the |a> and |v> chains;
+ * a, b, c (nlevmax, 2, nz, ngroup) complex chain coefficients and projections, or NULL.  depth_tol > 0: the depth test
+ * on g and f of :173-179; tail as asr_chains_run (a closed chain uses the exact fraction, cf_closed :221-236). */
+int asr_ed3_blocks(asr_ctx* ctx, asr_op* op, const asr_ed3_group* groups, int ngroup, const double* z, int nz, double depth_tol,
+                   int tail, int precision, int project, double* bk, int* mused, double* a, double* b, double* c);
+
 /* Reverse mode of the batched energy-dependent chains (edc route, o = 0, fixed depth nlev per group): g(nz, ngroup) as
  * asr_chains_run, and grad(9, nsp, 3, ngroup) complex = sum_j w(j, q) dG(j, q)/dpar for the parameter arrays of group q:
  * kind 0 the diagonal c (the same derivative applies to e and pb, which enter only as c + e + pb), kind 1 d, kind 2 pa.

@@ -602,10 +602,7 @@ static void augcls_project_c(const Op& op, cd* x) {
 extern "C" void orc_project_c(void* h, double* x) { augcls_project_c(*(Op*)h, (cd*)x); }
 
 // augcls_hp_c src/asr_augcls.f90:301-320: y = h x, complex, normalised coordinates
-extern "C" void orc_hp_c(void* h, const double* xin, double* yout) {
-  Op& op = *(Op*)h;
-  const cd* x = (const cd*)xin;
-  cd* y = (cd*)yout;
+static void hp_c(const Op& op, const cd* x, cd* y) {
   size_t nd = 9 * (size_t)op.nn;
   std::vector<double> a(nd), b(nd), h1(nd), h2(nd), t1(nd), t2(nd), t3(nd);
   for (int i = 0; i < op.nn; ++i)
@@ -618,6 +615,7 @@ extern "C" void orc_hp_c(void* h, const double* xin, double* yout) {
   for (int i = 0; i < op.nn; ++i)
     for (int l = 0; l < 9; ++l) { size_t q = 9 * (size_t)i + l; y[q] = op.sq[i] * cd(h1[q], h2[q]); }
 }
+extern "C" void orc_hp_c(void* h, const double* xin, double* yout) { hp_c(*(Op*)h, (const cd*)xin, (cd*)yout); }
 
 // ===================================================================================================== eigenvalues
 // Eigenvalues of a complex upper-Hessenberg matrix (here: the complex-symmetric tridiagonal chain matrix) by the
@@ -1231,6 +1229,144 @@ extern "C" void orc_edc_green_blk(void* h, int ns, const double* dc, const doubl
   BlkWork wk;
   wk.init(nb, 9 * (size_t)op.nn);
   edc_green_blk(op, wk, ed, (const cd*)zs, nb, iv, nlev, depth_tol, tail, project != 0, (cd*)g, mused, (cd*)a, (cd*)b, nfall);
+}
+
+// ===================================================================================================== route ed3
+// src/asr_ed3.f90: K'(z) = et - h' + u h' + h' u - h' Qt h' with h' = g + D_c^1/2 S D_c^1/2 (the operator's parameters
+// c = g, d = D_c^1/2, o = e = 0 set by the caller, start site frozen to the central species); chains on z - K' from
+// |a> = |u> + o_c |v> and |v> = h'|u>, each projected on the other start vector.
+struct Ed3 { int ns; std::vector<double> dc, del, enu, o, p; };   // dc (9); del, enu, o, p (9, ns)
+
+// ed3_coefs :91-107
+static void ed3_coefs(const Ed3& ed, cd z, cd* et, cd* uu, cd* qt) {
+  for (int s = 0; s < ed.ns; ++s)
+    for (int l = 0; l < 9; ++l) {
+      int q = l + 9 * s;
+      cd eps = z - ed.enu[q];
+      et[q] = ed.dc[l] / ed.del[q] * eps;
+      uu[q] = ed.o[q] * eps;
+      qt[q] = ed.del[q] / ed.dc[l] * (ed.o[q] - ed.p[q] * eps);
+    }
+}
+
+// ed3_kmul :110-131: y = et x - h'x + u h'x + h'(u x - Qt h'x)
+static void ed3_kmul(const Op& op, const cd* et, const cd* uu, const cd* qt, const cd* x, cd* y, std::vector<cd>* t) {
+  size_t nd = 9 * (size_t)op.nn;
+  hp_c(op, x, t[0].data());
+  augcls_rand_c(op, qt, t[0].data(), t[1].data());
+  augcls_rand_c(op, uu, x, t[2].data());
+  for (size_t q = 0; q < nd; ++q) t[2][q] = t[2][q] - t[1][q];
+  hp_c(op, t[2].data(), t[3].data());
+  augcls_rand_c(op, et, x, y);
+  augcls_rand_c(op, uu, t[0].data(), t[1].data());
+  for (size_t q = 0; q < nd; ++q) y[q] = y[q] - t[0][q] + t[1][q] + t[3][q];
+}
+
+// cf_closed :221-236: the Krylov space is exhausted, the fraction is exact
+static void cf_closed(const cd* a, const cd* b, const cd* c, int m, cd z, cd& g, cd& f) {
+  std::vector<cd> gt(m);
+  gt[m - 1] = 1.0 / (z - a[m - 1]);
+  for (int j = m - 2; j >= 0; --j) gt[j] = 1.0 / (z - a[j] - b[j] * b[j] * gt[j + 1]);
+  g = gt[0];
+  f = 0.0;
+  cd prod = gt[0];
+  for (int k = 0; k < m; ++k) {
+    f = f + c[k] * prod;
+    if (k < m - 1) prod = prod * b[k] * gt[k + 1];
+  }
+}
+
+// chain :147-218: one complex-symmetric chain on z - K' from start (start . start = 1), projections c_k = tv . u_k
+static void ed3_chain(const Op& op, const cd* et, const cd* uu, const cd* qt, cd z, int nlev, double tnorm, double depth_tol,
+                      int tail, bool project, const cd* start, const cd* tv, cd& g, cd& f, int& m, cd* acoef, cd* bcoef,
+                      cd* ccoef, long* nfall) {
+  size_t nd = 9 * (size_t)op.nn;
+  std::vector<cd> u(start, start + nd), up(nd, 0.0), w(nd), t[4];
+  for (auto& v : t) v.assign(nd, 0.0);
+  std::vector<cd> a(nlev, 0.0), b(nlev, 0.0), c(nlev, 0.0);
+  cd gprev = 0.0, fprev = 0.0, gtry, ftry;
+  m = 0;
+  bool closed = false;
+  for (int k = 1; k <= nlev; ++k) {
+    cd s = 0.0;
+    for (size_t q = 0; q < nd; ++q) s += tv[q] * u[q];
+    c[k - 1] = s;
+    ed3_kmul(op, et, uu, qt, u.data(), w.data(), t);
+    for (size_t q = 0; q < nd; ++q) w[q] = z * u[q] - w[q];
+    s = 0.0;
+    for (size_t q = 0; q < nd; ++q) s += u[q] * w[q];
+    a[k - 1] = s;
+    m = k;
+    if (k == nlev) break;
+    if (depth_tol > 0.0 && k >= 8 && k % 4 == 0) {
+      cf_species(a.data(), b.data(), c.data(), k, z, tail, gtry, ftry, nullptr, nullptr, nfall);
+      if (k > 8 && std::abs(gtry - gprev) <= depth_tol * std::abs(gtry) &&
+          std::abs(ftry - fprev) <= depth_tol * std::max(std::abs(ftry), tnorm * std::abs(gtry)))
+        break;
+      gprev = gtry; fprev = ftry;
+    }
+    cd ak = a[k - 1], bk = 0.0;
+    if (k > 1) bk = b[k - 2];
+    for (size_t q = 0; q < nd; ++q) {
+      w[q] = w[q] - ak * u[q];
+      if (k > 1) w[q] = w[q] - bk * up[q];
+    }
+    if (project) augcls_project_c(op, w.data());
+    s = 0.0;
+    for (size_t q = 0; q < nd; ++q) s += w[q] * w[q];
+    b[k - 1] = std::sqrt(s);
+    if (std::abs(b[k - 1]) < 1.0e-12) { closed = true; break; }
+    bk = b[k - 1];
+    for (size_t q = 0; q < nd; ++q) { up[q] = u[q]; u[q] = w[q] / bk; }
+  }
+  if (closed) cf_closed(a.data(), b.data(), c.data(), m, z, g, f);
+  else cf_species(a.data(), b.data(), c.data(), m, z, tail, g, f, nullptr, nullptr, nfall);
+  for (int k = 0; k < m; ++k) {
+    if (acoef) acoef[k] = a[k];
+    if (bcoef) bcoef[k] = b[k];
+    if (ccoef) ccoef[k] = c[k];
+  }
+}
+
+// ed3_start :135-144 and ed3_blocks :242-265 at one energy: bk(0) = G_11, bk(1) = (hG)_11, bk(2) = (hGh)_11,
+// bk(3) = q1 of the |a> chain - q1 of the |v> chain.  m(2): depths of the two chains.
+extern "C" int orc_ed3_blocks(void* h, int ns, const double* dc, const double* del, const double* enu, const double* o,
+                              const double* p, int central, double zr, double zi, int iv, int nlev, double depth_tol, int tail,
+                              int project, double* bk, int* mout, double* acoef, double* bcoef, double* ccoef, long* nfall) {
+  Op& op = *(Op*)h;
+  Ed3 ed{ns, std::vector<double>(dc, dc + 9), std::vector<double>(del, del + 9 * ns), std::vector<double>(enu, enu + 9 * ns),
+         std::vector<double>(o, o + 9 * ns), std::vector<double>(p, p + 9 * ns)};
+  size_t nd = 9 * (size_t)op.nn;
+  std::vector<cd> s0(nd, 0.0), vv(nd), av(nd);
+  s0[iv - 1] = 1.0;
+  hp_c(op, s0.data(), vv.data());
+  if (project) augcls_project_c(op, vv.data());
+  const double oc = ed.o[(iv - 1) + 9 * (size_t)(central - 1)];
+  for (size_t q = 0; q < nd; ++q) av[q] = s0[q] + oc * vv[q];
+  cd sv = 0.0, sa = 0.0;
+  for (size_t q = 0; q < nd; ++q) { sv += vv[q] * vv[q]; sa += av[q] * av[q]; }
+  double nv = std::sqrt(sv.real()), na = std::sqrt(sa.real());
+  if (nv < 1.0e-14 || na < 1.0e-14) return fail("ed3_start: zero start vector");
+  cd z(zr, zi);
+  std::vector<cd> et(9 * (size_t)ns), uu(9 * (size_t)ns), qt(9 * (size_t)ns);
+  ed3_coefs(ed, z, et.data(), uu.data(), qt.data());
+  std::vector<cd> st(nd);
+  cd gt, fm;
+  int m1 = 0, m2 = 0;
+  for (size_t q = 0; q < nd; ++q) st[q] = av[q] / na;
+  ed3_chain(op, et.data(), uu.data(), qt.data(), z, nlev, nv, depth_tol, tail, project != 0, st.data(), vv.data(), gt, fm, m1,
+            acoef ? (cd*)acoef : nullptr, bcoef ? (cd*)bcoef : nullptr, ccoef ? (cd*)ccoef : nullptr, nfall);
+  cd q0 = na * na * gt, q1a = na * fm;
+  for (size_t q = 0; q < nd; ++q) st[q] = vv[q] / nv;
+  ed3_chain(op, et.data(), uu.data(), qt.data(), z, nlev, na, depth_tol, tail, project != 0, st.data(), av.data(), gt, fm, m2,
+            acoef ? (cd*)acoef + nlev : nullptr, bcoef ? (cd*)bcoef + nlev : nullptr, ccoef ? (cd*)ccoef + nlev : nullptr,
+            nfall);
+  cd q2 = nv * nv * gt, q1b = nv * fm;
+  fm = 0.5 * (q1a + q1b);
+  cd out[4] = {q0 - 2.0 * oc * fm + oc * oc * q2, fm - oc * q2, q2, q1a - q1b};
+  for (int k = 0; k < 4; ++k) { bk[2 * k] = out[k].real(); bk[2 * k + 1] = out[k].imag(); }
+  if (mout) { mout[0] = m1; mout[1] = m2; }
+  return 0;
 }
 
 // ===================================================================================================== chain scheduler

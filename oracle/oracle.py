@@ -64,6 +64,8 @@ def lib():
                                         C.c_int, _d, _i, _d, _d, _l]
         L.orc_chain_greens.argtypes = [C.c_void_p, C.c_int, _d, _i, C.c_int, _i, _i, _d, C.c_int, C.c_int, C.c_double,
                                        C.c_int, C.c_int, C.c_int, _d, _l]
+        L.orc_ed3_blocks.argtypes = [C.c_void_p, C.c_int, _d, _d, _d, _d, _d, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
+                                     C.c_double, C.c_int, C.c_int, _d, _i, _d, _d, _d, _l]
         L.orc_gauss_legendre.argtypes = [C.c_int, _d, _d]
         L.orc_contour_nodes.argtypes = [C.c_double, C.c_double, C.c_int, C.c_double, _d, _d]
         L.orc_contour_nodes_closed.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, _d, _d]
@@ -234,6 +236,26 @@ class OracleOp:
                                 depth_tol, TAILS[tail], int(project), _pd(g), _pi(mu),
                                 _pd(a), _pd(b), C.byref(nf))
         return g, mu, a.T, b.T
+
+    def ed3_blocks(self, ed3, zs, iv, nlev, depth_tol=0.0, tail="hull", project=True):
+        """``ed3_blocks`` (src/asr_ed3.f90:242-265) per energy on the operator's current parameters (set_params with
+        c = g, d, o = e = 0; start site frozen to the central species; set_start(iv)).  Returns (bk (4, nz), m (2, nz),
+        a, b, c (nz, 2, nlev))."""
+        ns = int(np.asarray(ed3["dl"]).shape[1])
+        arrs = [_f64(ed3[k]) for k in ("dc", "dl", "enu", "o", "p")]
+        zs = np.atleast_1d(np.asarray(zs, np.complex128))
+        nz = zs.shape[0]
+        bk = np.zeros((nz, 4), np.complex128)
+        m = np.zeros((nz, 2), np.int32)
+        a = np.zeros((nz, 2, nlev), np.complex128)
+        b = np.zeros((nz, 2, nlev), np.complex128)
+        c = np.zeros((nz, 2, nlev), np.complex128)
+        nf = C.c_long(0)
+        for j in range(nz):
+            _check(lib().orc_ed3_blocks(self.h, ns, *[_pd(x) for x in arrs], int(ed3["central"]), zs[j].real, zs[j].imag, iv,
+                                        nlev, depth_tol, TAILS[tail], int(project), _pd(bk[j]), _pi(m[j]), _pd(a[j]), _pd(b[j]),
+                                        _pd(c[j]), C.byref(nf)))
+        return bk.T, m.T, a, b, c
 
     def chain_greens(self, groups, gcomp, iorb, nlevq, zs, nbe, depth_tol=0.0, tail="hull", project=True, nthreads=0):
         """``chain_greens`` (src/asr_class_scf.f90:966-1160): groups is a list of dicts with c, d, o, e, dc, dl, enu;

@@ -127,6 +127,23 @@ def test_edc_general_operator_with_o_and_depth_tol():
     assert np.max(np.abs(g - go) / np.abs(go)) < 1e-8
 
 
+def test_edc_depth_test_stops_where_the_oracle_stops():
+    """The depth test |G_k - G_{k-4}| <= tol |G_k| (src/asr_edc.f90:121-127) near the real axis, where the stopping depth
+    varies from energy to energy."""
+    case = K.cubic("bcc", 3, 2, (0.5, 0.5), group="d4h", maxlevel=3, maxrank=1)
+    gop, oop = K.build_both(case, A.build_augcls_operator, O.OracleOp)
+    ed = S.edc_params(S.draw_species(2, 8), 1)
+    for op in (gop, oop):
+        op.set_params(ed["c"], ed["d"], ed["o"], ed["e"])
+        op.unfreeze()
+        op.freeze_site(1, 1)
+    zs = np.linspace(-0.8, 0.4, 41) + 0.01j
+    g, m, a, b, go, mo, ao, bo = _edc_compare(gop, oop, ed, zs, 1, 40, 1e-3, "hull")
+    assert np.array_equal(m, mo)
+    assert len(set(m.tolist())) > 1
+    assert np.max(np.abs(g - go) / np.abs(go)) < 1e-8
+
+
 def test_edc_fp32_matvec_error_is_bounded():
     case = K.cubic("bcc", 3, 2, (0.5, 0.5), group="d4h", maxlevel=3, maxrank=1)
     gop, oop = K.build_both(case, A.build_augcls_operator, O.OracleOp)
