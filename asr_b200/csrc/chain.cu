@@ -152,6 +152,49 @@ template <> struct Pair<double> { typedef double2 T; };
 template <> struct Pair<float> { typedef float2 T; };
 
 constexpr int RW = 12;   // padded row of a shared-memory block (16-byte aligned pairs for FP64 and FP32)
+// packed orbital operation of the identity: permutation pi(l) = l in bits 4l..4l+3, no signs (bits 40..48)
+constexpr unsigned long long PW_IDENTITY = 0x876543210ull;
+
+// the output of one node of the S application: t2 (unscaled), or with FINAL y = s (d t2 + (c + e + X(z)) U) and the
+// node's share of the dot sum norb (s U) . y
+template <typename ST, bool FINAL, typename T2, typename A2>
+__device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView& bv, int tile, int i, int lane, int L, int grp,
+                                              int gflags, int gfrozen, const unsigned long long* piw, const T2* __restrict__ in,
+                                              T2* __restrict__ out, const A2* acc, double2& dot) {
+  if (!FINAL) {
+    for (int l = 0; l < 9; ++l) stv(out + vix(tile, bv.nn, i, l) + lane, make_double2(acc[l].x, acc[l].y));
+  } else {
+    // y_l = s (d_l t2_l + P_l(U)),  P = c + e + X(z) (src/asr_augblk.f90:219-250), orbital by orbital
+    const double* gb = bv.gblob + (size_t)(grp >= 0 ? grp : 0) * bv.GL.stride;
+    const double2 z = bv.lane_z[L];
+    const double2 s = bv.su[L];
+    const bool withx = !(gflags & GF_X_ZERO);
+    const double norb = op.sq[i] * op.sq[i];
+    const int fs = (op.start[i] && gfrozen > 0) ? gfrozen : (int)op.frozen[i];
+    const int nsm = op.nsmax, kap = op.ncl[i], l0 = op.lst[i], nk = op.nsc[kap];
+    for (int l = 0; l < 9; ++l) {
+      double2 ui = ld(in + vix(tile, bv.nn, i, l) + lane);
+      double2 pt;
+      if (fs > 0) {
+        pt = cmul(praw(gb, bv.GL, PCEB, withx ? PA : -1, z, fs, l), ui);
+      } else {
+        pt = cmul(pweight(gb, bv.GL, PCEB, withx ? PA : -1, z, nsm, kap, l0, l0, l), ui);
+        for (int k = 0; k < nk; ++k) {
+          if (k == l0) continue;
+          int r = op.flipr[k + nsm * i];
+          if (r < 0) continue;
+          const unsigned long long pw = piw[op.flipg[k + nsm * i]];
+          int p = (int)((pw >> (4 * l)) & 15ull);
+          double2 xr = flip_if(ld(in + vix(tile, bv.nn, r, p) + lane), (uint32_t)((pw >> (40 + l)) & 1ull));
+          pt = cadd(pt, cmul(pweight(gb, bv.GL, PCEB, withx ? PA : -1, z, nsm, kap, l0, k, l), xr));
+        }
+      }
+      double2 y = cmul(s, cadd(make_double2(acc[l].x, acc[l].y), pt));
+      stv_cs(out + vix(tile, bv.nn, i, l) + lane, y);
+      dot = cadd(dot, cscale(cmul(cmul(s, ui), y), norb));
+    }
+  }
+}
 
 // ------------------------------------------------------------------------------------------------ S application
 // t2 = S t1 (src/asr_augcls.f90:456-477 / src/asr_augblk.f90:170-203), unscaled amplitude coordinates.
@@ -248,38 +291,192 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
         acc[l].y = fma_(row[8], v[8].y, acc[l].y);
       }
     }
-    if (!FINAL) {
-      for (int l = 0; l < 9; ++l) stv(out + vix(it.tile, bv.nn, i, l) + lane, make_double2(acc[l].x, acc[l].y));
-    } else {
-      // y_l = s (d_l t2_l + P_l(U)),  P = c + e + X(z) (src/asr_augblk.f90:219-250), orbital by orbital
-      const double* gb = bv.gblob + (size_t)(grp >= 0 ? grp : 0) * bv.GL.stride;
-      const double2 z = bv.lane_z[L];
-      const double2 s = bv.su[L];
-      const bool withx = !(gflags & GF_X_ZERO);
-      const double norb = op.sq[i] * op.sq[i];
-      const int fs = (op.start[i] && gfrozen > 0) ? gfrozen : (int)op.frozen[i];
-      const int nsm = op.nsmax, kap = op.ncl[i], l0 = op.lst[i], nk = op.nsc[kap];
-      for (int l = 0; l < 9; ++l) {
-        double2 ui = ld(in + vix(it.tile, bv.nn, i, l) + lane);
-        double2 pt;
-        if (fs > 0) {
-          pt = cmul(praw(gb, bv.GL, PCEB, withx ? PA : -1, z, fs, l), ui);
-        } else {
-          pt = cmul(pweight(gb, bv.GL, PCEB, withx ? PA : -1, z, nsm, kap, l0, l0, l), ui);
-          for (int k = 0; k < nk; ++k) {
-            if (k == l0) continue;
-            int r = op.flipr[k + nsm * i];
-            if (r < 0) continue;
-            const unsigned long long pw = piw[op.flipg[k + nsm * i]];
-            int p = (int)((pw >> (4 * l)) & 15ull);
-            double2 xr = flip_if(ld(in + vix(it.tile, bv.nn, r, p) + lane), (uint32_t)((pw >> (40 + l)) & 1ull));
-            pt = cadd(pt, cmul(pweight(gb, bv.GL, PCEB, withx ? PA : -1, z, nsm, kap, l0, k, l), xr));
-          }
-        }
-        double2 y = cmul(s, cadd(make_double2(acc[l].x, acc[l].y), pt));
-        stv_cs(out + vix(it.tile, bv.nn, i, l) + lane, y);
-        dot = cadd(dot, cscale(cmul(cmul(s, ui), y), norb));
+    smul_node_out<ST, FINAL>(op, bv, it.tile, i, lane, L, grp, gflags, gfrozen, piw, in, out, acc, dot);
+  }
+  if (FINAL) block_reduce_store(dot, part, it.tile, bpt);
+}
+
+// ------------------------------------------------------------------------------------------------ staged S application
+// The same product with the neighbour rows staged in shared memory by the bulk-copy engine: one node's nine rows of a
+// tile are contiguous (9 x 32 lanes), so lane 0 of each warp copies whole rows with cp.async.bulk into a ring of NST
+// stages per warp, completion counted on one mbarrier per stage, while the warp multiplies the previous rows out of
+// shared memory.  The gathers then cost no registers and no load latency in the FMA stream.  Every wait is bounded: on
+// timeout the warp records an error, stops computing, drains its copies (bounded) and still reaches the block barrier.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* mb, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(mb)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* mb, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mb)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mb) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(mb))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* mb, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(mb)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+constexpr int SMUL_NST = 2;            // stages per warp
+constexpr long SMUL_WAIT_LIMIT = 1L << 24;
+
+size_t smul_smem(const asr_op* op, size_t st_size);
+
+template <typename ST>
+size_t smul_bulk_smem(const asr_op* op) {
+  typedef typename St2<ST>::T T2;
+  size_t b = smul_smem(op, sizeof(ST));
+  b = (b + 127) & ~(size_t)127;
+  b += (size_t)WPB * SMUL_NST * 9 * TL * sizeof(T2);
+  b += (size_t)WPB * SMUL_NST * sizeof(uint64_t);
+  return b;
+}
+
+// acc += B x with x the staged rows (row pi(lp) for column lp, signs of pw)
+template <typename ST, typename T2>
+__device__ __forceinline__ void mac9_staged(const ST* __restrict__ Bk, const T2* __restrict__ rows, unsigned long long pw, T2* acc) {
+  typedef typename Pair<ST>::T P2;
+  T2 x[9];
+#pragma unroll
+  for (int lp = 0; lp < 9; ++lp)
+    x[lp] = flip_if(rows[(int)((pw >> (4 * lp)) & 15ull) * TL], (uint32_t)((pw >> (40 + lp)) & 1ull));
+#pragma unroll
+  for (int l = 0; l < 9; ++l) {
+    const ST* row = Bk + l * RW;
+#pragma unroll
+    for (int lp = 0; lp < 8; lp += 2) {
+      P2 bb = *(const P2*)(row + lp);
+      acc[l].x = fma_(bb.x, x[lp].x, acc[l].x);
+      acc[l].y = fma_(bb.x, x[lp].y, acc[l].y);
+      acc[l].x = fma_(bb.y, x[lp + 1].x, acc[l].x);
+      acc[l].y = fma_(bb.y, x[lp + 1].y, acc[l].y);
+    }
+    acc[l].x = fma_(row[8], x[8].x, acc[l].x);
+    acc[l].y = fma_(row[8], x[8].y, acc[l].y);
+  }
+}
+
+template <typename ST, bool FUSE_D, bool FINAL>
+__global__ void __launch_bounds__(WPB * TL) k_smul_bulk(OpView op, BatchView bv, const ST* __restrict__ blocks,
+                                                        const typename St2<ST>::T* __restrict__ in,
+                                                        typename St2<ST>::T* __restrict__ out, double2* part, int npw, int* err) {
+  typedef typename St2<ST>::T T2;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int ns1 = op.nslot + 1;
+  ST* Bs = (ST*)smem_raw;                                                        // [ntype][ns1][9][RW]
+  const size_t bs_bytes = ((size_t)op.ntype * ns1 * 9 * RW * sizeof(ST) + 15) & ~(size_t)15;
+  unsigned long long* piw = (unsigned long long*)(smem_raw + bs_bytes);
+  const size_t stage_off = (bs_bytes + (size_t)op.nop * sizeof(unsigned long long) + 127) & ~(size_t)127;
+  T2* stages = (T2*)(smem_raw + stage_off);                                     // [WPB][NST][9][TL]
+  uint64_t* mbar = (uint64_t*)(smem_raw + stage_off + (size_t)WPB * SMUL_NST * 9 * TL * sizeof(T2));
+  NodeIter it;
+  int bpt;
+  bool live = node_iter(bv, npw, it, bpt);
+  const int grp = live ? bv.tile_group[it.tile] : -1;
+  unsigned long long chimask = 0ull;
+  int gflags = 0, gfrozen = 0;
+  if (grp >= 0) {
+    chimask = bv.ginfo[grp].chimask;
+    gflags = bv.ginfo[grp].flags;
+    gfrozen = bv.ginfo[grp].frozen_sp;
+  }
+  {
+    const double* dd = grp >= 0 ? bv.ginfo[grp].dd : nullptr;
+    const int nb = op.ntype * ns1 * 81;
+    for (int q = threadIdx.x; q < nb; q += blockDim.x) {
+      int lp = q % 9, l = (q / 9) % 9, tk = q / 81;
+      double v = (double)blocks[q];
+      if (FUSE_D && dd) v *= dd[lp];
+      if (FINAL && dd) v *= dd[l];
+      Bs[((size_t)tk * 9 + l) * RW + lp] = (ST)v;
+    }
+    for (int g = threadIdx.x; g < op.nop; g += blockDim.x) {
+      unsigned long long w = 0ull;
+      for (int l = 0; l < 9; ++l) w |= (unsigned long long)op.pi[g * 9 + l] << (4 * l);
+      uint32_t sg = op.sgm[g] ^ (((chimask >> g) & 1ull) ? 0x1FFu : 0u);
+      piw[g] = w | ((unsigned long long)sg << 40);
+    }
+    if (threadIdx.x < WPB * SMUL_NST) mbar_init(mbar + threadIdx.x, 1);
+    mbar_init_fence();
+  }
+  __syncthreads();
+  if (!live) return;
+  const int lane = threadIdx.x % TL, w = threadIdx.x / TL;
+  const int L = it.tile * TL + lane;
+  T2* stg = stages + (size_t)w * SMUL_NST * 9 * TL;
+  uint64_t* mb = mbar + w * SMUL_NST;
+  const uint32_t slab = 9 * TL * sizeof(T2);
+  double2 dot = make_double2(0.0, 0.0);
+  // slab stream of this warp: for each of its nodes, the own rows (slot -1) then every slot with a neighbour
+  auto node_of = [&](int qn) { return it.first + w + WPB * qn; };
+  auto valid_node = [&](int qn) { return qn < npw && node_of(qn) < bv.nn; };
+  auto next_slot = [&](int i, int k) {   // next slot after k with a neighbour, nslot if none
+    int kk = k + 1;
+    while (kk < op.nslot && op.hopr[kk + op.nslot * i] < 0) ++kk;
+    return kk;
+  };
+  int pq = 0, pk = -1;          // producer position
+  bool pdone = !valid_node(0);
+  auto issue = [&](int s) {     // lane 0: copy the producer's slab into stage s, then advance the producer
+    const int i = node_of(pq);
+    const int r = pk < 0 ? i : op.hopr[pk + op.nslot * i];
+    if (lane == 0) {
+      mbar_expect_tx(mb + s, slab);
+      bulk_g2s(stg + (size_t)s * 9 * TL, in + vix(it.tile, bv.nn, r, 0), slab, mb + s);
+    }
+    pk = next_slot(i, pk);
+    if (pk >= op.nslot) { ++pq; pk = -1; pdone = !valid_node(pq); }
+  };
+  for (int s = 0; s < SMUL_NST && !pdone; ++s) issue(s);
+  bool ok = true;
+  long t = 0;
+  int cq = 0, ck = -1;
+  bool cdone = !valid_node(0);
+  T2 acc[9];
+  for (int l = 0; l < 9; ++l) { acc[l].x = 0; acc[l].y = 0; }
+  while (!cdone) {
+    const int s = (int)(t % SMUL_NST);
+    const uint32_t parity = (uint32_t)((t / SMUL_NST) & 1);
+    if (ok) {
+      long n = 0;
+      while (!mbar_try_wait(mb + s, parity)) {
+        if (++n > SMUL_WAIT_LIMIT) { ok = false; if (lane == 0) dev_fail(err, DERR_WAIT); break; }
       }
+    }
+    const int i = node_of(cq);
+    if (ok) {
+      const ST* B = Bs + (size_t)op.typ[i] * ns1 * 9 * RW;
+      const unsigned long long pw = ck < 0 ? PW_IDENTITY : piw[op.hopg[ck + op.nslot * i]];
+      mac9_staged<ST>(B + (size_t)(ck + 1) * 9 * RW, stg + (size_t)s * 9 * TL + lane, pw, acc);
+    }
+    __syncwarp();
+    if (ok && !pdone) {
+      if (lane == 0) fence_proxy_async_smem();
+      issue(s);
+    }
+    ++t;
+    ck = next_slot(i, ck);
+    if (ck >= op.nslot) {   // the node is complete
+      if (ok) smul_node_out<ST, FINAL>(op, bv, it.tile, i, lane, L, grp, gflags, gfrozen, piw, in, out, acc, dot);
+      for (int l = 0; l < 9; ++l) { acc[l].x = 0; acc[l].y = 0; }
+      ++cq;
+      ck = -1;
+      cdone = !valid_node(cq);
+    }
+  }
+  if (!ok) {   // drain: the copies issued after the failed wait (bounded)
+    for (int s = 0; s < SMUL_NST; ++s) {
+      long n = 0;
+      while (!mbar_try_wait(mb + s, (uint32_t)(((t + s) / SMUL_NST) & 1)) && ++n < SMUL_WAIT_LIMIT) {}
     }
   }
   if (FINAL) block_reduce_store(dot, part, it.tile, bpt);
@@ -585,6 +782,41 @@ size_t smul_smem(const asr_op* op, size_t st_size) {
   return b;
 }
 
+// the staged (bulk-copy) S application when ASR_SMUL_BULK=1.  Measured on the fcc ternary workload it is slower than
+// the direct gathers (FP64 5.3 / 7.1 / 7.4 ms per 16-tile launch with 2 / 3 / 4 stages against 4.55 ms; FP32 1.72 ms
+// against 1.35 ms): the per-node rows are small copies, and the stage buffers cost the occupancy that hides the gathers
+bool smul_bulk_enabled() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = getenv("ASR_SMUL_BULK");
+    on = (e && atoi(e) == 1) ? 1 : 0;
+  }
+  return on == 1;
+}
+
+template <typename ST, bool FUSE_D, bool FINAL>
+void launch_smul(asr_op* op, const BatchView& bv, const ST* blk, const typename St2<ST>::T* in, typename St2<ST>::T* out,
+                 double2* part, int npw, int grid, cudaStream_t s) {
+  OpView ov = op->view();
+  if (smul_bulk_enabled())
+    k_smul_bulk<ST, FUSE_D, FINAL><<<grid, WPB * TL, smul_bulk_smem<ST>(op), s>>>(ov, bv, blk, in, out, part, npw, op->ctx->d_err);
+  else
+    k_smul<ST, FUSE_D, FINAL><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
+}
+
+// a bounded wait of the staged kernels that ran out (the device error word), as a status
+int check_wait_error(asr_ctx* ctx) {
+  int h = 0;
+  ASR_CUDA(cudaMemcpyAsync(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  ASR_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (h == DERR_WAIT) {
+    cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream);
+    set_error("chains: a bulk copy of the staged operator did not complete in time");
+    return ASR_ESTATE;
+  }
+  return ASR_OK;
+}
+
 // One chain step of the general operator on the batch; writes y into Y and the a-partials.
 template <typename ST>
 int step_apply(asr_ctx* ctx, asr_op* op, const BatchView& bv, bool fused, bool any_o, bool all_dunif,
@@ -596,15 +828,15 @@ int step_apply(asr_ctx* ctx, asr_op* op, const BatchView& bv, bool fused, bool a
   size_t sm = smul_smem(op, sizeof(ST));
   dim3 B(WPB * TL);
   if (fused) {
-    k_smul<ST, true, true><<<grid, B, sm, s>>>(ov, bv, blk, U, Y, part, npw);
+    launch_smul<ST, true, true>(op, bv, blk, U, Y, part, npw, grid, s);
     return ASR_OK;
   }
   // t1 = D x0, t2 = S t1
   if (all_dunif) {
-    k_smul<ST, true, false><<<grid, B, sm, s>>>(ov, bv, blk, U, T2, part, npw);
+    launch_smul<ST, true, false>(op, bv, blk, U, T2, part, npw, grid, s);
   } else {
     k_rand<ST><<<grid, B, 0, s>>>(ov, bv, PD, U, T1, npw);
-    k_smul<ST, false, false><<<grid, B, sm, s>>>(ov, bv, blk, T1, T2, part, npw);
+    launch_smul<ST, false, false>(op, bv, blk, T1, T2, part, npw, grid, s);
   }
   if (!any_o) {   // y = s (D t2 + (c + e + X) U)
     k_combine<ST><<<grid, B, 0, s>>>(ov, bv, T2, U, PCEB, true, U, false, nullptr, 1.0, true, Y, part, npw);
@@ -614,7 +846,7 @@ int step_apply(asr_ctx* ctx, asr_op* op, const BatchView& bv, bool fused, bool a
   k_combine<ST><<<grid, B, 0, s>>>(ov, bv, T2, U, PC, false, U, false, nullptr, 1.0, false, H1, part, npw);
   k_rand<ST><<<grid, B, 0, s>>>(ov, bv, PO, H1, R1, npw);
   k_rand<ST><<<grid, B, 0, s>>>(ov, bv, PD, R1, T1, npw);
-  k_smul<ST, false, false><<<grid, B, sm, s>>>(ov, bv, blk, T1, T2, part, npw);
+  launch_smul<ST, false, false>(op, bv, blk, T1, T2, part, npw, grid, s);
   k_combine<ST><<<grid, B, 0, s>>>(ov, bv, T2, R1, PC, false, U, true, H1, -1.0, true, Y, part, npw);
   return ASR_OK;
 }
@@ -784,6 +1016,7 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   int nf = 0;
   ASR_CUDA(cudaMemcpyAsync(&nf, d_nfall.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaStreamSynchronize(s));
+  ASR_TRY(check_wait_error(ctx));
   for (int L = 0; L < nlane; ++L) nsteps += hm_all[L];
   if (m_out) *m_out = hm_all;
   if (nfall_out) *nfall_out = nf;
@@ -1100,10 +1333,10 @@ void apply_SD(asr_op* op, const BatchView& bv, bool dunif, const typename St2<ST
   const ST* blk = std::is_same<ST, double>::value ? (const ST*)op->d_blocks : (const ST*)op->d_blocks_f;
   size_t sm = smul_smem(op, sizeof(ST));
   if (dunif) {
-    k_smul<ST, true, false><<<grid, WPB * TL, sm, s>>>(ov, bv, blk, x, t2, part, npw);
+    launch_smul<ST, true, false>(op, bv, blk, x, t2, part, npw, grid, s);
   } else {
     k_rand<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, PD, x, tmp, npw);
-    k_smul<ST, false, false><<<grid, WPB * TL, sm, s>>>(ov, bv, blk, tmp, t2, part, npw);
+    launch_smul<ST, false, false>(op, bv, blk, tmp, t2, part, npw, grid, s);
   }
 }
 
@@ -1326,6 +1559,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     const int nsd = dunif ? 1 : 2;   // launches of one S application
     ctx->launches += 1 + (int64_t)kmax * ((4 + nsd) + (3 + nsd) + (12 + nsd));
   }
+  ASR_TRY(check_wait_error(ctx));
   return ASR_OK;
 }
 
@@ -1729,6 +1963,7 @@ int run_ed3_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
   ASR_CUDA(cudaMemcpyAsync(&nf, d_nfall.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaStreamSynchronize(s));
   ASR_CUDA(cudaGetLastError());
+  ASR_TRY(check_wait_error(ctx));
   if (nfall_out) *nfall_out = nf;
   return ASR_OK;
 }
@@ -1747,6 +1982,12 @@ static void smem_attrs() {
   cudaFuncSetAttribute(k_smul<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   cudaFuncSetAttribute(k_smul<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   cudaFuncSetAttribute(k_smul<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul_bulk<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_smul_bulk<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_smul_bulk<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_smul_bulk<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_smul_bulk<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_smul_bulk<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   done[dev] = true;
 }
 
@@ -1792,6 +2033,7 @@ int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
 // ------------------------------------------------------------------------------------------------ drop-in applications
 int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
                   const GroupLayout& GL, int nvec, const double* x_host, bool complex_in, double* y_host, int what) {
+  smem_attrs();
   cudaStream_t s = ctx->stream;
   const int nn = op->nn;
   const int nt = (nvec + TL - 1) / TL;

@@ -36,6 +36,7 @@ enum DevErr : int {
   DERR_STAB = 3,          // stabiliser size * orbit size != group order
   DERR_KEY = 4,           // configuration longer than the key width
   DERR_START = 5,         // start site not invariant
+  DERR_WAIT = 6,          // a bounded wait on a bulk copy ran out
 };
 
 __device__ __forceinline__ void dev_fail(int* err, int code) { atomicCAS(err, 0, code); }
