@@ -40,6 +40,8 @@ def parse():
     p.add_argument("--nz-slice", type=int, default=NZ_SLICE)
     p.add_argument("--cpu-sample", type=int, default=1, help="run the bounded CPU baseline sample (1) or skip it (0)")
     p.add_argument("--e2e", type=int, default=1, help="time the host-buffer C-ABI path too (1) or skip it (0)")
+    p.add_argument("--scf", type=int, default=0,
+                   help="SCF leg: 0 none, 1 two timed iterations at full size + convergence on a small cluster, 2 converge at full size")
     p.add_argument("--legs", type=int, default=1,
                    help="also measure the mixed-precision leg with its DOS error and the adjoint leg (1) or not (0)")
     return p.parse_args()
@@ -267,6 +269,47 @@ def plain_leg(torch):
             "dos_abs_error_vs_oracle": err}
 
 
+def scf_model(l, maxlevel, precision):
+    """The large batched SCF configuration: equiatomic 5-component fcc random alloy (Fe, Co, Ni, Cr, Mn-like parameters
+    drawn from seed 4), spd 9 orbitals, spin-polarised (2 x 5 x 9 = 90 chain groups), depths U{20..32}, 64-point
+    contour; model potential update (screened on-site response 0.08 Ry/e, exchange splitting 0.06 Ry per unit moment)."""
+    import asr_b200 as A
+    from asr_b200 import scf as SC, synthetic as S
+    case = S.cubic_case("fcc", l, 5, [0.2] * 5, seed=4, group="d2h")
+    fl = np.ones(case["graph"].n, np.int32)
+    fl[0] = 0
+    op = A.build_augcls_operator(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, maxlevel, maxrank=1,
+                                 flippable=fl)
+    sp = S.draw_species(5, 4)
+    depths = np.random.default_rng(4).integers(20, 33, size=(2, 5, 9))
+    return SC.ScfModel(op=op, x=np.full(5, 0.2), c0=sp.c, d=sp.d, delta=sp.delta, z=np.array([8.0, 9.0, 10.0, 6.0, 7.0]),
+                       u=np.full(5, 0.08), stoner=np.full(5, 0.06), depths=depths, ebot=-2.0, ncont=64, precision=precision)
+
+
+def scf_leg(torch, full: bool):
+    """Time per SCF iteration at full size (5^3-cell cluster, levels 3): the reference's scheme (FP64 forward, E_F search,
+    Anderson) against the mixed one (FP32 forward, E_F search, adjoint Jacobian, quasi-Newton step); iterations to a
+    1e-6 charge residual on the same alloy (a 3^3-cell cluster at levels 2 unless full)."""
+    from asr_b200 import scf as SC
+    out = {}
+    for prec, mixer in (("fp64", "anderson"), ("fp32", "broyden")):
+        m = scf_model(5, 3, prec)
+        q0 = np.vstack([m.z / 2 + 0.3, m.z / 2 - 0.3])
+        torch.cuda.synchronize()
+        r = SC.scf_run(m, q0, 0.0, mixer=mixer, tol=1e-6, maxit=40 if full else 2)
+        out[f"{prec}_{mixer}"] = {"seconds_per_iteration": r["seconds"] / r["iterations"], "iterations_run": r["iterations"],
+                                 "converged": r["converged"], "forward_runs": r["stats"]["forward"],
+                                 "adjoint_runs": r["stats"]["adjoint"], "nodes": int(m.op.nn)}
+    if not full:
+        for prec, mixer in (("fp64", "anderson"), ("fp32", "broyden")):
+            m = scf_model(3, 2, prec)
+            q0 = np.vstack([m.z / 2 + 0.3, m.z / 2 - 0.3])
+            r = SC.scf_run(m, q0, 0.0, mixer=mixer, tol=1e-6, maxit=60)
+            out[f"{prec}_{mixer}"]["iterations_to_1e-6_small_cluster"] = r["iterations"] if r["converged"] else None
+            out[f"{prec}_{mixer}"]["small_cluster_nodes"] = int(m.op.nn)
+    return out
+
+
 def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
     """The mixed-precision leg (FP32 matvec and vectors, FP64 coefficients and fractions) with its DOS and charge error
     against the FP64 run, and the adjoint leg (forward plus reverse sweep) on the contour energies."""
@@ -327,6 +370,8 @@ def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
     out["fp64_peak_tflops"] = fp64_peak_tflops(torch)
     out["kpm"] = kpm_leg(torch)
     out["plain"] = plain_leg(torch)
+    if args.scf:
+        out["scf"] = scf_leg(torch, args.scf == 2)
     return out
 
 
