@@ -301,3 +301,59 @@ def heusler_case(l: int = 4, seed: int = 3, sublattice: int = 1, maxlevel: int =
     return dict(graph=g, coord=coord, bvec=bvec, cls=cls, perm=np.asfortranarray(perm, dtype=np.int32),
                 dmat=np.asfortranarray(dmat), model=mdl, maxlevel=maxlevel, maxrank=maxrank, flippable=fl,
                 sublattice=sublattice)
+
+
+# The operator inputs of the reference's shipped examples (example/*.toml): bcc graph (NN + NNN, the structure-constant
+# range 1.2 a_bcc) on a periodic cluster large enough for the closure, class-preserving operations with the z axis kept
+# (the monomial reduction group under which the start orbitals are one dimensional), the start site not flippable.
+# The augmented-space node counts of these inputs are printed by the reference ("nodes / sublattice" of
+# example/reference/*/asr.out).
+EXAMPLES = {
+    # name: (lattice, cluster l, levels, classes of the sublattices, species per class, concentrations per class)
+    "cuzn_alloy": ("bcc", 8, 4, ("a2",), ((1, 2),), ((0.5, 0.5),)),
+    "fe66ni14cr20_fcc": ("fcc", 8, 3, ("fcc",), ((1, 2, 3),), ((0.66, 0.14, 0.20),)),
+    "cuzn_b2": ("bcc", 12, 4, ("b2_a", "b2_b"), ((1,), (2,)), ((1.0,), (1.0,))),
+    "co2fe04cr06al_l21": ("bcc", 8, 4, ("l21_8c", "l21_4a", "l21_4b"), ((1,), (2,), (3, 4)), ((1.0,), (1.0,), (0.4, 0.6))),
+}
+_EXAMPLE_SHIFT = {"a2": (0, 0, 0), "fcc": (0, 0, 0), "b2_a": (0, 0, 0), "b2_b": (1, 1, 1),
+                  "l21_8c": (1, 1, 1), "l21_4a": (0, 0, 0), "l21_4b": (2, 0, 0)}
+
+
+def _example_classes(kind: str, coord: np.ndarray, shift) -> np.ndarray:
+    c = coord + np.asarray(shift, dtype=np.int64)[:, None]
+    if kind in ("a2", "fcc"):
+        return np.ones(coord.shape[1], np.int32)
+    odd = (c[0] % 2).astype(np.int64)
+    if kind.startswith("b2"):
+        return (1 + odd).astype(np.int32)          # 1: cube corners, 2: cube centres
+    half = (c.sum(axis=0) // 2) % 2
+    return np.where(odd == 1, 1, np.where(half == 0, 2, 3)).astype(np.int32)   # 1: 8c, 2: 4a, 3: 4b
+
+
+def example_case(name: str, sublattice: int = 1, seed: int = 0):
+    """Operator inputs of the reference example ``name`` with the start site on ``sublattice`` (1-based), the classes
+    relabelled so that the class list is that of the example; returns the case dict of ``cubic_case`` plus maxlevel."""
+    kind, l, levels, cnames, spcs, concs = EXAMPLES[name]
+    g, coord, bvec = lat.periodic_graph_shells(kind, l, 4)
+    cname = cnames[sublattice - 1]
+    cls = _example_classes(cname, coord, _EXAMPLE_SHIFT[cname])
+    if cname.startswith("b2"):
+        # classes of the example: 1 = sublattice a, 2 = sublattice b; with the shift, site 1 carries the start class
+        cls = np.where(cls == 1, sublattice, 3 - sublattice).astype(np.int32)
+    perm, mats = lat.class_ops(coord, 2 * l, cls)
+    dmat = lat.orbital_rep(mats)
+    block, block0 = sk_blocks(bvec, seed)
+    ncls = len(cnames)
+    ld = max(len(s) for s in spcs)
+    spc = np.zeros((ld, ncls), np.int32, order="F")
+    conc = np.zeros((ld, ncls), order="F")
+    for k in range(ncls):
+        spc[: len(spcs[k]), k] = spcs[k]
+        conc[: len(concs[k]), k] = concs[k]
+    nsp = int(max(max(s) for s in spcs))
+    mdl = ClassModel(nsp=nsp, nsc=np.array([len(s) for s in spcs], np.int32), spc=spc, conc=conc,
+                     block=np.asfortranarray(block.reshape(9, 9, -1, 1)), block0=np.asfortranarray(block0.reshape(9, 9, 1)))
+    fl = np.ones(g.n, np.int32)
+    fl[0] = 0
+    return dict(graph=g, coord=coord, bvec=bvec, cls=cls, perm=np.asfortranarray(perm, dtype=np.int32), dmat=np.asfortranarray(dmat),
+                model=mdl, maxlevel=levels, maxrank=1, flippable=fl)
