@@ -269,6 +269,41 @@ def plain_leg(torch):
             "dos_abs_error_vs_oracle": err}
 
 
+def example_leg(torch):
+    """Chain throughput on the node set of the reference's bcc Cu0.5Zn0.5 example (levels 4, 17,515 nodes; the count
+    of example/reference/cuzn_alloy/asr.out:105): 2 central species x start orbitals s, p_z, d_xy, d_3z2-r2 (one
+    dimensional under the class group), depth 24 with the depth test at 1e-5, 8 contours of 77 energies each.
+    chain-steps counts the levels each chain actually used; the whole host call (copies included) is timed, the way the
+    reference's wall-clock chain count is."""
+    import asr_b200 as A
+    from asr_b200 import contour as CT
+    from asr_b200 import synthetic as S
+    c = S.example_case("cuzn_alloy", 1)
+    op = A.build_augcls_operator(c["graph"], c["model"], c["cls"], c["perm"], c["dmat"], 1, c["maxlevel"],
+                                 maxrank=c["maxrank"], flippable=c["flippable"])
+    sp = S.draw_species(2, 7)
+    specs = []
+    for cen in (1, 2):
+        ed = S.edc_params(sp, cen)
+        for l0 in (1, 3, 5, 7):
+            specs.append(A.ChainSpec(c=ed["c"], d=ed["d"], o=ed["o"], e=ed["e"], pa=ed["pa"], pb=ed["pb"], frozen_sp=cen,
+                                     start_orb=l0, nlev=24))
+    z = np.concatenate([CT.contour_nodes(-1.2 - 0.02 * k, 0.2 + 0.01 * k, 77)[0] for k in range(8)])
+    A.chains_run(op, specs, z[:77], "edc", 1e-5, "hull", "fp64")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = A.chains_run(op, specs, z, "edc", 1e-5, "hull", "fp64")
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    steps = int(np.sum(r["m"]))
+    chains = int(r["m"].size)
+    val = steps / sec
+    return {"nodes": int(op.nn), "chains": chains, "mean_depth_used": steps / chains, "seconds": sec,
+            "chain_steps_per_s": val, "chains_per_s": chains / sec,
+            "published_chain_steps_per_s": 1.40e3, "ratio_to_published": val / 1.40e3,
+            "published_basis": "67 chains/s x 20.86 mean depth, 2 x 48 CPU threads (example/reference/cuzn_alloy/asr.out)"}
+
+
 def scf_model(l, maxlevel, precision):
     """The large batched SCF configuration: equiatomic 5-component fcc random alloy (Fe, Co, Ni, Cr, Mn-like parameters
     drawn from seed 4), spd 9 orbitals, spin-polarised (2 x 5 x 9 = 90 chain groups), depths U{20..32}, 64-point
@@ -370,6 +405,7 @@ def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
     out["fp64_peak_tflops"] = fp64_peak_tflops(torch)
     out["kpm"] = kpm_leg(torch)
     out["plain"] = plain_leg(torch)
+    out["example_cuzn"] = example_leg(torch)
     if args.scf:
         out["scf"] = scf_leg(torch, args.scf == 2)
     return out
