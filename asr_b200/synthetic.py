@@ -330,10 +330,12 @@ def _example_classes(kind: str, coord: np.ndarray, shift) -> np.ndarray:
     return np.where(odd == 1, 1, np.where(half == 0, 2, 3)).astype(np.int32)   # 1: 8c, 2: 4a, 3: 4b
 
 
-def example_case(name: str, sublattice: int = 1, seed: int = 0):
+def example_case(name: str, sublattice: int = 1, seed: int = 0, l: int | None = None):
     """Operator inputs of the reference example ``name`` with the start site on ``sublattice`` (1-based), the classes
-    relabelled so that the class list is that of the example; returns the case dict of ``cubic_case`` plus maxlevel."""
-    kind, l, levels, cnames, spcs, concs = EXAMPLES[name]
+    relabelled so that the class list is that of the example; returns the case dict of ``cubic_case`` plus maxlevel.
+    ``l`` overrides the periodic cluster (the examples' own: the supercell their published runs used)."""
+    kind, l0, levels, cnames, spcs, concs = EXAMPLES[name]
+    l = l0 if l is None else l
     g, coord, bvec = lat.periodic_graph_shells(kind, l, 4)
     cname = cnames[sublattice - 1]
     cls = _example_classes(cname, coord, _EXAMPLE_SHIFT[cname])
@@ -357,3 +359,72 @@ def example_case(name: str, sublattice: int = 1, seed: int = 0):
     fl[0] = 0
     return dict(graph=g, coord=coord, bvec=bvec, cls=cls, perm=np.asfortranarray(perm, dtype=np.int32), dmat=np.asfortranarray(dmat),
                 model=mdl, maxlevel=levels, maxrank=1, flippable=fl)
+
+
+def structure_blocks(bvec: np.ndarray, seed: int, ntype: int = 1):
+    """Bond blocks for float bond vectors (alat units): one set of two-centre integrals per shell of equal length, the
+    shells after the first scaled by 0.4; the same blocks for every translation type.  block (9, 9, nslot, ntype),
+    block0 (9, 9, ntype), Fortran order."""
+    rng = np.random.default_rng(seed)
+    r2 = np.round(np.sum(np.asarray(bvec, float) ** 2, axis=0), 6)
+    shells = sorted(set(float(x) for x in r2))
+    ints = {s: draw_two_centre(rng, 1.0 if i == 0 else 0.4) for i, s in enumerate(shells)}
+    ns = bvec.shape[1]
+    block = np.zeros((9, 9, ns, ntype), order="F")
+    for k in range(ns):
+        block[:, :, k, :] = sk_block(bvec[:, k], ints[float(r2[k])])[:, :, None]
+    on = rng.uniform(-0.2, 0.2, size=4)
+    b0 = np.diag([on[0], on[1], on[1], on[1], on[2], on[2], on[3], on[2], on[3]])
+    block0 = np.asfortranarray(np.repeat(b0[:, :, None], ntype, axis=2))
+    return block, block0
+
+
+# the reference examples as structures (primitive cells in units of the bcc / fcc cube edge, labels per sublattice);
+# species per class and concentrations as in EXAMPLES
+STRUCTURE_EXAMPLES = {
+    "cuzn_alloy": ("bcc", None, 4),
+    "fe66ni14cr20_fcc": ("fcc", None, 3),
+    "cuzn_b2": ("b2", None, 4),
+    # L2_1 with a = 2 a_bcc: fcc primitive cell of cube edge 2; 8c at (1/4, 1/4, 1/4) and (3/4, 3/4, 3/4) of the
+    # conventional cube (label 1), 4a at the origin (label 2), 4b at (1/2, 1/2, 1/2) (label 3)
+    "co2fe04cr06al_l21": ("l21", None, 4),
+}
+
+
+def example_structure(name: str):
+    """The Structure of reference example ``name``."""
+    from . import crystal as X
+    kind = STRUCTURE_EXAMPLES[name][0]
+    if kind != "l21":
+        return X.prototype_structure(kind)
+    avec = np.array([[0.0, 1.0, 1.0], [1.0, 0.0, 1.0], [1.0, 1.0, 0.0]])
+    cart = np.array([[0.5, 0.5, 0.5], [1.5, 1.5, 1.5], [0.0, 0.0, 0.0], [1.0, 1.0, 1.0]]).T
+    return X.Structure(avec, X.inv3(avec) @ cart, [1, 1, 2, 3])
+
+
+def structure_case(name: str, sublattice: int = 1, seed: int = 0, rcl: float = 1.2, levels: int | None = None,
+                   group: str = "reduction"):
+    """Operator inputs of reference example ``name`` built from its structure alone (crystal.sublattice_inputs): the
+    ball about the start site, the class-preserving site group, its start orbitals and weights, and the reduction group.
+    Returns the keys of ``example_case`` plus reps, weights, stype and the crystal graph."""
+    from . import crystal as X
+    _, _, lev = STRUCTURE_EXAMPLES[name]
+    levels = lev if levels is None else levels
+    spcs, concs = EXAMPLES[name][4], EXAMPLES[name][5]
+    s = example_structure(name)
+    ops = X.space_group(s)
+    inp = X.sublattice_inputs(s, ops, sublattice, rcl, levels, group=group)
+    _, ntype = X.translation_types(s)
+    block, block0 = structure_blocks(inp["cg"].bvec, seed, ntype)
+    ncls = len(spcs)
+    ld = max(len(x) for x in spcs)
+    spc = np.zeros((ld, ncls), np.int32, order="F")
+    conc = np.zeros((ld, ncls), order="F")
+    for k in range(ncls):
+        spc[: len(spcs[k]), k] = spcs[k]
+        conc[: len(concs[k]), k] = concs[k]
+    nsp = int(max(max(x) for x in spcs))
+    mdl = ClassModel(nsp=nsp, nsc=np.array([len(x) for x in spcs], np.int32), spc=spc, conc=conc, block=block, block0=block0)
+    return dict(graph=inp["graph"], cls=inp["cls"], perm=inp["perm"], dmat=inp["dmat"], model=mdl, maxlevel=levels, maxrank=1,
+                flippable=inp["flippable"], stype=inp["stype"], reps=inp["reps"], weights=inp["weights"], cg=inp["cg"],
+                site_group=inp["site_group"])
