@@ -31,7 +31,8 @@ EXPORTS = ["asr_version", "asr_last_error", "asr_ctx_create", "asr_ctx_destroy",
            "asr_chains_run", "asr_chains_run_dev", "asr_cf_eval", "asr_cf_adjoint",
     "asr_chains_adjoint", "asr_cf_eval_noalloc", "asr_ed3_blocks", "asr_supercell_build", "asr_supercell_free",
            "asr_supercell_apply", "asr_kpm_moments", "asr_kpm_dos", "asr_sro_layout", "asr_gauss_legendre", "asr_contour_nodes",
-           "asr_contour_nodes_closed", "asr_contour_nodes_fermi", "asr_contour_moment"]
+           "asr_contour_nodes_closed", "asr_contour_nodes_fermi", "asr_contour_moment", "asr_op_build_targets",
+           "asr_chains_proj"]
 
 
 class ChainGroup(C.Structure):
@@ -72,6 +73,7 @@ def lib():
     L.asr_ctx_launches.argtypes = [vp, i64_p]
     L.asr_op_build.argtypes = [vp, C.c_int, i_p, i_p, C.c_int, i_p, i_p, C.c_int, d_p, C.c_int, i_p, i_p, C.c_int, d_p, C.c_int,
                                C.c_int, C.c_int, i_p, i_p, d_p, C.c_int, C.c_int, d_p, C.POINTER(vp)]
+    L.asr_op_build_targets.argtypes = L.asr_op_build.argtypes[:-1] + [i_p, C.c_int, i_p, i_p, C.POINTER(vp)]
     L.asr_op_free.argtypes = [vp]
     L.asr_op_dims.argtypes = [vp, i_p]
     L.asr_op_export_tables.argtypes = [vp] + [i_p] * 8 + [d_p, d_p, i_p, i_p]
@@ -93,6 +95,8 @@ def lib():
     L.asr_cf_eval_noalloc.argtypes = [vp, d_p, d_p, i_p, C.c_int, C.c_int, d_p, C.c_int, C.c_int, d_p, i64_p]
     L.asr_chains_adjoint.argtypes = [vp, vp, C.POINTER(ChainGroup), C.c_int, d_p, C.c_int, d_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                      d_p, d_p]
+    L.asr_chains_proj.argtypes = [vp, vp, C.POINTER(ChainGroup), C.c_int, d_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, i_p,
+                                  i_p, d_p, d_p, d_p, d_p, i_p]
     L.asr_ed3_blocks.argtypes = [vp, vp, C.POINTER(Ed3Group), C.c_int, d_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, d_p,
                                  i_p, d_p, d_p, d_p]
     L.asr_supercell_build.argtypes = [vp, C.c_int, C.c_int, i_p, i_p, C.c_int, d_p, d_p, d_p, d_p, d_p, d_p, C.POINTER(vp)]

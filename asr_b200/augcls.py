@@ -192,11 +192,13 @@ class AugclsOp:
 
 
 def build_augcls_operator(g, mdl, cls, perm, dmat, start: int, maxlevel: int, maxrank: int | None = None, flippable=None,
-                          stype=None, ctx: Context | None = None) -> AugclsOp:
+                          stype=None, ctx: Context | None = None, tsite=None):
     """``build_augcls_operator`` (src/asr_augcls.f90:596-823) on the GPU.
 
     g: ``Graph`` (1-based CSR); mdl: ``ClassModel`` (nsc, spc, conc, block, block0, nsp); cls (nsite); perm (nsite, nop);
-    dmat (9, 9, nop); flippable (nsite, bool) and stype (nsite) optional."""
+    dmat (9, 9, nop); flippable (nsite, bool) and stype (nsite) optional.  With ``tsite`` (target graph sites, 1-based)
+    returns (op, tnode, tgop): tnode (nsmax, nt) the node of each target alone in local state k (1-based, 0: none) and
+    tgop (nsmax, nt) the operation mapping it onto that node (1-based), as the reference's optional outputs (:808-820)."""
     ctx = ctx or default_context()
     nbr_ptr, nbr = _i32(g.nbr_ptr), _i32(g.nbr)
     nsc, spc, conc = _i32(mdl.nsc), _i32(mdl.spc), _f64(mdl.conc)
@@ -210,7 +212,15 @@ def build_augcls_operator(g, mdl, cls, perm, dmat, start: int, maxlevel: int, ma
     if block0 is not None and block0.ndim == 2:
         block0 = np.asfortranarray(block0.reshape(9, 9, 1))
     h = C.c_void_p()
-    check(lib().asr_op_build(ctx.h, g.n, _pi(nbr_ptr), _pi(nbr), int(nsc.shape[0]), _pi(nsc), _pi(spc), spc.shape[0], _pd(conc),
-                             mdl.nsp, _pi(cls), _pi(perm), perm.shape[1], _pd(dmat), start, maxlevel, int(maxrank or 0), _pi(fl),
-                             _pi(st), _pd(block), block.shape[2], block.shape[3], _pd(block0), C.byref(h)))
-    return AugclsOp(ctx, h, mdl.nsp)
+    args = (ctx.h, g.n, _pi(nbr_ptr), _pi(nbr), int(nsc.shape[0]), _pi(nsc), _pi(spc), spc.shape[0], _pd(conc), mdl.nsp, _pi(cls),
+            _pi(perm), perm.shape[1], _pd(dmat), start, maxlevel, int(maxrank or 0), _pi(fl), _pi(st), _pd(block), block.shape[2],
+            block.shape[3], _pd(block0))
+    if tsite is None:
+        check(lib().asr_op_build(*args, C.byref(h)))
+        return AugclsOp(ctx, h, mdl.nsp)
+    ts = _i32(np.atleast_1d(tsite))
+    nsm = int(np.max(nsc))
+    tnode = np.zeros((nsm, ts.shape[0]), np.int32, order="F")
+    tgop = np.zeros((nsm, ts.shape[0]), np.int32, order="F")
+    check(lib().asr_op_build_targets(*args, _pi(ts), ts.shape[0], _pi(tnode), _pi(tgop), C.byref(h)))
+    return AugclsOp(ctx, h, mdl.nsp), tnode, tgop

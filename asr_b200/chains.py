@@ -4,6 +4,8 @@
   every (group, energy) chain of the energy-dependent route, or one real chain per group in the plain route, in lanes of
   32 chains per tile;
 * ``edc_green_blk`` -- ``edc_green_blk`` (src/asr_edc.f90:237-316) on the operator's current parameters;
+* ``chains_proj`` / ``edc_green_proj`` -- ``edc_green_proj`` (src/asr_edc.f90:174-232): the chains with their
+  first-order projections on target states (off-site elements for the Bloch spectral function);
 * ``lanczos`` -- the plain real chain (src/reference/asr_recursion.f90:17-58) on ``augcls_apply``;
 * ``cf_species`` -- terminated continued fractions (src/asr_chain.f90:67-167) for many (chain, energy) pairs.
 """
@@ -155,6 +157,46 @@ def edc_green_blk(op: AugclsOp, ed: dict, zs, iv: int, nlev: int, depth_tol: flo
     spec = ChainSpec(c=p["c"], d=p["d"], o=p["o"], e=p["e"], pa=pa, pb=pb, frozen_sp=0, start_orb=iv, nlev=nlev)
     r = chains_run(op, [spec], zs, "edc", depth_tol, tail, precision, project, coefs=True)
     return r["g"][:, 0], r["m"][:, 0], r["a"][:, :, 0], r["b"][:, :, 0]
+
+
+def chains_proj(op: AugclsOp, specs, z, tnode, tgop, tw, tail: str = "hull", precision: str = "fp64", project: bool = True):
+    """``edc_green_proj`` (src/asr_edc.f90:174-232) for every (group, energy): each chain runs its full depth and its
+    Lanczos vectors are projected on the target states.  tnode, tgop (nsmax, nt) from ``build_augcls_operator(...,
+    tsite=...)``; tw (9, nsmax, nt) or (9, nsmax, nt, ngroup) dressing weights.  Returns dict(g (nz, ngroup), gp, gp4
+    (9, nt, nz, ngroup), m (nz, ngroup)); gp4 uses the chain cut four steps earlier."""
+    z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
+    nz, ng = z.shape[0], len(specs)
+    tnode = np.asfortranarray(tnode, dtype=np.int32)
+    tgop = np.asfortranarray(tgop, dtype=np.int32)
+    nsm, nt = tnode.shape
+    tw = np.asarray(tw, dtype=np.float64)
+    if tw.ndim == 3:
+        tw = np.repeat(tw[..., None], ng, axis=3)
+    if tw.shape != (9, nsm, nt, ng):
+        raise ValueError(f"chains_proj: tw must be (9, {nsm}, {nt}[, {ng}]), got {tw.shape}")
+    tw = np.asfortranarray(tw)
+    arr, keep = _groups(specs)
+    g = np.zeros((ng, nz), np.complex128)
+    gp = np.zeros((ng, nz, nt, 9), np.complex128)
+    gp4 = np.zeros((ng, nz, nt, 9), np.complex128)
+    m = np.zeros((ng, nz), np.int32)
+    check(lib().asr_chains_proj(op.ctx.h, op.h, arr, ng, _pd(z), nz, _lib.TAILS[tail], PREC[precision], int(bool(project)), nt,
+                                _pi(tnode), _pi(tgop), _pd(tw), _pd(g), _pd(gp), _pd(gp4), _pi(m)))
+    return dict(g=g.T, gp=gp.transpose(3, 2, 1, 0), gp4=gp4.transpose(3, 2, 1, 0), m=m.T)
+
+
+def edc_green_proj(op: AugclsOp, ed: dict, z, iv: int, nlev: int, tnode, tgop, tw, tail: str = "hull", precision: str = "fp64",
+                   project: bool = True):
+    """``edc_green_proj`` (src/asr_edc.f90:174-232) at one energy on the operator's current parameters (as
+    ``edc_green_blk``): returns (g, gp (9, nt), gp4 (9, nt))."""
+    dc = np.asarray(ed["dc"], float)
+    dl = np.asarray(ed["dl"], float)
+    en = np.asarray(ed["enu"], float)
+    p = op.params
+    spec = ChainSpec(c=p["c"], d=p["d"], o=p["o"], e=p["e"], pa=np.asfortranarray(1.0 - dc[:, None] / dl),
+                     pb=np.asfortranarray(dc[:, None] * en / dl), frozen_sp=0, start_orb=iv, nlev=nlev)
+    r = chains_proj(op, [spec], np.atleast_1d(z), tnode, tgop, tw, tail, precision, project)
+    return r["g"][0, 0], r["gp"][:, :, 0, 0], r["gp4"][:, :, 0, 0]
 
 
 def lanczos(op: AugclsOp, l0: int, nmax: int, precision: str = "fp64"):

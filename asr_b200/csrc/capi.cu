@@ -312,10 +312,11 @@ int asr_ctx_stats(const asr_ctx* ctx, int64_t* nchain, int64_t* nlev, int64_t* n
   return ASR_OK;
 }
 
-int asr_op_build(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc, int ldspc,
-                 const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat, int start,
-                 int maxlevel, int maxrank, const int* flippable, const int* stype, const double* block, int nblock_slots,
-                 int ntype_blocks, const double* block0, asr_op** out) {
+static int op_build(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc, int ldspc,
+                    const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat, int start,
+                    int maxlevel, int maxrank, const int* flippable, const int* stype, const double* block, int nblock_slots,
+                    int ntype_blocks, const double* block0, const int* tsite, int ntarget, int* tnode, int* tgop,
+                    asr_op** out) {
   if (!ctx || !out || !nbr_ptr || !nbr || !nsc || !spc || !conc || !cls || !perm || !dmat || !block) {
     set_error("asr_op_build: null argument");
     return ASR_EINVAL;
@@ -348,7 +349,8 @@ int asr_op_build(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, in
   op->nsc.assign(nsc, nsc + ncls);
   op->ldspc = ldspc;
   op->spc.assign(spc, spc + (size_t)ldspc * ncls);
-  int rc = build_operator(ctx, nsite, nbr_ptr, nbr, ncls, nsc, cls, perm, nop, start, maxlevel, maxrank, flippable, stype, op);
+  int rc = build_operator(ctx, nsite, nbr_ptr, nbr, ncls, nsc, cls, perm, nop, start, maxlevel, maxrank, flippable, stype, op,
+                          tsite, ntarget, tnode, tgop);
   if (rc != ASR_OK) { free_op(op); return rc; }
   const int nsm = op->nsmax;
   op->mt.assign((size_t)nsm * nsm * nsm * ncls, 0.0);
@@ -361,6 +363,27 @@ int asr_op_build(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, in
   op->start_l = 1;
   *out = op;
   return ASR_OK;
+}
+
+int asr_op_build(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc, int ldspc,
+                 const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat, int start,
+                 int maxlevel, int maxrank, const int* flippable, const int* stype, const double* block, int nblock_slots,
+                 int ntype_blocks, const double* block0, asr_op** out) {
+  return op_build(ctx, nsite, nbr_ptr, nbr, ncls, nsc, spc, ldspc, conc, nsp, cls, perm, nop, dmat, start, maxlevel, maxrank,
+                  flippable, stype, block, nblock_slots, ntype_blocks, block0, nullptr, 0, nullptr, nullptr, out);
+}
+
+int asr_op_build_targets(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc,
+                         int ldspc, const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat,
+                         int start, int maxlevel, int maxrank, const int* flippable, const int* stype, const double* block,
+                         int nblock_slots, int ntype_blocks, const double* block0, const int* tsite, int ntarget, int* tnode,
+                         int* tgop, asr_op** out) {
+  if (ntarget < 0 || (ntarget > 0 && (!tsite || !tnode || !tgop))) {
+    set_error("asr_op_build_targets: tsite needs tnode and tgop");
+    return ASR_EINVAL;
+  }
+  return op_build(ctx, nsite, nbr_ptr, nbr, ncls, nsc, spc, ldspc, conc, nsp, cls, perm, nop, dmat, start, maxlevel, maxrank,
+                  flippable, stype, block, nblock_slots, ntype_blocks, block0, tsite, ntarget, tnode, tgop, out);
 }
 
 int asr_op_free(asr_op* op) {
@@ -835,6 +858,75 @@ int asr_chains_run(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int 
   cudaFree(d_z);
   cudaFree(d_g);
   return rc;
+}
+
+// edc_green_proj (src/asr_edc.f90:174-232) for every (group, energy): all nlev steps (no depth test), g (nz, ngroup),
+// gp / gp4 (9, nt, nz, ngroup) complex, mused (nz, ngroup) optional.  tnode, tgop (nsmax, nt) 1-based as returned by
+// asr_op_build_targets; tw (9, nsmax, nt, ngroup) the dressing weights of every group.
+int asr_chains_proj(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz, int tail,
+                    int precision, int project, int nt, const int* tnode, const int* tgop, const double* tw, double* g,
+                    double* gp, double* gp4, int* mused) {
+  if (!ctx || !op || !groups || ngroup < 1 || !z || nz < 1 || nt < 1 || !tnode || !tgop || !tw || !g || !gp || !gp4) {
+    set_error("asr_chains_proj: bad argument");
+    return ASR_EINVAL;
+  }
+  if (tail < 0 || tail > 3) { set_error("asr_chains_proj: unknown tail"); return ASR_EINVAL; }
+  const int nsm = op->nsmax;
+  std::vector<int> tn((size_t)nsm * nt), tg((size_t)nsm * nt);
+  for (size_t q = 0; q < tn.size(); ++q) {
+    if (tnode[q] < 0 || tnode[q] > op->nn) { set_error("asr_chains_proj: target node out of range"); return ASR_EINVAL; }
+    if (tnode[q] > 0 && (tgop[q] < 1 || tgop[q] > op->nop)) { set_error("asr_chains_proj: target operation out of range"); return ASR_EINVAL; }
+    tn[q] = tnode[q] - 1;
+    tg[q] = tnode[q] > 0 ? tgop[q] - 1 : 0;
+  }
+  ASR_TRY(set_device(ctx));
+  cudaStream_t s = ctx->stream;
+  GroupLayout GL = layout(op);
+  std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
+  std::vector<GroupInfo> gi(ngroup);
+  for (int q = 0; q < ngroup; ++q) {
+    const asr_chain_group& G = groups[q];
+    if (!G.c || !G.d) { set_error("asr_chains_proj: group %d without c or d", q + 1); return ASR_EINVAL; }
+    if (G.nlev < 1 || G.nlev > NLMAX) { set_error("asr_chains_proj: depth %d out of range 1..%d", G.nlev, NLMAX); return ASR_EINVAL; }
+    ASR_TRY(make_group(op, GL, G.c, G.d, G.o, G.e, G.pa, G.pb, G.frozen_sp, G.start_orb, G.nlev, nullptr,
+                       blob.data() + (size_t)GL.stride * q, gi[q]));
+  }
+  RunOptions opt;
+  opt.mode = ASR_MODE_EDC;
+  opt.depth_tol = 0.0;   // edc_green_proj runs every step
+  opt.tail = tail;
+  opt.precision = precision;
+  opt.project = project;
+  const int nlane = ngroup * nz;
+  const size_t nout = (size_t)nlane * 9 * nt;
+  std::vector<int> lg(nlane);
+  for (int q = 0; q < ngroup; ++q)
+    for (int j = 0; j < nz; ++j) lg[(size_t)q * nz + j] = q;
+  std::vector<double2> lz(nlane);
+  for (int q = 0; q < ngroup; ++q)
+    for (int j = 0; j < nz; ++j) lz[(size_t)q * nz + j] = make_double2(z[2 * j], z[2 * j + 1]);
+  Dev<double2> d_lz, d_g, d_gp, d_gp4;
+  Dev<int> d_tn, d_tg;
+  Dev<double> d_tw;
+  ASR_TRY(d_lz.alloc(nlane)); ASR_TRY(d_g.alloc(nlane)); ASR_TRY(d_gp.alloc(nout)); ASR_TRY(d_gp4.alloc(nout));
+  ASR_TRY(d_tn.alloc(tn.size())); ASR_TRY(d_tg.alloc(tg.size())); ASR_TRY(d_tw.alloc((size_t)9 * nsm * nt * ngroup));
+  ASR_CUDA(cudaMemcpyAsync(d_lz.p, lz.data(), nlane * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_tn.p, tn.data(), tn.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_tg.p, tg.data(), tg.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_tw.p, tw, (size_t)9 * nsm * nt * ngroup * sizeof(double), cudaMemcpyHostToDevice, s));
+  ProjSpec P;
+  P.nt = nt; P.nsm = nsm; P.tnode = d_tn.p; P.tgop = d_tg.p; P.tw = d_tw.p; P.gp = d_gp.p; P.gp4 = d_gp4.p;
+  std::vector<int> hm;
+  int64_t nfall = 0, nsteps = 0;
+  ASR_TRY(run_lanes(ctx, op, gi, blob, GL, lg, d_lz.p, nlane, opt, d_g.p, nullptr, nullptr, &hm, &nfall, &nsteps, &P));
+  ASR_CUDA(cudaMemcpyAsync(g, d_g.p, nlane * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(gp, d_gp.p, nout * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(gp4, d_gp4.p, nout * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  if (mused) for (int L = 0; L < nlane; ++L) mused[L] = hm[L];
+  ctx->nchain += nlane;
+  ctx->nfall += nfall;
+  return ASR_OK;
 }
 
 int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain, const double* z, int nz, int tail,

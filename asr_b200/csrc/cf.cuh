@@ -166,6 +166,25 @@ __host__ __device__ inline double2 cf_species_f_dev(const double2* a, const doub
   return gt[0];
 }
 
+// cf_species with the factors pv_k = [g]_{k1} = gt_1 prod_{j<k} (b_j gt_{j+1}) of the projections f = sum_k c_k pv_k
+// (src/asr_chain.f90:111-122, the pv output used by edc_green_proj); pv (m) receives them, the return value is g11.
+__host__ __device__ inline double2 cf_species_pv_dev(const double2* a, const double2* b, int m, double2 z, int tail, double2* pv,
+                                                     double2* wd, double2* we, int* nfall) {
+  double2 aa, bb;
+  cf_tail_dev(a, b, m, tail, wd, we, nfall, aa, bb);
+  double2 tl = cf_tail_term(z, aa, bb);
+  double2 one = make_double2(1.0, 0.0);
+  pv[m - 1] = cdiv(one, csub(csub(z, a[m - 1]), tl));   // gt in place, then turned into the products
+  for (int j = m - 2; j >= 0; --j) pv[j] = cdiv(one, csub(csub(z, a[j]), cmul(cmul(b[j], b[j]), pv[j + 1])));
+  double2 g11 = pv[0], prod = pv[0];
+  for (int k = 0; k < m; ++k) {
+    double2 gnext = k < m - 1 ? pv[k + 1] : make_double2(0.0, 0.0);
+    pv[k] = prod;
+    if (k < m - 1) prod = cmul(prod, cmul(b[k], gnext));
+  }
+  return g11;
+}
+
 // ---- real chains (plain mode)
 __host__ __device__ inline int sturm_count(int n, const double* d, const double* e, double x) {
   int cnt = 0;

@@ -738,6 +738,72 @@ __global__ void k_gather_z(int nlane, const int* lmap, const double2* z_all, dou
   if (L < nlane) z[L] = lmap[L] >= 0 ? z_all[lmap[L]] : make_double2(0.0, 0.0);
 }
 
+// projections of u_k on the target states (edc_green_proj, src/asr_edc.f90:196-202): one warp per (tile, target),
+// cpr(k, l, t) = sum_ks tw(l, ks, t) psi(node ks of t, l) with psi = chi(g) sg(l, g) u(r, pi(l, g)) in amplitude
+// coordinates (augcls_amp_c, src/asr_augcls.f90:251-261: the normalised v(r) over sqrt(orbit size)), times the lane
+// scale of the stored vector
+template <typename ST>
+__global__ void k_proj_gather(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ u, ProjView P, int k) {
+  const int lane = threadIdx.x % TL;
+  const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) / TL;
+  const int tile = (int)(warp / P.nt), t = (int)(warp % P.nt);
+  if (tile >= bv.ntile) return;
+  const int L = tile * TL + lane;
+  const int grp = bv.lane_group[L];
+  double2 acc[9];
+  for (int l = 0; l < 9; ++l) acc[l] = make_double2(0.0, 0.0);
+  if (grp >= 0) {
+    const double2 su = bv.su[L];
+    const unsigned long long chim = bv.ginfo[grp].chimask;
+    const double* tw = P.tw + ((size_t)grp * P.nt + t) * 9 * P.nsm;
+    for (int ks = 0; ks < P.nsm; ++ks) {
+      const int r = P.tnode[ks + P.nsm * t];
+      if (r < 0) continue;
+      const int g = P.tgop[ks + P.nsm * t];
+      const double chi = ((chim >> g) & 1ull) ? -1.0 : 1.0;
+      const unsigned sgm = op.sgm[g];
+      for (int l = 0; l < 9; ++l) {
+        const int pl = op.pi[l + 9 * g];
+        const double wgt = tw[l + 9 * ks] * chi * (((sgm >> l) & 1u) ? -1.0 : 1.0);
+        const double2 x = ld(u + vix(tile, bv.nn, r, pl) + lane);
+        acc[l] = cadd(acc[l], cscale(x, wgt));
+      }
+    }
+    for (int l = 0; l < 9; ++l) acc[l] = cmul(acc[l], su);
+  }
+  double2* dst = P.cpr + (((size_t)tile * P.kcap + (k - 1)) * 9 * P.nt + (size_t)t * 9) * TL + lane;
+  for (int l = 0; l < 9; ++l) dst[(size_t)l * TL] = acc[l];
+}
+
+// gp(l, t) = sum_k cpr(k, l, t) pv_k with pv of cf_species at depth m, and gp4 the same at max(1, m - 4)
+// (src/asr_edc.f90:221-231); one thread per lane
+__global__ void k_proj_final(BatchView bv, int nlane, const int* lmap, ProjView P) {
+  int L = blockIdx.x * blockDim.x + threadIdx.x;
+  if (L >= nlane) return;
+  int dst = lmap[L];
+  if (bv.lane_group[L] < 0 || dst < 0) return;
+  const int tile = L / TL, lane = L % TL, m = bv.lane_m[L];
+  double2 pv[NLMAX], wd[NLMAX], we[NLMAX];
+  int nf = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    double2* out = (pass == 0 ? P.gp : P.gp4) + (size_t)dst * P.nt * 9;
+    const int mm = pass == 0 ? m : (m - 4 > 1 ? m - 4 : 1);
+    if (m < 1) {
+      for (int q = 0; q < 9 * P.nt; ++q) out[q] = make_double2(0.0, 0.0);
+      continue;
+    }
+    cf_species_pv_dev(bv.acoef + (size_t)L * NLMAX, bv.bcoef + (size_t)L * NLMAX, mm, bv.lane_z[L], bv.tail, pv, wd, we,
+                      pass == 0 ? &nf : nullptr);
+    for (int q = 0; q < 9 * P.nt; ++q) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int kk = 0; kk < mm; ++kk)
+        acc = cadd(acc, cmul(P.cpr[(((size_t)tile * P.kcap + kk) * 9 * P.nt + q) * TL + lane], pv[kk]));
+      out[q] = acc;
+    }
+  }
+  if (nf) atomicAdd(bv.nfall, nf);
+}
+
 // start vectors: U = e_(node 0, l0) with scale 1, UP = 0
 template <typename ST>
 __global__ void k_init(BatchView bv, typename St2<ST>::T* u, typename St2<ST>::T* up) {
@@ -756,24 +822,6 @@ __global__ void k_init(BatchView bv, typename St2<ST>::T* u, typename St2<ST>::T
     stv(up + q, make_double2(0.0, 0.0));
   }
 }
-
-template <typename T>
-struct Dev {
-  T* p = nullptr;
-  size_t n = 0;
-  ~Dev() { if (p) cudaFree(p); }
-  int alloc(size_t m) {
-    if (m <= n && p) return ASR_OK;
-    if (p) cudaFree(p);
-    p = nullptr; n = 0;
-    if (cudaMalloc(&p, std::max<size_t>(m, 1) * sizeof(T)) != cudaSuccess) {
-      set_error("chains: device allocation of %zu bytes failed", m * sizeof(T));
-      return ASR_ENOMEM;
-    }
-    n = m;
-    return ASR_OK;
-  }
-};
 
 size_t smul_smem(const asr_op* op, size_t st_size) {
   size_t b = (size_t)op->ntype * (op->nslot + 1) * 9 * RW * st_size;
@@ -855,7 +903,7 @@ template <typename ST>
 int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
                 const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
                 const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
-                std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out) {
+                std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj) {
   typedef typename St2<ST>::T T2;
   cudaStream_t s = ctx->stream;
   const int nn = op->nn;
@@ -888,7 +936,9 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   // ternary workload: FP64 best at 16 tiles, FP32 at 8 with 4 nodes per warp)
   int tpb = opt.tiles_per_batch > 0 ? opt.tiles_per_batch : (std::is_same<ST, double>::value ? 16 : 8);
   if (const char* e = getenv("ASR_TILES_PER_BATCH")) tpb = std::max(1, atoi(e));
-  while (tpb > 1 && (size_t)tpb * nvec * vec_bytes > freeb / 2) tpb /= 2;
+  // projections: per tile nlevmax x 9 nt x 32 complex values
+  const size_t proj_tile_bytes = proj ? (size_t)nlevmax * 9 * proj->nt * TL * sizeof(double2) : 0;
+  while (tpb > 1 && (size_t)tpb * (nvec * vec_bytes + proj_tile_bytes) > freeb / 2) tpb /= 2;
   tpb = std::min(tpb, ntile_all);
   int npw = std::max(1, opt.nodes_per_warp);
   if (const char* e = getenv("ASR_NODES_PER_WARP")) npw = std::max(1, atoi(e));
@@ -911,6 +961,12 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   ASR_TRY(d_sup.alloc(nlp)); ASR_TRY(d_part.alloc((size_t)tpb * bpt * TL)); ASR_TRY(d_z.alloc(nlp));
   Dev<T2> V[7];
   for (int q = 0; q < nvec; ++q) ASR_TRY(V[q].alloc((size_t)tpb * nn * 9 * TL));
+  Dev<double2> d_cpr;
+  ProjView PV{0, 1, nlevmax, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  if (proj) {
+    ASR_TRY(d_cpr.alloc((size_t)tpb * nlevmax * 9 * proj->nt * TL));
+    PV = ProjView{proj->nt, proj->nsm, nlevmax, proj->tnode, proj->tgop, proj->tw, d_cpr.p, proj->gp, proj->gp4};
+  }
   ASR_CUDA(cudaMemsetAsync(d_nfall.p, 0, sizeof(int), s));
   if (a_out) { a_out->assign((size_t)nlane * NLMAX, make_double2(0, 0)); b_out->assign((size_t)nlane * NLMAX, make_double2(0, 0)); }
   if (m_out) m_out->assign(nlane, 0);
@@ -973,6 +1029,11 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
       T2* U = V[k % 3].p;
       T2* UP = V[(k + 2) % 3].p;
       T2* Y = V[(k + 1) % 3].p;
+      if (proj) {   // projections of u_k before the operator step (src/asr_edc.f90:196-202)
+        const long nwarp = (long)nt * proj->nt;
+        k_proj_gather<ST><<<(unsigned)((nwarp * TL + 255) / 256), 256, 0, s>>>(op->view(), bv, U, PV, k);
+        ctx->launches += 1;
+      }
       if (ctx->profile) ASR_CUDA(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used], s));
       ASR_TRY(step_apply<ST>(ctx, op, bv, fused, any_o, all_dunif, U, Y, nvec > 3 ? V[3].p : nullptr, nvec > 3 ? V[4].p : nullptr,
                              nvec > 5 ? V[5].p : nullptr, nvec > 5 ? V[6].p : nullptr, d_part.p, npw, gridb));
@@ -993,6 +1054,10 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
     ASR_CUDA(cudaGetLastError());
     if (opt.mode == ASR_MODE_EDC && d_g_out) {
       k_cf_final<<<(nlp + 63) / 64, 64, 0, s>>>(bv, nlp, d_lmap.p, d_g_out);
+      ctx->launches += 1;
+    }
+    if (proj && opt.mode == ASR_MODE_EDC) {
+      k_proj_final<<<(nlp + 63) / 64, 64, 0, s>>>(bv, nlp, d_lmap.p, PV);
       ctx->launches += 1;
     }
     k_scatter_m<<<(nlp + 127) / 128, 128, 0, s>>>(nlp, d_lmap.p, d_m.p, d_m_all.p);
@@ -2020,14 +2085,14 @@ int run_ed3(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const
 int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
               const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
               const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
-              std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out) {
+              std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj) {
   smem_attrs();
   if (smul_smem(op, sizeof(double)) > 96 * 1024) { set_error("chains: bond tables above 96 KB of shared memory"); return ASR_EINVAL; }
   if (opt.precision == ASR_FP32)
     return run_lanes_t<float>(ctx, op, ginfo, gblob, GL, lane_group, d_lane_z, nlane, opt, d_g_out, a_out, b_out, m_out, nfall_out,
-                              nsteps_out);
+                              nsteps_out, proj);
   return run_lanes_t<double>(ctx, op, ginfo, gblob, GL, lane_group, d_lane_z, nlane, opt, d_g_out, a_out, b_out, m_out, nfall_out,
-                             nsteps_out);
+                             nsteps_out, proj);
 }
 
 // ------------------------------------------------------------------------------------------------ drop-in applications

@@ -65,11 +65,55 @@ struct RunOptions {
   int nodes_per_warp = 4;
 };
 
+// owning device buffer (freed on scope exit)
+template <typename T>
+struct Dev {
+  T* p = nullptr;
+  size_t n = 0;
+  Dev() = default;
+  Dev(const Dev&) = delete;
+  Dev& operator=(const Dev&) = delete;
+  ~Dev() { if (p) cudaFree(p); }
+  int alloc(size_t m) {
+    if (m <= n && p) return ASR_OK;
+    if (p) cudaFree(p);
+    p = nullptr; n = 0;
+    if (cudaMalloc(&p, (m > 0 ? m : 1) * sizeof(T)) != cudaSuccess) {
+      set_error("chains: device allocation of %zu bytes failed", m * sizeof(T));
+      return ASR_ENOMEM;
+    }
+    n = m;
+    return ASR_OK;
+  }
+};
+
+// Projections of every Lanczos vector on target states (edc_green_proj, src/asr_edc.f90:174-232), device arrays:
+// tnode (nsm, nt) 0-based node (-1: none), tgop (nsm, nt) 0-based operation, tw (9, nsm, nt, ngroup) dressing weights;
+// outputs gp, gp4 (9, nt) per output lane (complex), gp4 with the chain cut four steps earlier.
+struct ProjSpec {
+  int nt = 0, nsm = 1;
+  const int* tnode = nullptr;
+  const int* tgop = nullptr;
+  const double* tw = nullptr;
+  double2* gp = nullptr;
+  double2* gp4 = nullptr;
+};
+struct ProjView {
+  int nt, nsm, kcap;
+  const int* tnode;
+  const int* tgop;
+  const double* tw;
+  double2* cpr;    // [tile][k][t * 9 + l][lane]
+  double2* gp;
+  double2* gp4;
+};
+
 // Runs chains for lanes (group, z) on the operator; results per lane: g (energy of the lane), a, b (NLMAX each), m.
+// proj (optional): the projections of edc_green_proj for every lane.
 int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
               const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
               const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
-              std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out);
+              std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj = nullptr);
 
 // route ed3: two chains per (group, energy) (lane kind 0: from |a>, 1: from |v>); per lane g, the projection f, the start
 // norms |a|, |v| and the depth

@@ -329,6 +329,31 @@ __global__ void k_tables(BuildView B, int nn, int nslot, const int* nkey, const 
   }
 }
 
+// target links (src/asr_augcls.f90:808-820): for target t and local state k, the site alone in state k (every other site
+// in its reference state) canonicalised and looked up; tnode 1-based (0: not in the node set), tgop 1-based operation
+__global__ void k_targets(BuildView B, int nt, const int* tsite, const int* nkey, const int* table, uint32_t tmask,
+                          const int* cls, const int* nsc, const int* canflip, int start_site, int* tnode, int* tgop) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nt * B.nsm) return;
+  int t = q / B.nsm, k = q % B.nsm;
+  int r = tsite[t];
+  tnode[q] = 0;
+  tgop[q] = 1;
+  if (k >= nsc[cls[r - 1] - 1]) return;
+  if (k > 0 && (r == start_site || !canflip[r - 1])) return;
+  int cc[RMAX + 1], ccf[RMAX], key[RMAX + 1];
+  int n = 0;
+  if (k > 0) cc[n++] = r * B.nsm + k;
+  if (n > B.R) return;
+  int cs, osz, gb;
+  canon_node(B, r, cc, n, ccf, cs, osz, gb);
+  key[0] = cs;
+  for (int p = 0; p < B.R; ++p) key[1 + p] = p < n ? ccf[p] : INT_MAX;
+  int j = find_node(B.W, key, nkey, table, tmask);
+  tgop[q] = gb + 1;
+  if (j >= 0) tnode[q] = j + 1;
+}
+
 // ---------------------------------------------------------------------------------------------------- host side
 template <typename T>
 struct DBuf {
@@ -390,7 +415,7 @@ inline int blocks(long n, int bs) { return (int)((n + bs - 1) / bs); }
 
 int build_operator(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* cls,
                    const int* perm, int nop, int start, int maxlevel, int maxrank, const int* flippable, const int* stype,
-                   asr_op* op) {
+                   asr_op* op, const int* tsite, int ntarget, int* tnode, int* tgop) {
   cudaStream_t s = ctx->stream;
   // ---- checks of the reference (src/asr_augcls.f90:620-637)
   for (int i = 0; i < nsite; ++i)
@@ -549,6 +574,20 @@ int build_operator(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, 
   k_tables<<<blocks(nn, 128), 128, 0, s>>>(B, nn, nslot, nkey.p, norb.p, table.p, tcap - 1, d_cls.p, d_nsc.p, d_canflip.p,
                                            d_stype.p, start, T);
   ASR_TRY(check_err(ctx, "tables"));
+  if (tsite && ntarget > 0) {
+    for (int t = 0; t < ntarget; ++t)
+      if (tsite[t] < 1 || tsite[t] > nsite) { set_error("build_augcls_operator: target site out of range"); return ASR_EINVAL; }
+    const int nq = ntarget * nsm;
+    DBuf<int> d_ts, d_tn, d_tg;
+    ASR_TRY(d_ts.alloc(ntarget)); ASR_TRY(d_tn.alloc(nq)); ASR_TRY(d_tg.alloc(nq));
+    ASR_CUDA(cudaMemcpyAsync(d_ts.p, tsite, ntarget * sizeof(int), cudaMemcpyHostToDevice, s));
+    k_targets<<<blocks(nq, 128), 128, 0, s>>>(B, ntarget, d_ts.p, nkey.p, table.p, tcap - 1, d_cls.p, d_nsc.p, d_canflip.p,
+                                             start, d_tn.p, d_tg.p);
+    ASR_CUDA(cudaMemcpyAsync(tnode, d_tn.p, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaMemcpyAsync(tgop, d_tg.p, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaStreamSynchronize(s));
+    ASR_TRY(check_err(ctx, "targets"));
+  }
   ASR_CUDA(cudaGetLastError());
   op->nn = nn; op->nslot = nslot; op->nsmax = nsm; op->nop = nop; op->ncls = ncls; op->nsite = nsite; op->nstab = nstab;
   op->start_site = start;

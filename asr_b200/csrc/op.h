@@ -88,7 +88,7 @@ namespace asrb {
 // graph_build.cu
 int build_operator(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* cls,
                    const int* perm, int nop, int start, int maxlevel, int maxrank, const int* flippable, const int* stype,
-                   asr_op* op);
+                   asr_op* op, const int* tsite = nullptr, int ntarget = 0, int* tnode = nullptr, int* tgop = nullptr);
 // host helpers (capi.cu)
 void class_mt(const double* conc, int nsc, int nsm, double* mt);
 }  // namespace asrb

@@ -72,6 +72,15 @@ int asr_op_build(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, in
                  int ldspc, const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat,
                  int start, int maxlevel, int maxrank, const int* flippable, const int* stype, const double* block,
                  int nblock_slots, int ntype_blocks, const double* block0, asr_op** op);
+/* build_augcls_operator with its optional targets (src/asr_augcls.f90:589-596, :808-820): for target graph site tsite(t)
+ * and local state k = 0 .. nsc - 1 (the site alone in state k, every other site in its reference state),
+ * tnode(k + 1, t) = the representative node (1-based; 0: not in the node set or the site cannot flip) and tgop(k + 1, t)
+ * the operation that maps the node onto it (1-based), both (nsmax, ntarget) with nsmax = max(nsc). */
+int asr_op_build_targets(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc,
+                         int ldspc, const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat,
+                         int start, int maxlevel, int maxrank, const int* flippable, const int* stype, const double* block,
+                         int nblock_slots, int ntype_blocks, const double* block0, const int* tsite, int ntarget, int* tnode,
+                         int* tgop, asr_op** op);
 /* augcls_free (src/asr_augcls.f90:569-585) */
 int asr_op_free(asr_op* op);
 /* dims: nn, nslot, nsmax, nop, ncls, ntype, nstab, nsp */
@@ -125,6 +134,16 @@ int asr_chains_run(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int 
 int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const void* z_dev, int nz,
                        int mode, double depth_tol, int tail, int precision, int project, void* g_dev, double* a, double* b,
                        int* mused);
+
+/* edc_green_proj (src/asr_edc.f90:174-232) for every (group, energy): each chain runs its full depth (no depth test) and
+ * every Lanczos vector is projected on the target states, cpr(k, l, t) = sum_ks tw(l, ks, t) psi_k(node ks of t, l) with
+ * psi the unreduced amplitude (augcls_amp_c, src/asr_augcls.f90:251-261); gp(l, t) = sum_k cpr(k, l, t) pv_k with pv of
+ * cf_species, gp4 the same with the chain cut four steps earlier.  tnode, tgop (nsmax, nt) as returned by
+ * asr_op_build_targets; tw (9, nsmax, nt, ngroup) dressing weights per group (spectral_dressing, src/asr_spectral.f90:200-229).
+ * Outputs g (nz, ngroup), gp and gp4 (9, nt, nz, ngroup) complex, mused (nz, ngroup) or NULL. */
+int asr_chains_proj(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz, int tail,
+                    int precision, int project, int nt, const int* tnode, const int* tgop, const double* tw, double* g,
+                    double* gp, double* gp4, int* mused);
 
 /* ---- route ed3 (src/asr_ed3.f90): chains on z - K'(z), K' = et - h' + u h' + h' u - h' Qt h', h' = g + d S d ---------- */
 typedef struct asr_ed3_group {

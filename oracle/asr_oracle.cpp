@@ -209,10 +209,12 @@ struct Op {
 // src/asr_augcls.f90:596-823 (build_augcls_operator)
 // graph: nbr_ptr(n+1), nbr (1-based); conc(ldspc, ncls); cls(n); perm(n, nop); dmat(9,9,nop); flippable (n) or null;
 // stype (n) or null; block(9,9,nsb,ntype) with nsb >= nslot; block0(9,9,ntype) or null.
-extern "C" int orc_build(int n, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc, int ldspc,
-                         const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat,
-                         int start, int maxlevel, int maxrank, const int* flippable, const int* stype,
-                         const double* block, int nsb, int ntb, const double* block0, void** handle) {
+// tsite (ntarget, 1-based sites) optional: target links tnode(nsm, ntarget) (1-based node, 0 absent), tgop (1-based op)
+static int build_impl(int n, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc, int ldspc,
+                      const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat,
+                      int start, int maxlevel, int maxrank, const int* flippable, const int* stype,
+                      const double* block, int nsb, int ntb, const double* block0, const int* tsite, int ntarget, int* tnode,
+                      int* tgop, void** handle) {
   *handle = nullptr;
   for (int i = 0; i < n; ++i) if (perm[i] != i + 1) return fail("build_augcls_operator: operation 1 must be the identity");
   for (int g = 0; g < nop; ++g) {
@@ -374,8 +376,37 @@ extern "C" int orc_build(int n, const int* nbr_ptr, const int* nbr, int ncls, co
       if (jj > 0) { op->hopr[k + (size_t)ns * i] = jj; op->hopg[k + (size_t)ns * i] = gb; }
     }
   }
+  // target links (src/asr_augcls.f90:808-820): site r alone in local state k, every other site in its reference state
+  for (int t = 0; tsite && t < ntarget; ++t) {
+    int r = tsite[t];
+    for (int k = 0; k < nsm; ++k) { tnode[k + (size_t)nsm * t] = 0; tgop[k + (size_t)nsm * t] = 1; }
+    if (r < 1 || r > n) { delete op; return fail("build_augcls_operator: target site out of range"); }
+    for (int k = 0; k < nsc[cls[r - 1] - 1]; ++k) {
+      if (k > 0 && (r == start || !canflip[r - 1])) continue;
+      std::vector<int> tmp = set_state(cfg0, r, k, nsm);
+      canon_node(perm, n, nop, nsm, r, tmp, cs, ccf, osz, gb);
+      tnode[k + (size_t)nsm * t] = st.find(cs, ccf.data(), (int)ccf.size());
+      if (tnode[k + (size_t)nsm * t] < 0) tnode[k + (size_t)nsm * t] = 0;
+      tgop[k + (size_t)nsm * t] = gb;
+    }
+  }
   *handle = op;
   return 0;
+}
+extern "C" int orc_build(int n, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc, int ldspc,
+                         const double* conc, int nsp, const int* cls, const int* perm, int nop, const double* dmat,
+                         int start, int maxlevel, int maxrank, const int* flippable, const int* stype,
+                         const double* block, int nsb, int ntb, const double* block0, void** handle) {
+  return build_impl(n, nbr_ptr, nbr, ncls, nsc, spc, ldspc, conc, nsp, cls, perm, nop, dmat, start, maxlevel, maxrank,
+                    flippable, stype, block, nsb, ntb, block0, nullptr, 0, nullptr, nullptr, handle);
+}
+extern "C" int orc_build_targets(int n, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* spc,
+                                 int ldspc, const double* conc, int nsp, const int* cls, const int* perm, int nop,
+                                 const double* dmat, int start, int maxlevel, int maxrank, const int* flippable,
+                                 const int* stype, const double* block, int nsb, int ntb, const double* block0,
+                                 const int* tsite, int ntarget, int* tnode, int* tgop, void** handle) {
+  return build_impl(n, nbr_ptr, nbr, ncls, nsc, spc, ldspc, conc, nsp, cls, perm, nop, dmat, start, maxlevel, maxrank,
+                    flippable, stype, block, nsb, ntb, block0, tsite, ntarget, tnode, tgop, handle);
 }
 
 extern "C" void orc_free(void* h) { delete (Op*)h; }
@@ -988,6 +1019,79 @@ extern "C" void orc_edc_green(void* h, int ns, const double* dc, const double* d
   cd gg;
   edc_green(*(Op*)h, ed, cd(zr, zi), iv, nlev, depth_tol, tail, project != 0, gg, (cd*)a, (cd*)b, mused, nfall);
   g[0] = gg.real(); g[1] = gg.imag();
+}
+
+// edc_green_proj src/asr_edc.f90:174-232: the chain of edc_green run all nlev steps (no depth test) with the projections
+// of every Lanczos vector on the target states, cpr(k, l, t) = sum_ks tw(l, ks, t) psi_k(node ks of t, l), where psi is
+// the unreduced amplitude augcls_amp_c (:251-261): csg(l, g) v(9 (r - 1) + pi(l, g)) / sq(r).  gp(l, t) =
+// sum_k cpr(k, l, t) pv_k with pv from cf_species; gp4 the same with the chain cut four steps earlier.
+// tnode, tgop (nsm, nt) 1-based (tnode 0: no node); tw (9, nsm, nt); gp, gp4 (9, nt) complex.
+extern "C" void orc_edc_green_proj(void* h, int ns, const double* dc, const double* del, const double* enu, double zr,
+                                   double zi, int iv, int nlev, int tail, int project, int nt, const int* tnode,
+                                   const int* tgop, const double* tw, double* g, double* gp_out, double* gp4_out, int* mused) {
+  Op& op = *(Op*)h;
+  const int nsm = op.nsmax;
+  const cd z(zr, zi);
+  size_t nd = 9 * (size_t)op.nn;
+  std::vector<cd> ep(9 * (size_t)ns);
+  for (int s = 0; s < ns; ++s)
+    for (int l = 0; l < 9; ++l) ep[l + 9 * s] = z - dc[l] * (z - enu[l + 9 * s]) / del[l + 9 * s];
+  std::vector<cd> u(nd, 0.0), up(nd, 0.0), w(nd), dg(nd);
+  std::vector<double> re(nd), im(nd), sre(nd), sim(nd);
+  u[iv - 1] = 1.0;
+  std::vector<cd> a(nlev, 0.0), b(nlev, 0.0), cc(nlev, 0.0), pv(nlev, 0.0);
+  std::vector<cd> cpr((size_t)nlev * 9 * nt, 0.0);   // (k, l, t): k fastest
+  int m = 0;
+  Work wk;
+  for (int k = 1; k <= nlev; ++k) {
+    for (int t = 0; t < nt; ++t)
+      for (int ks = 0; ks < nsm; ++ks) {
+        int r = tnode[ks + (size_t)nsm * t];
+        if (r <= 0) continue;
+        int gg = tgop[ks + (size_t)nsm * t] - 1;
+        for (int l = 0; l < 9; ++l) {
+          cd amp = op.csg[l + 9 * gg] * u[9 * (size_t)(r - 1) + op.pi[l + 9 * gg] - 1] / op.sq[r - 1];
+          cpr[(k - 1) + (size_t)nlev * (l + 9 * (size_t)t)] += tw[l + 9 * (ks + (size_t)nsm * t)] * amp;
+        }
+      }
+    for (size_t q = 0; q < nd; ++q) { re[q] = u[q].real(); im[q] = u[q].imag(); }
+    augcls_apply(op, wk, re.data(), sre.data());
+    augcls_apply(op, wk, im.data(), sim.data());
+    augcls_rand_c(op, ep.data(), u.data(), dg.data());
+    for (size_t q = 0; q < nd; ++q) w[q] = cd(sre[q], sim[q]) + dg[q];
+    cd s = 0.0;
+    for (size_t q = 0; q < nd; ++q) s += u[q] * w[q];
+    a[k - 1] = s;
+    m = k;
+    if (k == nlev) break;
+    cd ak = a[k - 1], bk = 0.0;
+    if (k > 1) bk = b[k - 2];
+    for (size_t q = 0; q < nd; ++q) {
+      w[q] = w[q] - ak * u[q];
+      if (k > 1) w[q] = w[q] - bk * up[q];
+    }
+    if (project) augcls_project_c(op, w.data());
+    s = 0.0;
+    for (size_t q = 0; q < nd; ++q) s += w[q] * w[q];
+    b[k - 1] = std::sqrt(s);
+    if (std::abs(b[k - 1]) < 1.0e-12) break;
+    bk = b[k - 1];
+    for (size_t q = 0; q < nd; ++q) { up[q] = u[q]; u[q] = w[q] / bk; }
+  }
+  cd gg, ff;
+  for (int pass = 0; pass < 2; ++pass) {
+    int mm = pass == 0 ? m : std::max(1, m - 4);
+    cf_species(a.data(), b.data(), cc.data(), mm, z, tail, gg, ff, nullptr, pv.data(), nullptr);
+    if (pass == 0) { g[0] = gg.real(); g[1] = gg.imag(); }
+    cd* out = (cd*)(pass == 0 ? gp_out : gp4_out);
+    for (int t = 0; t < nt; ++t)
+      for (int l = 0; l < 9; ++l) {
+        cd acc = 0.0;
+        for (int k = 0; k < mm; ++k) acc += cpr[k + (size_t)nlev * (l + 9 * (size_t)t)] * pv[k];
+        out[l + 9 * (size_t)t] = acc;
+      }
+  }
+  *mused = m;
 }
 
 // ---- block form: src/asr_augblk.f90 (rand_r :88-124, rand_lin_amp :127-165, smul :170-203, hmul :206-215,

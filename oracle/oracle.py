@@ -33,8 +33,12 @@ def lib():
         L = C.CDLL(path)
         L.orc_last_error.restype = C.c_char_p
         L.orc_build.restype = C.c_int
+        L.orc_build_targets.restype = C.c_int
         L.orc_build.argtypes = [C.c_int, _i, _i, C.c_int, _i, _i, C.c_int, _d, C.c_int, _i, _i, C.c_int, _d, C.c_int, C.c_int,
                                 C.c_int, _i, _i, _d, C.c_int, C.c_int, _d, C.POINTER(C.c_void_p)]
+        L.orc_build_targets.argtypes = L.orc_build.argtypes[:-1] + [_i, C.c_int, _i, _i, C.POINTER(C.c_void_p)]
+        L.orc_edc_green_proj.argtypes = [C.c_void_p, C.c_int, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, C.c_int, _i, _i, _d, _d, _d, _d, _i]
         L.orc_free.argtypes = [C.c_void_p]
         L.orc_dims.argtypes = [C.c_void_p, _i]
         L.orc_tables.argtypes = [C.c_void_p] + [_i] * 8 + [_d, _d, _i, _i, _i, _d, _d]
@@ -110,7 +114,9 @@ TAILS = {"none": 0, "hull": 1, "bp": 2, "avg2": 3}
 class OracleOp:
     """Restatement of ``augcls_op`` (src/asr_augcls.f90:45-68) built by ``build_augcls_operator`` (:596-823)."""
 
-    def __init__(self, graph, model, cls, perm, dmat, start=1, maxlevel=4, maxrank=0, flippable=None, stype=None):
+    def __init__(self, graph, model, cls, perm, dmat, start=1, maxlevel=4, maxrank=0, flippable=None, stype=None, tsite=None):
+        """tsite (1-based target sites, optional): the target links of build_augcls_operator (src/asr_augcls.f90:808-820)
+        become self.tnode, self.tgop (nsmax, nt), 1-based (tnode 0: no node)."""
         L = lib()
         self._keep = []
         nbr_ptr, nbr = _i32(graph.nbr_ptr), _i32(graph.nbr)
@@ -120,9 +126,18 @@ class OracleOp:
         st = _i32(stype) if stype is not None else None
         block, block0 = _f64(model.block), _f64(model.block0)
         h = C.c_void_p()
-        rc = L.orc_build(graph.n, _pi(nbr_ptr), _pi(nbr), model.ncls, _pi(nsc), _pi(spc), spc.shape[0], _pd(conc), model.nsp,
-                         _pi(cls), _pi(perm), perm.shape[1], _pd(dmat), start, maxlevel, maxrank, _pi(fl), _pi(st), _pd(block),
-                         block.shape[2], block.shape[3], _pd(block0), C.byref(h))
+        args = (graph.n, _pi(nbr_ptr), _pi(nbr), model.ncls, _pi(nsc), _pi(spc), spc.shape[0], _pd(conc), model.nsp, _pi(cls),
+                _pi(perm), perm.shape[1], _pd(dmat), start, maxlevel, maxrank, _pi(fl), _pi(st), _pd(block), block.shape[2],
+                block.shape[3], _pd(block0))
+        self.tnode = self.tgop = None
+        if tsite is None:
+            rc = L.orc_build(*args, C.byref(h))
+        else:
+            ts = _i32(np.atleast_1d(tsite))
+            nsm = int(np.max(nsc))
+            self.tnode = np.zeros((nsm, ts.shape[0]), np.int32, order="F")
+            self.tgop = np.zeros((nsm, ts.shape[0]), np.int32, order="F")
+            rc = L.orc_build_targets(*args, _pi(ts), ts.shape[0], _pi(self.tnode), _pi(self.tgop), C.byref(h))
         _check(rc)
         self.h = h
         dims = np.zeros(7, dtype=np.int32)
@@ -221,6 +236,19 @@ class OracleOp:
         lib().orc_edc_green(self.h, dl.shape[1], _pd(dc), _pd(dl), _pd(en), z.real, z.imag, iv, nlev, depth_tol, TAILS[tail],
                             int(project), _pd(g), _pd(a), _pd(b), C.byref(m), C.byref(nf))
         return complex(g[0], g[1]), a[: m.value], b[: m.value], m.value, nf.value
+
+    def edc_green_proj(self, ed, z, iv, nlev, tnode, tgop, tw, tail="hull", project=True):
+        """``edc_green_proj`` (src/asr_edc.f90:174-232): returns (g, gp (9, nt), gp4 (9, nt), mused)."""
+        dc, dl, en = _f64(ed["dc"]), _f64(ed["dl"]), _f64(ed["enu"])
+        tnode, tgop, tw = _i32(tnode), _i32(tgop), _f64(tw)
+        nt = tnode.shape[1]
+        g = np.zeros(2)
+        gp = np.zeros((9, nt), np.complex128, order="F")
+        gp4 = np.zeros((9, nt), np.complex128, order="F")
+        m = C.c_int()
+        lib().orc_edc_green_proj(self.h, dl.shape[1], _pd(dc), _pd(dl), _pd(en), z.real, z.imag, iv, nlev, TAILS[tail],
+                                 int(project), nt, _pi(tnode), _pi(tgop), _pd(tw), _pd(g), _pd(gp), _pd(gp4), C.byref(m))
+        return complex(g[0], g[1]), gp, gp4, m.value
 
     def edc_green_blk(self, ed, zs, iv, nlev, depth_tol=0.0, tail="hull", project=True):
         """``edc_green_blk`` (src/asr_edc.f90:237-316): returns (g(nb), mused(nb), a(nlev, nb), b(nlev, nb))."""

@@ -1,0 +1,130 @@
+"""Bloch spectral function helpers and the projected chains (edc_green_proj) of the oracle, after the reference's
+test/test_spectral.f90: (A) the k path, the unfolded Bloch sum (exact for a lattice Green function), the Fourier window,
+the dressing weights; (B) readout on a random bcc binary: the projections are the same with the operator reduced by
+D4h, D2h and the identity (the same Krylov process in three bases), the projection on the origin is g_11, and the cubic
+rotation (x, y, z) -> (y, z, x) maps G_{px,px}(d) onto G_{pz,pz}(P d)."""
+import numpy as np
+import pytest
+
+from asr_b200 import spectral as SP
+from oracle.oracle import OracleOp
+from tests.spectral_case import readout_inputs
+
+Z = 0.35 + 0.08j
+
+
+def test_kpath():
+    kv, dist, ic = SP.spectral_kpath(np.array([[0, 1, 1], [0, 0, 0.5], [0, 0, 0]], float), 4)
+    assert kv.shape[1] == 9 and list(ic) == [0, 4, 8]
+    assert abs(dist[-1] - 1.5) < 1e-12 and np.max(np.abs(kv[:, -1] - [1, 0.5, 0])) < 1e-14
+
+
+def test_unfolded_bloch_sum_is_exact_for_a_lattice_green_function():
+    nper, z = 6, 0.13 + 0.07j
+    ks = np.array([[jx, jy, jz] for jx in range(nper) for jy in range(nper) for jz in range(nper)], float).T / nper
+    ek = -0.5 * np.sum(np.cos(2 * np.pi * ks), axis=0)
+    r = np.array([[ix, iy, iz] for ix in range(nper) for iy in range(nper) for iz in range(nper)], float).T
+    disp = r - nper * np.rint(r / nper)
+    gR = np.exp(2j * np.pi * (ks.T @ disp)).T @ (1.0 / (z - ek)) / nper ** 3
+    v = -np.imag(gR) / np.pi
+    err = max(abs(SP.spectral_unfold(disp, v, ks[:, q]) + np.imag(1.0 / (z - ek[q])) / np.pi) for q in range(ks.shape[1]))
+    assert err < 1e-12
+
+
+def test_window():
+    assert SP.spectral_window("ball", 0.0, 2.0) == 1.0 and SP.spectral_window("ball", 2.0, 2.0) == 0.0
+    assert SP.spectral_window("ball", 2.5, 2.0) == 0.0 and abs(SP.spectral_window("ball", 1.0, 2.0) - 0.3125) < 1e-15
+    assert SP.spectral_window("sharp", 2.0, 2.0) == 1.0 and SP.spectral_window("sharp", 2.01, 2.0) == 0.0
+    rng = np.random.default_rng(3)
+    for lat in ("fcc", "bcc"):
+        wmin = {"ball": np.inf, "sharp": np.inf}
+        i = np.arange(-8, 9)
+        h = 0.5 * np.array(np.meshgrid(i, i, i, indexing="ij")).reshape(3, -1)
+        hi = np.rint(2 * h).astype(int)
+        on = (np.sum(hi, axis=0) % 2 == 0) if lat == "fcc" else ((hi[0] - hi[1]) % 2 == 0) & ((hi[1] - hi[2]) % 2 == 0)
+        h = h[:, on]
+        for rm in (1.0, 1.5, 2.0, 3.0):
+            keep = np.linalg.norm(h, axis=0) <= rm + 1e-9
+            rr = h[:, keep]
+            for kind in wmin:
+                ww = np.array([SP.spectral_window(kind, np.linalg.norm(rr[:, q]), rm) for q in range(rr.shape[1])])
+                for _ in range(400):
+                    k = 2 * rng.random(3) - 1
+                    wmin[kind] = min(wmin[kind], SP.spectral_unfold(rr, ww, k) / ww.sum())
+        assert wmin["ball"] > -1e-12 and wmin["sharp"] < -0.01
+
+
+def test_dressing():
+    dc = np.full(9, 0.04)
+    dl = np.zeros((9, 2))
+    dl[:, 0], dl[:, 1] = 0.04, 0.09
+    tau = SP.spectral_dressing(dc, dl, [1, 2], [0.6, 0.4], True)
+    assert np.all(tau[:, 0] == 1.0) and np.all(tau[:, 1] == 0.0)
+    tau = SP.spectral_dressing(dc, dl, [2], [1.0], False)
+    assert np.max(np.abs(tau[:, 0] - np.sqrt(0.04 / 0.09))) < 1e-14
+    dl[:, 1] = 0.04
+    tau = SP.spectral_dressing(dc, dl, [1, 2], [0.6, 0.4], False)
+    assert np.max(np.abs(tau[:, 0] - 1.0)) + np.max(np.abs(tau[:, 1])) < 1e-14
+
+
+@pytest.fixture(scope="module")
+def readout():
+    r = readout_inputs()
+    ops = {}
+    for key, (perm, dmat) in r["groups"].items():
+        op = OracleOp(r["graph"], r["model"], r["cls"], perm, dmat, 1, 2, 1, r["flippable"], tsite=r["tsite"])
+        ed = r["ed"]
+        op.set_params(ed["c"], ed["d"], ed["o"], ed["e"])
+        op.freeze_site(1, 1)
+        ops[key] = op
+    return r, ops
+
+
+def test_target_links(readout):
+    r, ops = readout
+    assert len(r["tsite"]) == 15 and ops["d4h"].nop == 16 and ops["d2h"].nop == 8
+    t0 = r["t0"]
+    other = np.arange(15) != t0
+    tn1 = ops["identity"].tnode
+    assert np.all(tn1[:, other] > 0) and tn1[0, t0] > 0 and tn1[1, t0] == 0
+    for key in ("d2h", "d4h"):
+        assert np.all(ops[key].tnode[:, other] > 0) and ops[key].tnode[1, t0] == 0
+
+
+@pytest.mark.parametrize("nlev,tol_abs,tol_origin", [(8, 1e-11, 1e-13), (24, None, 1e-9)])
+def test_projections_in_three_bases(readout, nlev, tol_abs, tol_origin):
+    r, ops = readout
+    ed, tw, t0 = r["ed"], r["tw"], r["t0"]
+    d4 = r["groups"]["d4h"][1]
+    gp = {}
+    e21 = e41 = e0 = 0.0
+    for l0 in range(1, 10):
+        out = {}
+        for key in ("identity", "d2h", "d4h"):
+            if key == "d4h" and not np.all(np.abs(np.abs(d4[l0 - 1, l0 - 1, :]) - 1.0) < 1e-9):
+                continue
+            op = ops[key]
+            op.set_start(l0)
+            g, p, p4, m = op.edc_green_proj(ed, Z, l0, nlev, op.tnode, op.tgop, tw, tail="none")
+            assert m == nlev
+            out[key] = (g, p)
+        gp[l0] = out["d2h"][1]
+        e21 = max(e21, np.max(np.abs(out["d2h"][1] - out["identity"][1])), abs(out["d2h"][0] - out["identity"][0]))
+        e0 = max(e0, abs(out["d2h"][1][l0 - 1, t0] - out["d2h"][0]))
+        if "d4h" in out:
+            e41 = max(e41, np.max(np.abs(out["d4h"][1] - out["identity"][1])))
+    gmax = max(np.max(np.abs(np.delete(gp[l0], t0, axis=1))) for l0 in gp)
+    assert gmax > 1e-3
+    if tol_abs is not None:
+        assert e21 < tol_abs and e41 < tol_abs
+    else:
+        assert e21 / gmax < 1e-8 and e41 / gmax < 1e-8
+    assert e0 < tol_origin
+    if nlev == 8:   # cubic rotation P: (d1, d2, d3) -> (d2, d3, d1) maps p_x onto p_z
+        td = r["tdisp"]
+        erot = 0.0
+        for t in range(td.shape[1]):
+            pd = np.array([td[1, t], td[2, t], td[0, t]])
+            tr = int(np.nonzero(np.all(np.abs(td - pd[:, None]) < 1e-9, axis=0))[0][0])
+            erot = max(erot, abs(gp[4][3, t] - gp[3][2, tr]))
+        assert erot < 1e-11
