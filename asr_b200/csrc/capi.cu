@@ -686,6 +686,62 @@ static int chains_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups
   return ASR_OK;
 }
 
+// epi_blocks (src/asr_epi.f90:639-663) for every (group, energy): v9 (9, ngroup) symmetry-adapted start vectors on the
+// start node, chi (nop, ngroup) their characters (+-1); the chains of the edc route from s0 (projection on h'|s0>) and from
+// h'|s0> / |h'|s0>| (projection on s0), full depth.  x (4, nz, ngroup) complex = X0, X1 (mean of the two chains), X2, and
+// the X1 mismatch; mused (2, nz, ngroup) optional.
+int asr_epi_blocks(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, const double* v9, const double* chi, int ngroup,
+                   const double* z, int nz, int tail, int precision, int project, double* x, int* mused) {
+  if (!ctx || !op || !groups || !v9 || !chi || ngroup < 1 || nz < 1 || !z || !x) { set_error("asr_epi_blocks: bad argument"); return ASR_EINVAL; }
+  if (tail < 0 || tail > 3) { set_error("asr_epi_blocks: unknown tail"); return ASR_EINVAL; }
+  ASR_TRY(set_device(ctx));
+  GroupLayout GL = layout(op);
+  std::vector<double> blob((size_t)GL.stride * ngroup, 0.0), vv(9 * (size_t)ngroup);
+  std::vector<GroupInfo> gi(ngroup);
+  for (int q = 0; q < ngroup; ++q) {
+    const asr_chain_group& G = groups[q];
+    if (!G.c || !G.d || !G.pa || !G.pb) { set_error("asr_epi_blocks: group %d without c, d, pa or pb", q + 1); return ASR_EINVAL; }
+    if (G.nlev < 1 || G.nlev > NLMAX) { set_error("asr_epi_blocks: depth %d out of range 1..%d", G.nlev, NLMAX); return ASR_EINVAL; }
+    const double* cq = chi + (size_t)op->nop * q;
+    for (int g = 0; g < op->nop; ++g)
+      if (std::fabs(std::fabs(cq[g]) - 1.0) > 1.0e-12) { set_error("asr_epi_blocks: characters must be +-1"); return ASR_EINVAL; }
+    double n2 = 0.0;
+    for (int l = 0; l < 9; ++l) { vv[9 * (size_t)q + l] = v9[9 * (size_t)q + l]; n2 += v9[9 * (size_t)q + l] * v9[9 * (size_t)q + l]; }
+    if (std::fabs(n2 - 1.0) > 1.0e-10) { set_error("asr_epi_blocks: start vector %d is not normalised", q + 1); return ASR_EINVAL; }
+    ASR_TRY(make_group(op, GL, G.c, G.d, G.o, G.e, G.pa, G.pb, G.frozen_sp, G.start_orb, G.nlev, cq,
+                       blob.data() + (size_t)GL.stride * q, gi[q]));
+  }
+  const int nlane = 2 * ngroup * nz;
+  std::vector<int> lg(nlane), lk(nlane);
+  std::vector<double2> lz(nlane);
+  for (int q = 0; q < ngroup; ++q)
+    for (int j = 0; j < nz; ++j)
+      for (int kd = 0; kd < 2; ++kd) {
+        size_t L = 2 * ((size_t)q * nz + j) + kd;
+        lg[L] = q; lk[L] = kd; lz[L] = make_double2(z[2 * j], z[2 * j + 1]);
+      }
+  std::vector<double2> g, f;
+  std::vector<double> nv;
+  std::vector<int> m;
+  int64_t nfall = 0;
+  ASR_TRY(run_epi(ctx, op, gi, blob, GL, vv, lg, lk, lz, tail, project, precision, g, f, nv, m, &nfall));
+  for (int q = 0; q < ngroup; ++q)
+    for (int j = 0; j < nz; ++j) {
+      size_t LU = 2 * ((size_t)q * nz + j), LV = LU + 1;
+      double2 fa = f[LU], fb = cscale(f[LV], nv[LV]);
+      double2 out[4] = {g[LU], cscale(cadd(fa, fb), 0.5), cscale(g[LV], nv[LV] * nv[LV]), csub(fa, fb)};
+      for (int k = 0; k < 4; ++k) {
+        size_t dst = 2 * (4 * ((size_t)j + (size_t)nz * q) + k);
+        x[dst] = out[k].x;
+        x[dst + 1] = out[k].y;
+      }
+      if (mused) { mused[2 * ((size_t)j + (size_t)nz * q)] = m[LU]; mused[2 * ((size_t)j + (size_t)nz * q) + 1] = m[LV]; }
+    }
+  ctx->nchain += nlane;
+  ctx->nfall += nfall;
+  return ASR_OK;
+}
+
 int asr_ed3_blocks(asr_ctx* ctx, asr_op* op, const asr_ed3_group* groups, int ngroup, const double* z, int nz, double depth_tol,
                    int tail, int precision, int project, double* bk, int* mused, double* a, double* b, double* c) {
   if (!ctx || !op || !groups || ngroup < 1 || nz < 1 || !z || !bk) { set_error("asr_ed3_blocks: bad argument"); return ASR_EINVAL; }

@@ -2033,6 +2033,218 @@ int run_ed3_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
   return ASR_OK;
 }
 
+// ================================================================================================ EPI block chains
+// epi_blocks (src/asr_epi.f90:639-663): per symmetry-adapted start vector s0 (9 values on the start node, characters of
+// the group in the lane group's chimask) two complex-symmetric chains on z - H(z) of the edc route, full depth: kind 0
+// from s0 with the projection on |v> = h'|s0> (projected), kind 1 from |v> / |v| with the projection on s0; a chain that
+// closes (|b| < 1e-12) gets no tail.  Per lane g and f = sum_k c_k pv_k, c_k = tv . u_k.
+
+// U = s0 (node 0, 9 values of the lane's group), UP = 0
+template <typename ST>
+__global__ void k_epi_init(BatchView bv, const double* v9, typename St2<ST>::T* u, typename St2<ST>::T* up) {
+  size_t n = (size_t)bv.ntile * bv.nn * 9 * TL;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    int lane = (int)(q % TL);
+    size_t rest = q / TL;
+    int l = (int)(rest % 9);
+    size_t nt = rest / 9;
+    int node = (int)(nt % bv.nn);
+    int tile = (int)(nt / bv.nn);
+    int grp = bv.lane_group[tile * TL + lane];
+    double v = (grp >= 0 && node == 0) ? v9[9 * grp + l] : 0.0;
+    stv(u + q, make_double2(v, 0.0));
+    stv(up + q, make_double2(0.0, 0.0));
+  }
+}
+
+// kind 0: U = s0, TV = v; kind 1: U = v / nv, TV = s0 (s0 read from S0, v from VV), UP = 0
+template <typename ST>
+__global__ void k_epi_start(BatchView bv, const typename St2<ST>::T* __restrict__ S0, const typename St2<ST>::T* __restrict__ VV,
+                            const int* kind, const double* nv, typename St2<ST>::T* U, typename St2<ST>::T* UP,
+                            typename St2<ST>::T* TV) {
+  size_t n = (size_t)bv.ntile * bv.nn * 9 * TL;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+    int lane = (int)(q % TL);
+    int tile = (int)(q / ((size_t)bv.nn * 9 * TL));
+    int L = tile * TL + lane;
+    double2 u = make_double2(0, 0), t = make_double2(0, 0);
+    if (bv.lane_group[L] >= 0) {
+      double2 s0 = ld(S0 + q), v = ld(VV + q);
+      if (kind[L] == 0) { u = s0; t = v; }
+      else { u = cscale(v, 1.0 / nv[L]); t = s0; }
+    }
+    stv(U + q, u);
+    stv(UP + q, make_double2(0, 0));
+    stv(TV + q, t);
+  }
+}
+
+// c_k = su * sum of the partial dots tv . X_k of this step
+__global__ void k_epi_store_c(BatchView bv, const double2* part, int bpt, int k, double2* ccoef) {
+  int tile = blockIdx.x, lane = threadIdx.x;
+  if (tile >= bv.ntile || !bv.tile_act[tile]) return;
+  int L = tile * TL + lane;
+  if (bv.lane_group[L] < 0 || !bv.lane_act[L]) return;
+  double2 c = make_double2(0, 0);
+  for (int q = 0; q < bpt; ++q) c = cadd(c, part[((size_t)tile * bpt + q) * TL + lane]);
+  ccoef[(size_t)L * NLMAX + k - 1] = cmul(c, bv.su[L]);
+}
+
+template <typename ST>
+int run_epi_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+              const GroupLayout& GL, const std::vector<double>& v9, const std::vector<int>& lane_group,
+              const std::vector<int>& lane_kind, const std::vector<double2>& lane_z, int tail, int project,
+              std::vector<double2>& g_out, std::vector<double2>& f_out, std::vector<double>& nv_out, std::vector<int>& m_out,
+              int64_t* nfall_out) {
+  typedef typename St2<ST>::T T2;
+  cudaStream_t s = ctx->stream;
+  const int nn = op->nn, nlane = (int)lane_group.size();
+  bool dunif = true, any_o = false;
+  for (auto& g : ginfo) {
+    if (!(g.flags & GF_D_UNIFORM)) dunif = false;
+    if (!(g.flags & GF_O_ZERO)) any_o = true;
+    if (g.nlev > NLMAX) { set_error("epi_blocks: depth %d above %d", g.nlev, NLMAX); return ASR_EINVAL; }
+  }
+  const bool fused = dunif && !any_o;
+  std::vector<std::vector<int>> tiles;
+  {
+    std::vector<std::vector<int>> per_group(ginfo.size());
+    for (int L = 0; L < nlane; ++L) per_group[lane_group[L]].push_back(L);
+    for (auto& lst : per_group)
+      for (size_t q = 0; q < lst.size(); q += TL)
+        tiles.emplace_back(lst.begin() + q, lst.begin() + std::min(lst.size(), q + (size_t)TL));
+  }
+  const int ntile_all = (int)tiles.size();
+  const size_t vec_bytes = (size_t)nn * 9 * TL * sizeof(T2);
+  const int nvec = 3 + 1 + 4 + 2;   // U, UP, Y (rotating), TV, four step temporaries, S d x and d x of h'
+  size_t freeb = 0, totb = 0;
+  cudaMemGetInfo(&freeb, &totb);
+  int tpb = std::is_same<ST, double>::value ? 16 : 8;
+  while (tpb > 1 && (size_t)tpb * nvec * vec_bytes > freeb / 2) tpb /= 2;
+  if ((size_t)nvec * vec_bytes > freeb) { set_error("epi_blocks: %d vectors of %zu bytes do not fit", nvec, vec_bytes); return ASR_ENOMEM; }
+  tpb = std::min(tpb, ntile_all);
+  const int npw = 4, npb = WPB * npw, bpt = (nn + npb - 1) / npb;
+  const int nlp = tpb * TL;
+  Dev<double> d_gblob, d_v9, d_nv;
+  Dev<GroupInfo> d_ginfo;
+  ASR_TRY(d_gblob.alloc(gblob.size())); ASR_TRY(d_ginfo.alloc(ginfo.size())); ASR_TRY(d_v9.alloc(v9.size()));
+  ASR_CUDA(cudaMemcpyAsync(d_gblob.p, gblob.data(), gblob.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_ginfo.p, ginfo.data(), ginfo.size() * sizeof(GroupInfo), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_v9.p, v9.data(), v9.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  ASR_TRY(d_nv.alloc(nlp));
+  Dev<int> d_lgroup, d_act, d_wact, d_m, d_tact, d_nfall, d_tgroup, d_kind, d_closed, d_lmap;
+  Dev<double2> d_a, d_b, d_c, d_gprev, d_acur, d_bprev, d_su, d_sup, d_part, d_part2, d_z, d_g, d_f, d_sv;
+  ASR_TRY(d_lgroup.alloc(nlp)); ASR_TRY(d_act.alloc(nlp)); ASR_TRY(d_wact.alloc(nlp)); ASR_TRY(d_m.alloc(nlp));
+  ASR_TRY(d_tact.alloc(tpb)); ASR_TRY(d_nfall.alloc(1)); ASR_TRY(d_tgroup.alloc(tpb)); ASR_TRY(d_kind.alloc(nlp));
+  ASR_TRY(d_closed.alloc(nlp)); ASR_TRY(d_lmap.alloc(nlp));
+  ASR_TRY(d_a.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_b.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_c.alloc((size_t)nlp * NLMAX));
+  ASR_TRY(d_gprev.alloc(nlp)); ASR_TRY(d_acur.alloc(nlp)); ASR_TRY(d_bprev.alloc(nlp)); ASR_TRY(d_su.alloc(nlp));
+  ASR_TRY(d_sup.alloc(nlp)); ASR_TRY(d_z.alloc(nlp)); ASR_TRY(d_g.alloc(nlane)); ASR_TRY(d_f.alloc(nlane));
+  ASR_TRY(d_part.alloc((size_t)tpb * bpt * TL)); ASR_TRY(d_part2.alloc((size_t)tpb * bpt * TL)); ASR_TRY(d_sv.alloc(nlp));
+  const size_t vlen = (size_t)tpb * nn * 9 * TL;
+  std::vector<Dev<T2>> V(nvec);
+  for (int q = 0; q < nvec; ++q) ASR_TRY(V[q].alloc(vlen));
+  T2 *TV = V[3].p, *W1 = V[4].p, *W2 = V[5].p, *W3 = V[6].p, *W4 = V[7].p, *SA = V[8].p, *TMP = V[9].p;
+  OpView ov = op->view();
+  g_out.assign(nlane, make_double2(0, 0));
+  f_out.assign(nlane, make_double2(0, 0));
+  nv_out.assign(nlane, 0.0);
+  m_out.assign(nlane, 0);
+  std::vector<int> hgroup(nlp), lmap(nlp), hkind(nlp), hm(nlp);
+  std::vector<double2> hz(nlp), ones(nlp, make_double2(1.0, 0.0));
+  std::vector<double> hnv(nlp);
+  ASR_CUDA(cudaMemsetAsync(d_nfall.p, 0, sizeof(int), s));
+  for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
+    const int nt = std::min(tpb, ntile_all - t0);
+    std::vector<int> tact(tpb, 0), act(nlp, 0), tgroup(tpb, -1);
+    for (int q = 0; q < nlp; ++q) {
+      int bt = q / TL, L = -1;
+      if (bt < nt && q % TL < (int)tiles[t0 + bt].size()) L = tiles[t0 + bt][q % TL];
+      lmap[q] = L;
+      hgroup[q] = L >= 0 ? lane_group[L] : -1;
+      hkind[q] = L >= 0 ? lane_kind[L] : 0;
+      hz[q] = L >= 0 ? lane_z[L] : make_double2(0, 0);
+      if (L >= 0) { tact[bt] = 1; act[q] = 1; tgroup[bt] = hgroup[q]; }
+    }
+    ASR_CUDA(cudaMemcpyAsync(d_lgroup.p, hgroup.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_tgroup.p, tgroup.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_kind.p, hkind.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_lmap.p, lmap.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_act.p, act.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_tact.p, tact.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_z.p, hz.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_su.p, ones.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemsetAsync(d_wact.p, 0, nlp * sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_m.p, 0, nlp * sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_closed.p, 0, nlp * sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_a.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_b.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_c.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_gprev.p, 0, nlp * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_bprev.p, 0, nlp * sizeof(double2), s));
+    ASR_CUDA(cudaMemsetAsync(d_sup.p, 0, nlp * sizeof(double2), s));
+    BatchView bv{nt, nn, op->nsmax, 0, ASR_MODE_EDC, project, tail, NLMAX, 0.0, d_gblob.p, GL, d_ginfo.p, d_lgroup.p,
+                 d_tgroup.p, d_z.p, d_act.p, d_wact.p, d_m.p, d_a.p, d_b.p, d_gprev.p, d_acur.p, d_bprev.p, d_su.p, d_sup.p,
+                 d_tact.p, d_nfall.p, d_closed.p};
+    const int grid = nt * bpt;
+    const unsigned egrid = (unsigned)std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256);
+    int kmax = 0;
+    for (int q = 0; q < nlp; ++q) if (hgroup[q] >= 0) kmax = std::max(kmax, ginfo[hgroup[q]].nlev);
+    // ---- start vectors (epi_start, src/asr_epi.f90:578-587): s0 on the start node, |v> = h'|s0> projected, |v|
+    k_epi_init<ST><<<egrid, 256, 0, s>>>(bv, d_v9.p, W1, V[0].p);
+    apply_SD<ST>(op, bv, dunif, W1, TMP, SA, d_part.p, npw, grid, s);
+    k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, SA, W1, E3_G, false, W1, false, nullptr, 1.0, false, W2, d_part.p, npw);
+    if (project) k_project<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, W2, npw);
+    k_dot<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, W2, W2, d_part.p, npw);
+    k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_sv.p);
+    std::vector<double2> hsv(nlp);
+    ASR_CUDA(cudaMemcpyAsync(hsv.data(), d_sv.p, nlp * sizeof(double2), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaStreamSynchronize(s));
+    for (int q = 0; q < nlp; ++q) {
+      hnv[q] = 1.0;
+      if (hgroup[q] < 0) continue;
+      double nv = std::sqrt(hsv[q].x);   // sqrt(real(v . v)), as the reference
+      if (!(nv >= 1.0e-14)) { set_error("epi_start: zero start vector (group %d)", hgroup[q] + 1); return ASR_EINVAL; }
+      hnv[q] = nv;
+    }
+    ASR_CUDA(cudaMemcpyAsync(d_nv.p, hnv.data(), nlp * sizeof(double), cudaMemcpyHostToDevice, s));
+    k_epi_start<ST><<<egrid, 256, 0, s>>>(bv, W1, W2, d_kind.p, d_nv.p, V[1].p, V[0].p, TV);
+    // ---- the chains (chain, src/asr_epi.f90:588-636): full depth, projections c_k = tv . u_k
+    for (int k = 1; k <= kmax; ++k) {
+      bv.kstep = k;
+      T2* U = V[k % 3].p;
+      T2* UP = V[(k + 2) % 3].p;
+      T2* Y = V[(k + 1) % 3].p;
+      k_dot<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TV, U, d_part2.p, npw);
+      k_epi_store_c<<<nt, TL, 0, s>>>(bv, d_part2.p, bpt, k, d_c.p);
+      ASR_TRY(step_apply<ST>(ctx, op, bv, fused, any_o, dunif, U, Y, W1, W2, W3, W4, d_part.p, npw, grid));
+      k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+      k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, Y, U, UP, d_part.p, npw);
+      k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
+    }
+    ASR_CUDA(cudaGetLastError());
+    ctx->launches += 8 + (int64_t)kmax * (5 + (fused ? 1 : (any_o ? 7 : (dunif ? 2 : 3))));
+    k_ed3_final<<<(nlp + 127) / 128, 128, 0, s>>>(bv, nlp, d_lmap.p, d_c.p, d_closed.p, d_g.p, d_f.p);
+    ASR_CUDA(cudaMemcpyAsync(hm.data(), d_m.p, nlp * sizeof(int), cudaMemcpyDeviceToHost, s));
+    ASR_CUDA(cudaStreamSynchronize(s));
+    for (int q = 0; q < nlp; ++q) {
+      int L = lmap[q];
+      if (L < 0) continue;
+      m_out[L] = hm[q];
+      nv_out[L] = hnv[q];
+    }
+  }
+  ASR_CUDA(cudaMemcpyAsync(g_out.data(), d_g.p, nlane * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(f_out.data(), d_f.p, nlane * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  int nf = 0;
+  ASR_CUDA(cudaMemcpyAsync(&nf, d_nfall.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  ASR_CUDA(cudaGetLastError());
+  ASR_TRY(check_wait_error(ctx));
+  if (nfall_out) *nfall_out = nf;
+  return ASR_OK;
+}
+
 }  // namespace
 
 // the operator kernels stage up to 96 KB of bond blocks in shared memory (set once per device)
@@ -2080,6 +2292,20 @@ int run_ed3(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const
                             na_out, nv_out, m_out, a_out, b_out, c_out, nfall_out);
   return run_ed3_t<double>(ctx, op, ginfo, gblob, GL, oc, lane_group, lane_kind, lane_z, depth_tol, tail, project, g_out, f_out,
                            na_out, nv_out, m_out, a_out, b_out, c_out, nfall_out);
+}
+
+int run_epi(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+            const GroupLayout& GL, const std::vector<double>& v9, const std::vector<int>& lane_group,
+            const std::vector<int>& lane_kind, const std::vector<double2>& lane_z, int tail, int project, int precision,
+            std::vector<double2>& g_out, std::vector<double2>& f_out, std::vector<double>& nv_out, std::vector<int>& m_out,
+            int64_t* nfall_out) {
+  smem_attrs();
+  if (smul_smem(op, sizeof(double)) > 96 * 1024) { set_error("epi_blocks: bond tables above 96 KB of shared memory"); return ASR_EINVAL; }
+  if (precision == ASR_FP32)
+    return run_epi_t<float>(ctx, op, ginfo, gblob, GL, v9, lane_group, lane_kind, lane_z, tail, project, g_out, f_out, nv_out,
+                            m_out, nfall_out);
+  return run_epi_t<double>(ctx, op, ginfo, gblob, GL, v9, lane_group, lane_kind, lane_z, tail, project, g_out, f_out, nv_out,
+                           m_out, nfall_out);
 }
 
 int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,

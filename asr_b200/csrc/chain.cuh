@@ -115,6 +115,14 @@ int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
               const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
               std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj = nullptr);
 
+// EPI block chains (epi_blocks, src/asr_epi.f90:639-663): v9 (9, ngroup) start vectors on the start node; lane kind 0 runs
+// from s0 with the projection on |v> = h'|s0>, kind 1 from |v> / |v| with the projection on s0; per lane g, f, |v|, depth
+int run_epi(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
+            const GroupLayout& GL, const std::vector<double>& v9, const std::vector<int>& lane_group,
+            const std::vector<int>& lane_kind, const std::vector<double2>& lane_z, int tail, int project, int precision,
+            std::vector<double2>& g_out, std::vector<double2>& f_out, std::vector<double>& nv_out, std::vector<int>& m_out,
+            int64_t* nfall_out);
+
 // route ed3: two chains per (group, energy) (lane kind 0: from |a>, 1: from |v>); per lane g, the projection f, the start
 // norms |a|, |v| and the depth
 int run_ed3(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,

@@ -145,6 +145,16 @@ int asr_chains_proj(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int
                     int precision, int project, int nt, const int* tnode, const int* tgop, const double* tw, double* g,
                     double* gp, double* gp4, int* mused);
 
+/* epi_blocks (src/asr_epi.f90:639-663), the chains of the effective pair interactions, for every (group, energy): v9(9, ngroup)
+ * the symmetry-adapted start vector of each group on the start node (epi_adapted, unit norm) and chi(nop, ngroup) its
+ * characters under the operator's group (+-1).  Two full-depth chains of the edc route per (group, energy): from s0 with
+ * the projection on |v> = h'|s0> (projected, h' = c + d S d), and from |v>/|v| with the projection on s0 (a chain that
+ * closes gets no tail).  x(4, nz, ngroup) complex = X0 = <s0|G|s0>, X1 = <s0|h'G|s0> (the mean of the two chains),
+ * X2 = <s0|h'Gh'|s0> and the X1 mismatch of the two chains; mused(2, nz, ngroup) the two depths, or NULL.  Operator-level
+ * frozen sites (asr_op_freeze_site: the path site and the partner) apply to every group. */
+int asr_epi_blocks(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, const double* v9, const double* chi, int ngroup,
+                   const double* z, int nz, int tail, int precision, int project, double* x, int* mused);
+
 /* ---- route ed3 (src/asr_ed3.f90): chains on z - K'(z), K' = et - h' + u h' + h' u - h' Qt h', h' = g + d S d ---------- */
 typedef struct asr_ed3_group {
   const double *g, *d;                    /* (9, nsp): h' of ed3_setup (:57-79): g = (D_c / D_s)(C - E_nu), d = D_c^1/2 */

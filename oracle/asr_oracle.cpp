@@ -1021,6 +1021,81 @@ extern "C" void orc_edc_green(void* h, int ns, const double* dc, const double* d
   g[0] = gg.real(); g[1] = gg.imag();
 }
 
+// epi_start + epi_blocks src/asr_epi.f90:578-663 (with chain :588-636): s0 = v9 on node 1, |v> = h'|s0> (augcls_hp_c,
+// projected), nv = sqrt(re(v . v)); chain from s0 with tv = v gives X0 and fa, chain from v / nv with tv = s0 gives
+// X2 = nv^2 g and fb = nv f; x = (X0, (fa + fb) / 2, X2, fa - fb).  The operator's characters must be those of v9
+// (orc_set_chi).  ed: dc (9), del, enu (9, ns).  mused: the two depths.
+static void epi_chain(Op& op, const std::vector<cd>& ep, const std::vector<cd>& u0, const std::vector<cd>& tv, cd z, int nlev,
+                      int tail, bool project, cd& g, cd& f, int& m) {
+  size_t nd = 9 * (size_t)op.nn;
+  std::vector<cd> u = u0, up(nd, 0.0), w(nd), dg(nd);
+  std::vector<double> re(nd), im(nd), sre(nd), sim(nd);
+  std::vector<cd> a(nlev, 0.0), b(nlev, 0.0), c(nlev, 0.0);
+  Work wk;
+  bool closed = false;
+  m = 0;
+  for (int k = 1; k <= nlev; ++k) {
+    cd ck = 0.0;
+    for (size_t q = 0; q < nd; ++q) ck += tv[q] * u[q];
+    c[k - 1] = ck;
+    for (size_t q = 0; q < nd; ++q) { re[q] = u[q].real(); im[q] = u[q].imag(); }
+    augcls_apply(op, wk, re.data(), sre.data());
+    augcls_apply(op, wk, im.data(), sim.data());
+    augcls_rand_c(op, ep.data(), u.data(), dg.data());
+    for (size_t q = 0; q < nd; ++q) w[q] = cd(sre[q], sim[q]) + dg[q];
+    cd s = 0.0;
+    for (size_t q = 0; q < nd; ++q) s += u[q] * w[q];
+    a[k - 1] = s;
+    m = k;
+    if (k == nlev) break;
+    cd ak = a[k - 1], bk = k > 1 ? b[k - 2] : cd(0.0);
+    for (size_t q = 0; q < nd; ++q) {
+      w[q] = w[q] - ak * u[q];
+      if (k > 1) w[q] = w[q] - bk * up[q];
+    }
+    if (project) augcls_project_c(op, w.data());
+    s = 0.0;
+    for (size_t q = 0; q < nd; ++q) s += w[q] * w[q];
+    b[k - 1] = std::sqrt(s);
+    if (std::abs(b[k - 1]) < 1.0e-12) { closed = true; break; }
+    bk = b[k - 1];
+    for (size_t q = 0; q < nd; ++q) { up[q] = u[q]; u[q] = w[q] / bk; }
+  }
+  cf_species(a.data(), b.data(), c.data(), m, z, closed ? 0 : tail, g, f, nullptr, nullptr, nullptr);
+}
+extern "C" int orc_epi_blocks(void* h, int ns, const double* dc, const double* del, const double* enu, const double* v9,
+                              double zr, double zi, int nlev, int tail, int project, double* x, int* mused) {
+  Op& op = *(Op*)h;
+  const cd z(zr, zi);
+  size_t nd = 9 * (size_t)op.nn;
+  std::vector<cd> ep(9 * (size_t)ns);
+  for (int s = 0; s < ns; ++s)
+    for (int l = 0; l < 9; ++l) ep[l + 9 * s] = z - dc[l] * (z - enu[l + 9 * s]) / del[l + 9 * s];
+  std::vector<cd> s0(nd, 0.0), vv(nd, 0.0);
+  for (int l = 0; l < 9; ++l) s0[l] = v9[l];
+  hp_c(op, s0.data(), vv.data());
+  if (project) augcls_project_c(op, vv.data());
+  cd vn = 0.0;
+  for (size_t q = 0; q < nd; ++q) vn += vv[q] * vv[q];
+  double nv = std::sqrt(vn.real());
+  if (nv < 1.0e-14) return fail("epi_start: zero start vector");
+  cd g, fa, fb;
+  int m0, m1;
+  epi_chain(op, ep, s0, vv, z, nlev, tail, project != 0, g, fa, m0);
+  cd* out = (cd*)x;
+  out[0] = g;
+  std::vector<cd> u1(nd);
+  for (size_t q = 0; q < nd; ++q) u1[q] = vv[q] / nv;
+  epi_chain(op, ep, u1, s0, z, nlev, tail, project != 0, g, fb, m1);
+  out[2] = nv * nv * g;
+  fb = nv * fb;
+  out[1] = 0.5 * (fa + fb);
+  out[3] = fa - fb;
+  mused[0] = m0;
+  mused[1] = m1;
+  return 0;
+}
+
 // edc_green_proj src/asr_edc.f90:174-232: the chain of edc_green run all nlev steps (no depth test) with the projections
 // of every Lanczos vector on the target states, cpr(k, l, t) = sum_ks tw(l, ks, t) psi_k(node ks of t, l), where psi is
 // the unreduced amplitude augcls_amp_c (:251-261): csg(l, g) v(9 (r - 1) + pi(l, g)) / sq(r).  gp(l, t) =

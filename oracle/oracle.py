@@ -39,6 +39,8 @@ def lib():
         L.orc_build_targets.argtypes = L.orc_build.argtypes[:-1] + [_i, C.c_int, _i, _i, C.POINTER(C.c_void_p)]
         L.orc_edc_green_proj.argtypes = [C.c_void_p, C.c_int, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
                                          C.c_int, C.c_int, _i, _i, _d, _d, _d, _d, _i]
+        L.orc_epi_blocks.argtypes = [C.c_void_p, C.c_int, _d, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _d,
+                                     _i]
         L.orc_free.argtypes = [C.c_void_p]
         L.orc_dims.argtypes = [C.c_void_p, _i]
         L.orc_tables.argtypes = [C.c_void_p] + [_i] * 8 + [_d, _d, _i, _i, _i, _d, _d]
@@ -249,6 +251,16 @@ class OracleOp:
         lib().orc_edc_green_proj(self.h, dl.shape[1], _pd(dc), _pd(dl), _pd(en), z.real, z.imag, iv, nlev, TAILS[tail],
                                  int(project), nt, _pi(tnode), _pi(tgop), _pd(tw), _pd(g), _pd(gp), _pd(gp4), C.byref(m))
         return complex(g[0], g[1]), gp, gp4, m.value
+
+    def epi_blocks(self, ed, v9, z, nlev, tail="hull", project=True):
+        """``epi_start`` + ``epi_blocks`` (src/asr_epi.f90:578-663) on the operator's current parameters, frozen sites and
+        characters: returns (x (4,) complex = X0, X1, X2, X1 mismatch; (m0, m1))."""
+        dc, dl, en = _f64(ed["dc"]), _f64(ed["dl"]), _f64(ed["enu"])
+        x = np.zeros(4, np.complex128)
+        m = np.zeros(2, np.int32)
+        _check(lib().orc_epi_blocks(self.h, dl.shape[1], _pd(dc), _pd(dl), _pd(en), _pd(_f64(v9)), z.real, z.imag, nlev,
+                                    TAILS[tail], int(project), _pd(x), _pi(m)))
+        return x, (int(m[0]), int(m[1]))
 
     def edc_green_blk(self, ed, zs, iv, nlev, depth_tol=0.0, tail="hull", project=True):
         """``edc_green_blk`` (src/asr_edc.f90:237-316): returns (g(nb), mused(nb), a(nlev, nb), b(nlev, nb))."""
