@@ -267,10 +267,22 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
         acc[l].y = fma_(row[8], v[8].y, acc[l].y);
       }
     }
+    // the node's links, one slot per lane, read once with a coalesced load and broadcast by shuffles: the row gathers
+    // then wait on one global latency per slot instead of two dependent ones (link, then row)
+    const bool lane_links = op.nslot <= TL;
+    int my_r = -1, my_g = 0;
+    if (lane_links && lane < op.nslot) { my_r = op.hopr[lane + op.nslot * i]; my_g = op.hopg[lane + op.nslot * i]; }
     for (int k = 0; k < op.nslot; ++k) {
-      int r = op.hopr[k + op.nslot * i];
+      int r, gk;
+      if (lane_links) {
+        r = __shfl_sync(0xffffffffu, my_r, k);
+        gk = __shfl_sync(0xffffffffu, my_g, k);
+      } else {
+        r = op.hopr[k + op.nslot * i];
+        gk = op.hopg[k + op.nslot * i];
+      }
       if (r < 0) continue;
-      const unsigned long long pw = piw[op.hopg[k + op.nslot * i]];
+      const unsigned long long pw = piw[gk];
       const T2* src = in + vix(it.tile, bv.nn, r, 0) + lane;
       T2 v[9];
       for (int lp = 0; lp < 9; ++lp) {
