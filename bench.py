@@ -304,6 +304,96 @@ def example_leg(torch):
             "published_basis": "67 chains/s x 20.86 mean depth, 2 x 48 CPU threads (example/reference/cuzn_alloy/asr.out)"}
 
 
+def spectral_leg(torch):
+    """Projected chains (edc_green_proj) for the Bloch spectral function on the workload's operator: fcc ternary, D2h,
+    targets = the sites within 1.5 alat of the origin (minimum image), 3 central species x 9 start orbitals x 64 real
+    energies, depth 24.  Chain-steps/s with the projections against the same chains without them."""
+    import asr_b200 as A
+    from asr_b200 import spectral as SP
+    from asr_b200 import synthetic as S
+    case, fl, _, _ = workload()
+    coord = case["coord"]
+    m = 10
+    h = (coord + m // 2) % m - m // 2
+    sel = np.nonzero(np.sum(h * h, axis=0) <= int(4 * 1.5 ** 2 + 1e-9))[0]
+    tsite = (sel + 1).astype(np.int32)
+    op, tnode, tgop = A.build_augcls_operator(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, 3,
+                                              maxrank=1, flippable=fl, tsite=tsite)
+    sp = S.draw_species(3, seed=1)
+    conc = [0.66, 0.14, 0.20]
+    z = np.linspace(-1.2, 0.6, 64) + 0.01j
+    t0 = int(np.nonzero(tsite == 1)[0][0])
+    specs, tws = [], []
+    for cen in (1, 2, 3):
+        ed = S.edc_params(sp, cen)
+        tw = np.zeros((9, op.nsmax, len(tsite)))
+        for t in range(len(tsite)):
+            tw[:, :, t] = SP.spectral_dressing(ed["dc"], ed["dl"], [1, 2, 3], conc, t == t0, op.nsmax)
+        for l0 in range(1, 10):
+            specs.append(A.ChainSpec(c=ed["c"], d=ed["d"], o=ed["o"], e=ed["e"], pa=ed["pa"], pb=ed["pb"], frozen_sp=cen,
+                                     start_orb=l0, nlev=24))
+            tws.append(tw)
+    tw = np.stack(tws, axis=3)
+    A.chains_proj(op, specs[:1], z[:4], tnode, tgop, tw[..., :1])
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    r = A.chains_proj(op, specs, z, tnode, tgop, tw)
+    torch.cuda.synchronize()
+    sec_p = time.perf_counter() - t
+    t = time.perf_counter()
+    A.chains_run(op, specs, z, "edc", 0.0, "hull", "fp64")
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t
+    steps = int(np.sum(r["m"]))
+    return {"nodes": int(op.nn), "targets": int(len(tsite)), "chains": int(r["m"].size), "chain_steps_per_s": steps / sec_p,
+            "without_projections": steps / sec, "projection_overhead": sec_p / sec - 1.0}
+
+
+def epi_leg(torch):
+    """EPI block chains (two projected chains per symmetry-adapted start vector) for a first-shell pair of a bcc binary:
+    levels 4, rank 1, the pair group, the origin on the path 1 -> 2 at lambda = 0.5 and the partner at (1, 1, 1) frozen
+    to species 2, 32 contour energies, depth 24."""
+    import asr_b200 as A
+    from asr_b200 import contour as CT
+    from asr_b200 import epi as EP
+    from asr_b200 import lattices as lat
+    from asr_b200 import synthetic as S
+    l = 8
+    g, coord, bvec = lat.periodic_graph_shells("bcc", l, 4)
+    block, block0 = S.sk_blocks(bvec, 2)
+    jp = int(np.nonzero(np.all(coord == np.array([1, 1, 1])[:, None], axis=0))[0][0]) + 1
+    cls = np.ones(g.n, np.int32)
+    cls[jp - 1] = 2
+    spc = np.asfortranarray(np.array([[1, 1], [2, 0]], np.int32))
+    conc = np.asfortranarray(np.array([[0.5, 1.0], [0.5, 0.0]]))
+    mdl = S.ClassModel(nsp=3, nsc=np.array([2, 1], np.int32), spc=spc, conc=conc,
+                       block=np.asfortranarray(block.reshape(9, 9, -1, 1)), block0=np.asfortranarray(block0.reshape(9, 9, 1)))
+    perm, mats = EP.epi_pair_ops(coord, 2 * l, cls)
+    dmat = lat.orbital_rep(mats)
+    fl = (cls == 1).astype(np.int32)
+    fl[0] = 0
+    op = A.build_augcls_operator(g, mdl, cls, perm, dmat, 1, 4, maxrank=1, flippable=fl)
+    ll = S.ORB_L.astype(float)
+    par = [EP.EpiPar(e=0.10 * ll, c=0.30 - 0.15 * ll, d=0.30 - 0.07 * ll, o=0.0 * ll),
+           EP.EpiPar(e=0.05 * ll, c=0.45 - 0.10 * ll, d=0.27 - 0.06 * ll, o=0.0 * ll)]
+    pt = EP.epi_path(par[0], par[1], 0.5)
+    params, ed = EP.epi_setup(par, pt)
+    vec, chi, lo = EP.epi_adapted(dmat)
+    op.set_params(*params)
+    op.freeze_site(1, 3)
+    op.freeze_site(jp, 2)
+    z, _ = CT.contour_nodes(-1.2, 0.3, 32)
+    EP.epi_blocks(op, params, ed, vec[:, :1], chi[:, :1], lo[:1], z[:2], 24)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    x, m = EP.epi_blocks(op, params, ed, vec, chi, lo, z, 24)
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t
+    steps = int(np.sum(m))
+    return {"nodes": int(op.nn), "pair_group": int(perm.shape[1]), "chains": int(m.size), "chain_steps_per_s": steps / sec,
+            "seconds": sec, "x1_mismatch_max": float(np.max(np.abs(x[3]) / np.abs(x[1])))}
+
+
 def scf_model(l, maxlevel, precision):
     """The large batched SCF configuration: equiatomic 5-component fcc random alloy (Fe, Co, Ni, Cr, Mn-like parameters
     drawn from seed 4), spd 9 orbitals, spin-polarised (2 x 5 x 9 = 90 chain groups), depths U{20..32}, 64-point
@@ -406,6 +496,8 @@ def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
     out["kpm"] = kpm_leg(torch)
     out["plain"] = plain_leg(torch)
     out["example_cuzn"] = example_leg(torch)
+    out["spectral"] = spectral_leg(torch)
+    out["epi"] = epi_leg(torch)
     if args.scf:
         out["scf"] = scf_leg(torch, args.scf == 2)
     return out
