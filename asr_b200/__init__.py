@@ -6,10 +6,10 @@ The operator, chains and continued fractions run in the compiled library asr_b20
 from . import lattices, synthetic
 from ._lib import AsrError, LIB_PATH, lib
 from .augcls import AugclsOp, Context, build_augcls_operator, default_context
-from .chains import (ChainSpec, cf_species, chains_adjoint, chains_proj, chains_run, chains_run_device, edc_green_blk,
+from .chains import (ChainSpec, autotune, cf_species, chains_adjoint, chains_proj, chains_run, chains_run_device, edc_green_blk,
                      edc_green_proj, lanczos)
 from .contour import contour_moment, contour_nodes, contour_nodes_closed, contour_nodes_fermi, fermi_npole, gauss_legendre
 
 __all__ = ["lattices", "synthetic", "AsrError", "LIB_PATH", "lib", "AugclsOp", "Context", "build_augcls_operator",
-           "default_context", "ChainSpec", "cf_species", "chains_adjoint", "chains_proj", "edc_green_proj", "chains_run", "chains_run_device", "edc_green_blk", "lanczos",
+           "default_context", "ChainSpec", "autotune", "cf_species", "chains_adjoint", "chains_proj", "edc_green_proj", "chains_run", "chains_run_device", "edc_green_blk", "lanczos",
            "contour_moment", "contour_nodes", "contour_nodes_closed", "contour_nodes_fermi", "fermi_npole", "gauss_legendre"]

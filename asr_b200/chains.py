@@ -199,6 +199,19 @@ def edc_green_proj(op: AugclsOp, ed: dict, z, iv: int, nlev: int, tnode, tgop, t
     return r["g"][0, 0], r["gp"][:, :, 0, 0], r["gp4"][:, :, 0, 0]
 
 
+def autotune(op: AugclsOp, specs, z, precision: str = "fp64", levels: int = 8) -> dict:
+    """Choose the batch shape (tiles per batch, nodes per warp) of the chains on this operator by timing the given groups
+    (depth capped at ``levels``, at most 64 energies); later calls in this precision use it.  Returns dict(tiles_per_batch,
+    nodes_per_warp, ms_tiles (4, 8, 16, 32 tiles at 4 nodes per warp), ms_npw (1, 2, 4, 8 nodes per warp))."""
+    z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
+    arr, keep = _groups(specs)
+    tpb, npw = C.c_int(), C.c_int()
+    times = np.zeros(8)
+    check(lib().asr_autotune(op.ctx.h, op.h, arr, len(specs), _pd(z), z.shape[0], PREC[precision], int(levels), C.byref(tpb),
+                             C.byref(npw), _pd(times)))
+    return dict(tiles_per_batch=tpb.value, nodes_per_warp=npw.value, ms_tiles=times[:4].tolist(), ms_npw=times[4:].tolist())
+
+
 def lanczos(op: AugclsOp, l0: int, nmax: int, precision: str = "fp64"):
     """Reference ``lanczos`` (src/reference/asr_recursion.f90:17-58) from e_(node 1, l0) on the operator's parameters.
     Returns (a(nmax), b(nmax), n) with b(n) of the last step."""

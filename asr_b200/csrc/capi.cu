@@ -1,4 +1,5 @@
 // C ABI of asr_b200 (declarations and reference citations in include/asr_b200.h).
+#include <chrono>
 #include <cstdarg>
 #include <cmath>
 #include <cstring>
@@ -982,6 +983,70 @@ int asr_chains_proj(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int
   if (mused) for (int L = 0; L < nlane; ++L) mused[L] = hm[L];
   ctx->nchain += nlane;
   ctx->nfall += nfall;
+  return ASR_OK;
+}
+
+// Batch-shape autotuner: times the chains of the given groups (depth capped at `levels`, at most 64 of the energies) with
+// 4, 8, 16, 32 tiles per batch at 4 nodes per warp, then 1, 2, 4, 8 nodes per warp at the best batch, and keeps the
+// fastest pair on the operator for this precision (used whenever a call leaves the shape automatic).  times (8) receives
+// the wall times in ms (-1 where a candidate was skipped), or NULL.
+int asr_autotune(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz, int precision,
+                 int levels, int* tpb_out, int* npw_out, double* times) {
+  if (!ctx || !op || !groups || ngroup < 1 || !z || nz < 1 || levels < 1) { set_error("asr_autotune: bad argument"); return ASR_EINVAL; }
+  if (precision != ASR_FP64 && precision != ASR_FP32) { set_error("asr_autotune: unknown precision"); return ASR_EINVAL; }
+  ASR_TRY(set_device(ctx));
+  GroupLayout GL = layout(op);
+  std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
+  std::vector<GroupInfo> gi(ngroup);
+  for (int q = 0; q < ngroup; ++q) {
+    const asr_chain_group& G = groups[q];
+    if (!G.c || !G.d) { set_error("asr_autotune: group %d without c or d", q + 1); return ASR_EINVAL; }
+    int nl = std::min(std::max(G.nlev, 1), std::min(levels, NLMAX));
+    ASR_TRY(make_group(op, GL, G.c, G.d, G.o, G.e, G.pa, G.pb, G.frozen_sp, G.start_orb, nl, nullptr,
+                       blob.data() + (size_t)GL.stride * q, gi[q]));
+  }
+  const int nzt = std::min(nz, 64), nlane = ngroup * nzt;
+  std::vector<int> lg(nlane);
+  std::vector<double2> lz(nlane);
+  for (int q = 0; q < ngroup; ++q)
+    for (int j = 0; j < nzt; ++j) { lg[(size_t)q * nzt + j] = q; lz[(size_t)q * nzt + j] = make_double2(z[2 * j], z[2 * j + 1]); }
+  Dev<double2> d_lz, d_g;
+  ASR_TRY(d_lz.alloc(nlane)); ASR_TRY(d_g.alloc(nlane));
+  ASR_CUDA(cudaMemcpy(d_lz.p, lz.data(), nlane * sizeof(double2), cudaMemcpyHostToDevice));
+  const int ntile = ngroup * ((nzt + TL - 1) / TL);
+  const int pix = precision == ASR_FP64 ? 0 : 1;
+  auto timed = [&](int tpb, int npw, double& ms) -> int {
+    RunOptions opt;
+    opt.mode = ASR_MODE_EDC; opt.tail = ASR_TAIL_HULL; opt.precision = precision; opt.project = 1;
+    opt.tiles_per_batch = tpb; opt.nodes_per_warp = npw;
+    int64_t nf = 0, ns = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    ASR_TRY(run_lanes(ctx, op, gi, blob, GL, lg, d_lz.p, nlane, opt, d_g.p, nullptr, nullptr, nullptr, &nf, &ns));
+    ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return ASR_OK;
+  };
+  const int tpbs[4] = {4, 8, 16, 32}, npws[4] = {1, 2, 4, 8};
+  double tab[8];
+  for (double& t : tab) t = -1.0;
+  double warm;
+  ASR_TRY(timed(4, 4, warm));
+  int best_t = 0, best_n = 4;
+  double best = 1e300;
+  for (int c = 0; c < 4; ++c) {
+    if (tpbs[c] > ntile && c > 0) continue;
+    ASR_TRY(timed(tpbs[c], 4, tab[c]));
+    if (tab[c] < best) { best = tab[c]; best_t = tpbs[c]; }
+  }
+  best = 1e300;
+  for (int c = 0; c < 4; ++c) {
+    ASR_TRY(timed(best_t, npws[c], tab[4 + c]));
+    if (tab[4 + c] < best) { best = tab[4 + c]; best_n = npws[c]; }
+  }
+  op->tuned_tpb[pix] = best_t;
+  op->tuned_npw[pix] = best_n;
+  if (tpb_out) *tpb_out = best_t;
+  if (npw_out) *npw_out = best_n;
+  if (times) for (int c = 0; c < 8; ++c) times[c] = tab[c];
   return ASR_OK;
 }
 

@@ -946,13 +946,15 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   cudaMemGetInfo(&freeb, &totb);
   // 32-lane tiles per batch: larger batches amortise the per-level reductions and launch gaps (measured on the fcc
   // ternary workload: FP64 best at 16 tiles, FP32 at 8 with 4 nodes per warp)
-  int tpb = opt.tiles_per_batch > 0 ? opt.tiles_per_batch : (std::is_same<ST, double>::value ? 16 : 8);
+  const int prec_ix = std::is_same<ST, double>::value ? 0 : 1;
+  int tpb = opt.tiles_per_batch > 0 ? opt.tiles_per_batch
+          : op->tuned_tpb[prec_ix] > 0 ? op->tuned_tpb[prec_ix] : (std::is_same<ST, double>::value ? 16 : 8);
   if (const char* e = getenv("ASR_TILES_PER_BATCH")) tpb = std::max(1, atoi(e));
   // projections: per tile nlevmax x 9 nt x 32 complex values
   const size_t proj_tile_bytes = proj ? (size_t)nlevmax * 9 * proj->nt * TL * sizeof(double2) : 0;
   while (tpb > 1 && (size_t)tpb * (nvec * vec_bytes + proj_tile_bytes) > freeb / 2) tpb /= 2;
   tpb = std::min(tpb, ntile_all);
-  int npw = std::max(1, opt.nodes_per_warp);
+  int npw = opt.nodes_per_warp > 0 ? opt.nodes_per_warp : op->tuned_npw[prec_ix] > 0 ? op->tuned_npw[prec_ix] : 4;
   if (const char* e = getenv("ASR_NODES_PER_WARP")) npw = std::max(1, atoi(e));
   const int npb = WPB * npw;
   const int bpt = (nn + npb - 1) / npb;

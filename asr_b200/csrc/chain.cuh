@@ -61,8 +61,8 @@ struct RunOptions {
   int tail = ASR_TAIL_HULL;
   int precision = ASR_FP64;
   int project = 1;
-  int tiles_per_batch = 0;   // 0: automatic
-  int nodes_per_warp = 4;
+  int tiles_per_batch = 0;   // 0: automatic (the operator's tuned value, else 16 in FP64 and 8 in FP32)
+  int nodes_per_warp = 0;    // 0: automatic (the operator's tuned value, else 4)
 };
 
 // owning device buffer (freed on scope exit)

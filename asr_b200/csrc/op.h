@@ -55,6 +55,8 @@ struct asr_op {
   asr_ctx* ctx = nullptr;
   int nn = 0, nslot = 0, nsmax = 0, nop = 0, ncls = 0, nsp = 0, ntype = 1, nsite = 0, nstab = 0, start_site = 1;
   int start_l = 1;
+  // batch shape chosen by asr_autotune per precision (index 0 FP64, 1 FP32); 0: the built-in defaults
+  int tuned_tpb[2] = {0, 0}, tuned_npw[2] = {0, 0};
   // host copies of the model and group
   std::vector<int> nsc, spc;       // spc(ldspc, ncls)
   int ldspc = 1;

@@ -42,6 +42,7 @@ def parse():
     p.add_argument("--e2e", type=int, default=1, help="time the host-buffer C-ABI path too (1) or skip it (0)")
     p.add_argument("--scf", type=int, default=0,
                    help="SCF leg: 0 none, 1 two timed iterations at full size + convergence on a small cluster, 2 converge at full size")
+    p.add_argument("--autotune", type=int, default=1, help="choose the batch shape by timing first (1) or use the defaults (0)")
     p.add_argument("--legs", type=int, default=1,
                    help="also measure the mixed-precision leg with its DOS error and the adjoint leg (1) or not (0)")
     return p.parse_args()
@@ -442,6 +443,7 @@ def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
     nzs = args.nz_slice
     depth = np.array([g["nlev"] for g in groups])
     out = {}
+    out["fp32_batch_shape"] = A.autotune(op, specs, z_all[:nzs], "fp32")
     step(0, "fp32")
     torch.cuda.synchronize()
     nsteps = max(1, min(args.steps, 3))
@@ -537,6 +539,10 @@ def main():
     depth_per_group = np.array([g["nlev"] for g in groups])
     chain_steps_per_step = int(depth_per_group.sum()) * nzs
 
+    # batch shape (tiles per batch, nodes per warp) chosen by timing on this operator (asr_autotune), outside the timed region
+    tune = (A.autotune(op, specs, z_all[:nzs], args.precision) if args.autotune else
+            {"tiles_per_batch": 16 if args.precision == "fp64" else 8, "nodes_per_warp": 4, "ms_tiles": None, "ms_npw": None})
+
     def slice_of(it):
         # each rank walks its own slices (weak scaling); rank r starts r slices further
         start = ((it * world + rank) * nzs) % (nall - nzs + 1)
@@ -627,6 +633,8 @@ def main():
                        "chains_per_step": len(specs) * nzs, "chain_steps_per_step": chain_steps_per_step,
                        "l2": "inputs larger than L2 (one 32-lane vector is %.0f MB)" % (op.nn * 9 * 32 * 16 / 1e6),
                        "parallelism": f"chain tasks over {world} GPU(s)", "operator_build_s": build_s,
+                       "batch_shape": {"tiles_per_batch": tune["tiles_per_batch"], "nodes_per_warp": tune["nodes_per_warp"],
+                                       "autotune_ms_tiles_4_8_16_32": tune["ms_tiles"], "autotune_ms_npw_1_2_4_8": tune["ms_npw"]},
                        "precision": args.precision},
             "e2e": {"value": e2e, "unit": "chain-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,

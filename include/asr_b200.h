@@ -155,6 +155,14 @@ int asr_chains_proj(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int
 int asr_epi_blocks(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, const double* v9, const double* chi, int ngroup,
                    const double* z, int nz, int tail, int precision, int project, double* x, int* mused);
 
+/* Batch-shape autotuner (no counterpart in the reference, which has no device): times the chains of the given groups
+ * (depth capped at `levels`, at most 64 of the energies) over tiles per batch {4, 8, 16, 32} and nodes per warp
+ * {1, 2, 4, 8} and keeps the fastest shape on the operator for this precision; later calls that leave the shape
+ * automatic use it.  The shape does not change results beyond the order of the per-block partial sums (rounding).
+ * tpb, npw: the chosen shape; times(8) the wall times in ms (-1: skipped) or NULL. */
+int asr_autotune(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz, int precision,
+                 int levels, int* tpb, int* npw, double* times);
+
 /* ---- route ed3 (src/asr_ed3.f90): chains on z - K'(z), K' = et - h' + u h' + h' u - h' Qt h', h' = g + d S d ---------- */
 typedef struct asr_ed3_group {
   const double *g, *d;                    /* (9, nsp): h' of ed3_setup (:57-79): g = (D_c / D_s)(C - E_nu), d = D_c^1/2 */
