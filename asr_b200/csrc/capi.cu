@@ -427,24 +427,33 @@ int asr_op_export_tables(const asr_op* op, int* flipr, int* flipg, int* hopr, in
   ASR_CUDA(cudaMemcpyAsync(nc.data(), op->d_ncl, nn, cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaMemcpyAsync(sqv.data(), op->d_sq, nn * sizeof(double), cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaStreamSynchronize(s));
-  for (size_t q = 0; q < nsm * nn; ++q) {
-    if (flipr) flipr[q] = fr[q] + 1;    // -1 -> 0 (absent), 0-based -> 1-based
-    if (flipg) flipg[q] = fg[q] + 1;
-  }
-  for (size_t q = 0; q < ns * nn; ++q) {
-    if (hopr) hopr[q] = hr[q] + 1;
-    if (hopg) hopg[q] = hg[q] + 1;
-  }
+  // the device keeps the nodes in its locality order: back to the reference numbering (node i of the build)
+  auto ref = [&](int dev) { return dev >= 0 ? op->ref_node(dev) : -1; };
   for (size_t i = 0; i < nn; ++i) {
-    if (lst) lst[i] = ls[i];
-    if (site) site[i] = st[i];
-    if (ncl) ncl[i] = nc[i] + 1;
-    if (level) level[i] = lv[i];
-    if (norb) norb[i] = (double)ob[i];
-    if (sq) sq[i] = sqv[i];
+    const size_t n = (size_t)op->dev_node((int)i);
+    for (size_t k = 0; k < nsm; ++k) {
+      if (flipr) flipr[k + nsm * i] = ref(fr[k + nsm * n]) + 1;    // -1 -> 0 (absent), 0-based -> 1-based
+      if (flipg) flipg[k + nsm * i] = fg[k + nsm * n] + 1;
+    }
+    for (size_t k = 0; k < ns; ++k) {
+      if (hopr) hopr[k + ns * i] = ref(hr[k + ns * n]) + 1;
+      if (hopg) hopg[k + ns * i] = hg[k + ns * n] + 1;
+    }
+    if (lst) lst[i] = ls[n];
+    if (site) site[i] = st[n];
+    if (ncl) ncl[i] = nc[n] + 1;
+    if (level) level[i] = lv[n];
+    if (norb) norb[i] = (double)ob[n];
+    if (sq) sq[i] = sqv[n];
   }
-  if (stab_ptr) for (size_t i = 0; i <= nn; ++i) stab_ptr[i] = sp[i] + 1;
-  if (stab) for (int q = 0; q < op->nstab; ++q) stab[q] = sb[q] + 1;
+  int pos = 0;
+  for (size_t i = 0; i < nn; ++i) {
+    const int n = op->dev_node((int)i), len = sp[n + 1] - sp[n];
+    if (stab_ptr) stab_ptr[i] = pos + 1;
+    if (stab) for (int q = 0; q < len; ++q) stab[pos + q] = sb[sp[n] + q] + 1;
+    pos += len;
+  }
+  if (stab_ptr) stab_ptr[nn] = pos + 1;
   return ASR_OK;
 }
 
@@ -933,7 +942,7 @@ int asr_chains_proj(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int
   for (size_t q = 0; q < tn.size(); ++q) {
     if (tnode[q] < 0 || tnode[q] > op->nn) { set_error("asr_chains_proj: target node out of range"); return ASR_EINVAL; }
     if (tnode[q] > 0 && (tgop[q] < 1 || tgop[q] > op->nop)) { set_error("asr_chains_proj: target operation out of range"); return ASR_EINVAL; }
-    tn[q] = tnode[q] - 1;
+    tn[q] = tnode[q] > 0 ? op->dev_node(tnode[q] - 1) : -1;   // reference numbering -> the device's node order
     tg[q] = tnode[q] > 0 ? tgop[q] - 1 : 0;
   }
   ASR_TRY(set_device(ctx));

@@ -2350,10 +2350,11 @@ int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   std::vector<double2> hx(nel, make_double2(0, 0));
   for (int v = 0; v < nvec; ++v)
     for (int i = 0; i < nn; ++i)
-      for (int l = 0; l < 9; ++l) {
+      for (int l = 0; l < 9; ++l) {   // user vectors in the reference numbering, device rows in the device node order
+        const int n = op->dev_node(i);
         size_t src = (size_t)v * 9 * nn + 9 * (size_t)i + l;
-        size_t dst = (((size_t)(v / TL) * nn + i) * 9 + l) * TL + v % TL;
-        double f = what == APPLY_PROJECT ? 1.0 : 1.0 / sqv[i];
+        size_t dst = (((size_t)(v / TL) * nn + n) * 9 + l) * TL + v % TL;
+        double f = what == APPLY_PROJECT ? 1.0 : 1.0 / sqv[n];
         hx[dst] = complex_in ? make_double2(f * x_host[2 * src], f * x_host[2 * src + 1]) : make_double2(f * x_host[src], 0.0);
       }
   Dev<double> d_gblob;
@@ -2408,9 +2409,10 @@ int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   for (int v = 0; v < nvec; ++v)
     for (int i = 0; i < nn; ++i)
       for (int l = 0; l < 9; ++l) {
+        const int n = op->dev_node(i);
         size_t dst = (size_t)v * 9 * nn + 9 * (size_t)i + l;
-        double2 val = hy[(((size_t)(v / TL) * nn + i) * 9 + l) * TL + v % TL];
-        if (what != APPLY_PROJECT) val = cscale(val, sqv[i]);
+        double2 val = hy[(((size_t)(v / TL) * nn + n) * 9 + l) * TL + v % TL];
+        if (what != APPLY_PROJECT) val = cscale(val, sqv[n]);
         if (complex_in || what != APPLY_H) { y_host[2 * dst] = val.x; y_host[2 * dst + 1] = val.y; }
         else y_host[dst] = val.x;
       }

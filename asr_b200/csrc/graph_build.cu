@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <string>
 #include <vector>
 
 #include "op.h"
@@ -413,6 +414,142 @@ inline int blocks(long n, int bs) { return (int)((n + bs - 1) / bs); }
 
 }  // namespace
 
+// ---------------------------------------------------------------------------------------------------- node order
+// The build numbers nodes in the reference's serial order (breadth-first over two-hop candidates), in which the hop
+// neighbours of a node lie a median of ~1e3 nodes away (up to the width of a level).  The chain kernels gather the 9
+// orbital rows of every hop neighbour, so the device keeps its tables in a reverse Cuthill-McKee order of the hop graph
+// (start node kept first), where the neighbours lie within ~1e2 nodes and the gathers stay in L2.  Results do not
+// depend on the order: every vector and table is permuted consistently, and the host interfaces translate.
+template <typename T>
+__global__ void k_perm_rows(int nn, int w, const int* old_of_new, const int* new_of_old, const T* in, T* out, bool remap) {
+  long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long)nn * w) return;
+  int n = (int)(q / w), k = (int)(q % w);
+  T v = in[(size_t)old_of_new[n] * w + k];
+  if (remap && v >= 0) v = (T)new_of_old[(int)v];
+  out[q] = v;
+}
+
+template <typename T>
+int permute_rows(cudaStream_t s, int nn, int w, const int* d_oon, const int* d_noo, T*& p, bool remap) {
+  if (!p || w == 0) return ASR_OK;
+  T* q = nullptr;
+  ASR_CUDA(cudaMalloc(&q, std::max<size_t>((size_t)nn * w, 1) * sizeof(T)));
+  long n = (long)nn * w;
+  k_perm_rows<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(nn, w, d_oon, d_noo, p, q, remap);
+  ASR_CUDA(cudaGetLastError());
+  ASR_CUDA(cudaStreamSynchronize(s));
+  cudaFree(p);
+  p = q;
+  return ASR_OK;
+}
+
+// reverse Cuthill-McKee order of the symmetrised hop graph (host; components in order of their lowest node, each from a
+// pseudo-peripheral node of minimum degree), with node 0 moved to the front
+static std::vector<int> rcm_order(int nn, int ns, const std::vector<int>& hopr) {
+  std::vector<std::vector<int>> adj(nn);
+  for (int i = 0; i < nn; ++i)
+    for (int k = 0; k < ns; ++k) {
+      int j = hopr[(size_t)i * ns + k];
+      if (j >= 0 && j != i) { adj[i].push_back(j); adj[j].push_back(i); }
+    }
+  for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+  std::vector<int> deg(nn), order, level(nn, -1);
+  for (int i = 0; i < nn; ++i) deg[i] = (int)adj[i].size();
+  order.reserve(nn);
+  std::vector<char> seen(nn, 0);
+  auto bfs_far = [&](int s0, std::vector<int>& comp) {   // breadth-first levels; returns a last-level node of min degree
+    comp.clear();
+    comp.push_back(s0);
+    level[s0] = 0;
+    for (size_t h = 0; h < comp.size(); ++h)
+      for (int j : adj[comp[h]]) if (level[j] < 0) { level[j] = level[comp[h]] + 1; comp.push_back(j); }
+    int far = comp.back(), lmax = level[far];
+    for (int v : comp) if (level[v] == lmax && deg[v] < deg[far]) far = v;
+    for (int v : comp) level[v] = -1;
+    return std::make_pair(far, lmax);
+  };
+  std::vector<int> comp;
+  for (int r = 0; r < nn; ++r) {
+    if (seen[r]) continue;
+    int s0 = r, ecc = -1;
+    for (int it = 0; it < 8; ++it) {   // pseudo-peripheral node: move to the far end while the eccentricity grows
+      auto fe = bfs_far(s0, comp);
+      if (fe.second <= ecc) break;
+      ecc = fe.second;
+      s0 = fe.first;
+    }
+    size_t base = order.size();
+    order.push_back(s0);
+    seen[s0] = 1;
+    for (size_t h = base; h < order.size(); ++h) {
+      int v = order[h];
+      std::vector<int> nb;
+      for (int j : adj[v]) if (!seen[j]) { seen[j] = 1; nb.push_back(j); }
+      std::sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+      order.insert(order.end(), nb.begin(), nb.end());
+    }
+  }
+  std::reverse(order.begin(), order.end());
+  std::vector<int> out;
+  out.reserve(nn);
+  out.push_back(0);
+  for (int v : order) if (v != 0) out.push_back(v);
+  return out;
+}
+
+int reorder_nodes(asr_ctx* ctx, asr_op* op) {
+  cudaStream_t s = ctx->stream;
+  const int nn = op->nn, ns = op->nslot, nsm = op->nsmax;
+  std::vector<int> hr((size_t)nn * std::max(ns, 1), -1);
+  if (ns) ASR_CUDA(cudaMemcpyAsync(hr.data(), op->d_hopr, (size_t)nn * ns * sizeof(int), cudaMemcpyDeviceToHost, s));
+  std::vector<int> sp(nn + 1);
+  std::vector<uint8_t> sb(std::max(op->nstab, 1));
+  ASR_CUDA(cudaMemcpyAsync(sp.data(), op->d_stab_ptr, (nn + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (op->nstab) ASR_CUDA(cudaMemcpyAsync(sb.data(), op->d_stab, op->nstab, cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> oon = rcm_order(nn, ns, hr), noo(nn);
+  for (int n = 0; n < nn; ++n) noo[oon[n]] = n;
+  int *d_oon = nullptr, *d_noo = nullptr;
+  ASR_CUDA(cudaMalloc(&d_oon, nn * sizeof(int)));
+  ASR_CUDA(cudaMalloc(&d_noo, nn * sizeof(int)));
+  ASR_CUDA(cudaMemcpyAsync(d_oon, oon.data(), nn * sizeof(int), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_noo, noo.data(), nn * sizeof(int), cudaMemcpyHostToDevice, s));
+  int rc = ASR_OK;
+  auto run = [&](int r) { if (rc == ASR_OK) rc = r; };
+  run(permute_rows<int>(s, nn, 1, d_oon, d_noo, op->d_site, false));
+  run(permute_rows<int>(s, nn, 1, d_oon, d_noo, op->d_level, false));
+  run(permute_rows<int>(s, nn, 1, d_oon, d_noo, op->d_orb, false));
+  run(permute_rows<int8_t>(s, nn, 1, d_oon, d_noo, op->d_lst, false));
+  run(permute_rows<int8_t>(s, nn, 1, d_oon, d_noo, op->d_ncl, false));
+  run(permute_rows<int8_t>(s, nn, 1, d_oon, d_noo, op->d_typ, false));
+  run(permute_rows<int8_t>(s, nn, 1, d_oon, d_noo, op->d_start, false));
+  run(permute_rows<int8_t>(s, nn, 1, d_oon, d_noo, op->d_frozen, false));
+  run(permute_rows<double>(s, nn, 1, d_oon, d_noo, op->d_sq, false));
+  run(permute_rows<double>(s, nn, 1, d_oon, d_noo, op->d_isq, false));
+  run(permute_rows<int>(s, nn, nsm, d_oon, d_noo, op->d_flipr, true));
+  run(permute_rows<uint8_t>(s, nn, nsm, d_oon, d_noo, op->d_flipg, false));
+  run(permute_rows<int>(s, nn, ns, d_oon, d_noo, op->d_hopr, true));
+  run(permute_rows<uint8_t>(s, nn, ns, d_oon, d_noo, op->d_hopg, false));
+  cudaFree(d_oon);
+  cudaFree(d_noo);
+  if (rc != ASR_OK) return rc;
+  // stabiliser lists (ragged): rebuilt on the host in the new order
+  std::vector<int> sp2(nn + 1, 0);
+  std::vector<uint8_t> sb2(std::max(op->nstab, 1));
+  for (int n = 0; n < nn; ++n) {
+    int o = oon[n], len = sp[o + 1] - sp[o];
+    sp2[n + 1] = sp2[n] + len;
+    std::copy(sb.begin() + sp[o], sb.begin() + sp[o] + len, sb2.begin() + sp2[n]);
+  }
+  ASR_CUDA(cudaMemcpyAsync(op->d_stab_ptr, sp2.data(), (nn + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+  if (op->nstab) ASR_CUDA(cudaMemcpyAsync(op->d_stab, sb2.data(), op->nstab, cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  op->old_of_new = std::move(oon);
+  op->new_of_old = std::move(noo);
+  return ASR_OK;
+}
+
 int build_operator(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, int ncls, const int* nsc, const int* cls,
                    const int* perm, int nop, int start, int maxlevel, int maxrank, const int* flippable, const int* stype,
                    asr_op* op, const int* tsite, int ntarget, int* tnode, int* tgop) {
@@ -596,6 +733,8 @@ int build_operator(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr, 
   op->d_frozen = frz.release(); op->d_sq = sq.release(); op->d_isq = isq.release();
   op->d_flipr = flipr.release(); op->d_flipg = flipg.release(); op->d_hopr = hopr.release(); op->d_hopg = hopg.release();
   op->d_stab_ptr = sptr.release(); op->d_stab = stab.release();
+  const char* order_env = getenv("ASR_NODE_ORDER");   // "build": keep the reference numbering on the device
+  if (!(order_env && std::string(order_env) == "build")) ASR_TRY(reorder_nodes(ctx, op));
   return ASR_OK;
 }
 

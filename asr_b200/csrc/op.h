@@ -67,6 +67,11 @@ struct asr_op {
   std::vector<double> block0;      // (9, 9, ntype)
   std::vector<double> c, d, o, e;  // (9, nsp) current operator parameters
   std::vector<int8_t> frozen_h;    // (nn) operator-level frozen species
+  // device node order: the tables live in a locality order (reverse Cuthill-McKee of the hop graph, start node first);
+  // old_of_new[n] is the reference (build) index of device node n, new_of_old its inverse; empty: the build order
+  std::vector<int> old_of_new, new_of_old;
+  int dev_node(int old) const { return new_of_old.empty() ? old : new_of_old[old]; }
+  int ref_node(int dev) const { return old_of_new.empty() ? dev : old_of_new[dev]; }
   // device tables
   int* d_site = nullptr;
   int* d_level = nullptr;
