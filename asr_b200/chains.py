@@ -201,7 +201,8 @@ def edc_green_proj(op: AugclsOp, ed: dict, z, iv: int, nlev: int, tnode, tgop, t
 
 def autotune(op: AugclsOp, specs, z, precision: str = "fp64", levels: int = 8) -> dict:
     """Choose the batch shape (tiles per batch, nodes per warp) of the chains on this operator by timing the given groups
-    (depth capped at ``levels``, at most 64 energies); later calls in this precision use it.  Returns dict(tiles_per_batch,
+    (depth capped at ``levels``, at most 64 energies); a candidate must beat the built-in default by 3 %.  Later calls in
+    this precision use the choice.  Returns dict(tiles_per_batch,
     nodes_per_warp, ms_tiles (4, 8, 16, 32 tiles at 4 nodes per warp), ms_npw (1, 2, 4, 8 nodes per warp))."""
     z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
     arr, keep = _groups(specs)
