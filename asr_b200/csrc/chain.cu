@@ -915,7 +915,7 @@ template <typename ST>
 int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
                 const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
                 const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
-                std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj) {
+                std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj, double* dev_ms) {
   typedef typename St2<ST>::T T2;
   cudaStream_t s = ctx->stream;
   const int nn = op->nn;
@@ -996,6 +996,12 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   for (int t = 0; t < ntile_all; ++t) order[t] = t;
   std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return tdepth[x] > tdepth[y]; });
   std::vector<double2> one(nlp, make_double2(1.0, 0.0));
+  cudaEvent_t tev[2] = {nullptr, nullptr};   // device time of the batches (after the allocations), for the autotuner
+  if (dev_ms) {
+    ASR_CUDA(cudaEventCreate(&tev[0]));
+    ASR_CUDA(cudaEventCreate(&tev[1]));
+    ASR_CUDA(cudaEventRecord(tev[0], s));
+  }
   for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
     const int nt = std::min(tpb, ntile_all - t0);
     int kmax = 0;
@@ -1089,6 +1095,15 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
           std::memcpy(&(*b_out)[(size_t)L * NLMAX], &hb[(size_t)q * NLMAX], NLMAX * sizeof(double2));
         }
     }
+  }
+  if (dev_ms) {
+    ASR_CUDA(cudaEventRecord(tev[1], s));
+    ASR_CUDA(cudaEventSynchronize(tev[1]));
+    float ms = 0.f;
+    ASR_CUDA(cudaEventElapsedTime(&ms, tev[0], tev[1]));
+    *dev_ms = ms;
+    cudaEventDestroy(tev[0]);
+    cudaEventDestroy(tev[1]);
   }
   ASR_CUDA(cudaMemcpyAsync(hm_all.data(), d_m_all.p, nlane * sizeof(int), cudaMemcpyDeviceToHost, s));
   int64_t nsteps = 0;
@@ -2325,14 +2340,14 @@ int run_epi(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const
 int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
               const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
               const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
-              std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj) {
+              std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj, double* dev_ms) {
   smem_attrs();
   if (smul_smem(op, sizeof(double)) > 96 * 1024) { set_error("chains: bond tables above 96 KB of shared memory"); return ASR_EINVAL; }
   if (opt.precision == ASR_FP32)
     return run_lanes_t<float>(ctx, op, ginfo, gblob, GL, lane_group, d_lane_z, nlane, opt, d_g_out, a_out, b_out, m_out, nfall_out,
-                              nsteps_out, proj);
+                              nsteps_out, proj, dev_ms);
   return run_lanes_t<double>(ctx, op, ginfo, gblob, GL, lane_group, d_lane_z, nlane, opt, d_g_out, a_out, b_out, m_out, nfall_out,
-                             nsteps_out, proj);
+                             nsteps_out, proj, dev_ms);
 }
 
 // ------------------------------------------------------------------------------------------------ drop-in applications

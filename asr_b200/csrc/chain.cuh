@@ -109,11 +109,13 @@ struct ProjView {
 };
 
 // Runs chains for lanes (group, z) on the operator; results per lane: g (energy of the lane), a, b (NLMAX each), m.
-// proj (optional): the projections of edc_green_proj for every lane.
+// proj (optional): the projections of edc_green_proj for every lane; dev_ms (optional): the device time of the batches,
+// allocations excluded.
 int run_lanes(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
               const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
               const RunOptions& opt, double2* d_g_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
-              std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj = nullptr);
+              std::vector<int>* m_out, int64_t* nfall_out, int64_t* nsteps_out, const ProjSpec* proj = nullptr,
+              double* dev_ms = nullptr);
 
 // EPI block chains (epi_blocks, src/asr_epi.f90:639-663): v9 (9, ngroup) start vectors on the start node; lane kind 0 runs
 // from s0 with the projection on |v> = h'|s0>, kind 1 from |v> / |v| with the projection on s0; per lane g, f, |v|, depth

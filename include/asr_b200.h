@@ -160,7 +160,8 @@ int asr_epi_blocks(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, cons
  * {1, 2, 4, 8} and keeps the fastest shape (a candidate must beat the built-in default, 16 tiles in FP64 and 8 in FP32
  * at 4 nodes per warp, by 3 %) on the operator for this precision; later calls that leave the shape
  * automatic use it.  The shape does not change results beyond the order of the per-block partial sums (rounding).
- * tpb, npw: the chosen shape; times(8) the wall times in ms (-1: skipped) or NULL. */
+ * Each candidate is timed on the device (CUDA events around its batches, allocations excluded, best of two runs).
+ * tpb, npw: the chosen shape; times(8) the device times in ms (-1: skipped) or NULL. */
 int asr_autotune(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz, int precision,
                  int levels, int* tpb, int* npw, double* times);
 
