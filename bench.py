@@ -27,7 +27,7 @@ sys.path.insert(0, ROOT)
 NZ_SLICE = 192
 # DRAM bytes (read + write) per launch of the step kernel from one ncu capture of a 16-tile launch, and the algorithmic
 # bytes of that launch (profiles/k_smul_fcc_ternary_edc.md); traffic is scaled to the bench's mean launch
-NCU_STEP_TRAFFIC = {"fp64": (6.14e9, 16 * 20969 * (2 * 4608.0 + 18 * 5 + 3 * 5 + 20))}
+NCU_STEP_TRAFFIC = {"fp64": (3.30e9, 16 * 20969 * (2 * 4608.0 + 18 * 5 + 3 * 5 + 20))}
 
 
 def parse():
