@@ -939,13 +939,14 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   fused = all_dunif && !any_o;
   if (nlevmax > NLMAX) { set_error("chains: depth %d above the device maximum %d", nlevmax, NLMAX); return ASR_EINVAL; }
   if (op->nop > MAXOP) { set_error("chains: at most %d group operations", MAXOP); return ASR_EINVAL; }
-  // batch size: tiles in flight bounded by memory (3 vectors + temporaries per tile) and by 8 tiles
+  // batch size: tiles in flight, bounded by memory (3 vectors + temporaries per tile)
   const size_t vec_bytes = (size_t)nn * 9 * TL * sizeof(T2);
   const int nvec = 3 + (fused ? 0 : (any_o ? 4 : 2));
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
-  // 32-lane tiles per batch: larger batches amortise the per-level reductions and launch gaps (measured on the fcc
-  // ternary workload: FP64 best at 16 tiles, FP32 at 8 with 4 nodes per warp)
+  // 32-lane tiles per batch: larger batches amortise the per-level reductions and launch gaps; the caller's shape, else
+  // the operator's autotuned one, else the measured defaults of the fcc ternary workload (FP64 16 tiles, FP32 8, 4 nodes
+  // per warp)
   const int prec_ix = std::is_same<ST, double>::value ? 0 : 1;
   int tpb = opt.tiles_per_batch > 0 ? opt.tiles_per_batch
           : op->tuned_tpb[prec_ix] > 0 ? op->tuned_tpb[prec_ix] : (std::is_same<ST, double>::value ? 16 : 8);
