@@ -602,7 +602,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_e2e = float(t.item())
     e2e = total_steps / (ms_e2e / 1000.0)
-    legs = run_legs(args, A, op, specs, groups, z_all, step, stream, world) if args.legs else None
+    # the legs measure single-GPU kernels and configurations: one GPU only (every rank skips them alike)
+    legs = run_legs(args, A, op, specs, groups, z_all, step, stream, world) if args.legs and world == 1 else None
     nsp = 3
     h2d = nzs * 16 + len(specs) * 6 * 9 * nsp * 8
     d2h = len(specs) * nzs * (16 + 4)
