@@ -11,13 +11,15 @@ Host-side restatement of the reference's ``asr_epi`` (src/asr_epi.f90) for the e
 * ``epi_adapted`` (:290-328): symmetry-adapted start vectors of an abelian group of involutions;
 * ``epi_pair_ops`` (:333-363): the pair group (class-preserving D4h about z, reduced to an abelian group of involutions);
 * ``epi_exchange``, ``epi_skip``, ``epi_mirror`` (:257-285);
+* ``epi_pair_list`` / ``epi_pair_ops_c`` / ``epi_pair_list_c`` (:365-568): the pair types of the first shells of the
+  origin (orbits of the class-preserving operations, representative with the largest pair group), on periodic cubic
+  cells and on site clusters;
 * ``epi_blocks`` -- the two projected chains per start vector and energy on the device (``asr_epi_blocks``);
 * ``pair_table`` -- U(c, s) = int_0^1 dlambda [dOmega/dlambda (c0 -> c | s) - dOmega/dlambda (c0 -> c | s0)] with
   Gauss-Legendre nodes in lambda and dOmega/dlambda = -(1/pi) Im sum_j w_j sum_a epi_integrand (the contour weights w_j).
 """
 from __future__ import annotations
 
-import ctypes as C
 from dataclasses import dataclass
 
 import numpy as np
@@ -26,10 +28,12 @@ from . import _lib
 from ._lib import check, lib
 from .augcls import AugclsOp, _pd, _pi
 from .chains import PREC, ChainSpec, _groups
-from .lattices import class_ops
+from .crystal import is_monomial
+from .lattices import class_ops, cubic_site_perms
 
 __all__ = ["EpiPar", "EpiPath", "epi_path", "epi_setup", "epi_integrand", "epi_adapted", "epi_pair_ops", "epi_exchange",
-           "epi_skip", "epi_mirror", "epi_blocks", "trace_at", "pair_table"]
+           "epi_skip", "epi_mirror", "EpiPair", "epi_pair_list", "epi_pair_ops_c", "epi_pair_list_c", "epi_blocks", "trace_at",
+           "pair_table"]
 
 ORB_L = np.array([0, 1, 1, 1, 2, 2, 2, 2, 2])
 
@@ -168,6 +172,147 @@ def epi_mirror(u: np.ndarray) -> np.ndarray:
         for s in range(1, c):
             u[c, s] = u[s, c]
     return u
+
+
+@dataclass
+class EpiPair:
+    """One pair type: shell (1-based), representative partner site (1-based), multiplicity, squared length (half-lattice
+    units squared), partner class, order of its pair group, partner - origin vector (half-lattice units; Cartesian alat
+    units in ``rvec``) and the vectors of every member (``orbit`` / ``rorbit``, columns)."""
+    shell: int
+    site: int
+    mult: int
+    r2: int
+    cls2: int
+    nop: int
+    vec: np.ndarray
+    orbit: np.ndarray
+    rvec: np.ndarray | None = None
+    rorbit: np.ndarray | None = None
+
+
+def epi_pair_list(coord: np.ndarray, mg: int, cls, nshell: int) -> list[EpiPair]:
+    """Pair types of the origin (site 1) with the sites of its first nshell shells on a periodic cubic cell (coordinates in
+    half-lattice units, period mg): each shell splits into orbits of the class-preserving cubic operations; the
+    representative is the member with the largest pair group.  A shell that does not fit into the cell raises ValueError."""
+    coord = np.asarray(coord, dtype=np.int64)
+    cls = np.asarray(cls, dtype=np.int64)
+    n = coord.shape[1]
+    v = (coord - coord[:, :1] + mg // 2) % mg - mg // 2
+    r2 = np.sum(v * v, axis=0)
+    shells, rcur = [], 0
+    for ish in range(1, nshell + 1):
+        rnext = int(np.min(r2[r2 > rcur]))
+        if 4 * rnext >= mg * mg:
+            raise ValueError(f"epi: shell {ish} does not fit into the supercell (increase the supercell)")
+        shells.append(rnext)
+        rcur = rnext
+    p48, _ = cubic_site_perms(coord, mg)
+    keep = [k for k in range(48) if np.array_equal(cls[p48[:, k] - 1], cls)]
+    pairs, done = [], np.zeros(n, dtype=bool)
+    for ish, sh in enumerate(shells, start=1):
+        for i in range(1, n):
+            if r2[i] != sh or done[i]:
+                continue
+            inorb = np.zeros(n, dtype=bool)
+            inorb[p48[i, keep] - 1] = True
+            done |= inorb
+            best, site = 0, -1
+            for j in np.nonzero(inorb)[0]:
+                cl2 = cls.copy()
+                cl2[j] = cls.max() + 1
+                pp, _ = epi_pair_ops(coord, mg, cl2)
+                if pp.shape[1] > best:
+                    best, site = pp.shape[1], int(j)
+            pairs.append(EpiPair(shell=ish, site=site + 1, mult=int(inorb.sum()), r2=int(sh), cls2=int(cls[site]), nop=best,
+                                 vec=v[:, site].copy(), orbit=v[:, inorb].copy()))
+    return pairs
+
+
+def epi_pair_ops_c(perm: np.ndarray, rot: np.ndarray, cls) -> np.ndarray:
+    """Pair group on a site cluster: of the site operations (identity first) the monomial ones that keep the z axis and
+    the classes, reduced to the sign changes of the axes when they do not all commute.  Returns 0-based indices."""
+    perm = np.asarray(perm)
+    rot = np.asarray(rot, dtype=float)
+    cls = np.asarray(cls)
+    tol = 1e-9
+    nk = perm.shape[1]
+    keep = [bool(is_monomial(rot[:, :, k]) and abs(abs(rot[2, 2, k]) - 1.0) < tol and np.array_equal(cls[perm[:, k] - 1], cls))
+            for k in range(nk)]
+    sel = [k for k in range(nk) if keep[k]]
+    one = np.eye(3)
+    abel = all(np.max(np.abs(rot[:, :, i] @ rot[:, :, i] - one)) <= tol for i in sel) and all(
+        np.max(np.abs(rot[:, :, i] @ rot[:, :, j] - rot[:, :, j] @ rot[:, :, i])) <= tol for a, i in enumerate(sel) for j in sel[a + 1:])
+    if not abel:
+        sel = [k for k in sel if np.max(np.abs(rot[:, :, k] - np.diag(np.diag(rot[:, :, k])))) < tol]
+    if not sel or sel[0] != 0:
+        raise RuntimeError("epi_pair_ops_c: operation 1 is not the identity")
+    return np.array(sel, dtype=np.int64)
+
+
+def _box_key(x: float) -> float:
+    return x + 1.0e6 if x < -1.0e-7 else x
+
+
+def _box_order(hv: np.ndarray) -> list[int]:
+    """Indices in the order of a periodic box: by z, then y, then x, each component >= 0 increasing before the negative
+    values increasing (a stable sort with a tolerance)."""
+    import functools
+
+    def cmp(a, b):
+        for c in (2, 1, 0):
+            ka, kb = _box_key(hv[c, a]), _box_key(hv[c, b])
+            if ka < kb - 1.0e-7:
+                return -1
+            if ka > kb + 1.0e-7:
+                return 1
+        return 0
+    return sorted(range(hv.shape[1]), key=functools.cmp_to_key(cmp))
+
+
+def epi_pair_list_c(disp: np.ndarray, perm: np.ndarray, rot: np.ndarray, cls, nshell: int) -> list[EpiPair]:
+    """``epi_pair_list`` on a site cluster (``crystal.crystal_graph`` + ``graph_site_ops``): disp (3, n) displacements from
+    site 1 (alat units); members, orbits and ties follow the order of a periodic box.  A shell outside the cluster raises
+    ValueError."""
+    disp = np.asarray(disp, dtype=float)
+    perm = np.asarray(perm)
+    cls = np.asarray(cls, dtype=np.int64)
+    tol = 1e-9
+    n = disp.shape[1]
+    r2 = np.sum(disp * disp, axis=0)
+    h = np.rint(2.0 * disp).astype(np.int64)
+    shells, rcur = [], 0.0
+    for ish in range(1, nshell + 1):
+        above = r2 > rcur + tol
+        if not above.any():
+            raise ValueError(f"epi: shell {ish} lies outside the site cluster (raise the levels)")
+        rcur = float(np.min(r2[above]))
+        shells.append(rcur)
+    sub = np.nonzero(r2 <= rcur + tol)[0]
+    ordr = [int(sub[q]) for q in _box_order(2.0 * disp[:, sub])]
+    keep = [k for k in range(perm.shape[1]) if np.array_equal(cls[perm[:, k] - 1], cls)]
+    pairs, done = [], np.zeros(n, dtype=bool)
+    for ish, sh in enumerate(shells, start=1):
+        for i in ordr:
+            if i == 0 or abs(r2[i] - sh) > tol or done[i]:
+                continue
+            inorb = np.zeros(n, dtype=bool)
+            inorb[perm[i, keep] - 1] = True
+            done |= inorb
+            best, site = 0, -1
+            for j in ordr:
+                if not inorb[j]:
+                    continue
+                cl2 = cls.copy()
+                cl2[j] = cls.max() + 1
+                nop = len(epi_pair_ops_c(perm, rot, cl2))
+                if nop > best:
+                    best, site = nop, j
+            members = [j for j in ordr if inorb[j]]
+            pairs.append(EpiPair(shell=ish, site=site + 1, mult=int(inorb.sum()), r2=int(round(4.0 * sh)), cls2=int(cls[site]),
+                                 nop=best, vec=h[:, site].copy(), orbit=h[:, members].copy(), rvec=disp[:, site].copy(),
+                                 rorbit=disp[:, members].copy()))
+    return pairs
 
 
 def epi_blocks(op: AugclsOp, params, ed: dict, vec: np.ndarray, chi: np.ndarray, lo, z, nlev: int, tail: str = "hull",

@@ -67,3 +67,49 @@ def test_oracle_chain_trace_equals_the_exact_configuration_average(group):
             tr += EP.epi_integrand(pt, int(lo[ia]), Z, x)
         # epi_integrand leaves out the constant -2 kappa: it equals the exact trace plus 2 sum_L kappa_L
         assert abs(tr - ref) / abs(ref) < 1e-8, (sj, tr, ref)
+
+
+def test_pair_lists_on_periodic_cubic_cells():
+    """Part (G) of the reference's test: pair types, multiplicities, lengths, pair-group orders; a shell that does not fit
+    into the cell is refused; B2 partners on the other and the own sublattice."""
+    c = E.cell()
+    cls = np.ones(c["graph"].n, np.int64)
+    pairs = EP.epi_pair_list(c["coord"], E.MG, cls, 1)
+    assert len(pairs) == 1 and (pairs[0].mult, pairs[0].r2, pairs[0].nop) == (8, 3, 2)
+    with pytest.raises(ValueError, match="does not fit"):
+        EP.epi_pair_list(c["coord"], E.MG, cls, 2)
+    gf, cf = lat.periodic_graph("fcc", 2)
+    pairs = EP.epi_pair_list(cf, 4, np.ones(gf.n, np.int64), 1)
+    assert len(pairs) == 1 and (pairs[0].mult, pairs[0].nop) == (12, 4)
+    g3, c3 = lat.periodic_graph("bcc", 3)
+    pairs = EP.epi_pair_list(c3, 6, np.ones(g3.n, np.int64), 3)
+    assert [p.mult for p in pairs] == [8, 6, 12] and [p.r2 for p in pairs] == [3, 4, 8] and [p.nop for p in pairs] == [2, 4, 4]
+    pairs = EP.epi_pair_list(c3, 6, 1 + c3[0] % 2, 2)
+    assert [p.cls2 for p in pairs] == [2, 1]
+
+
+def test_pair_lists_on_site_clusters():
+    """hcp (ideal): two pair types in the first shell, 6 + 6 sites at distance a; NiAs from an anion: cations, then
+    out-of-plane and in-plane anions, 6 each, at the expected lengths; adapted vectors of the pair group orthonormal."""
+    from asr_b200 import crystal as X
+    s = X.prototype_structure("hcp")
+    ops = X.space_group(s)
+    cg = X.crystal_graph(s, ops, 1.1, 2, start=0)
+    perm, rot, _ = X.graph_site_ops(cg, s, ops)
+    pairs = EP.epi_pair_list_c(cg.disp, perm, rot, s.label[cg.basis], 1)
+    assert len(pairs) == 2 and [p.mult for p in pairs] == [6, 6]
+    assert max(abs(np.linalg.norm(p.rvec) - 1.0) for p in pairs) < 1e-10
+    s = X.prototype_structure("nias", 1.62)
+    ops = X.space_group(s)
+    cg = X.crystal_graph(s, ops, 1.1, 2, start=2)
+    perm, rot, _ = X.graph_site_ops(cg, s, ops)
+    cls = s.label[cg.basis].astype(np.int64)
+    pairs = EP.epi_pair_list_c(cg.disp, perm, rot, cls, 3)
+    assert len(pairs) == 3 and [p.cls2 for p in pairs] == [1, 2, 2] and [p.mult for p in pairs] == [6, 6, 6]
+    assert abs(np.linalg.norm(pairs[1].rvec) - np.sqrt(1.0 / 3.0 + (0.5 * 1.62) ** 2)) < 1e-10
+    assert abs(np.linalg.norm(pairs[2].rvec) - 1.0) < 1e-10
+    cls[pairs[1].site - 1] = 3
+    idx = EP.epi_pair_ops_c(perm, rot, cls)
+    pd = np.stack([X.orbital_matrix(rot[:, :, k]) for k in idx], axis=2)
+    vec, _, _ = EP.epi_adapted(pd)
+    assert np.max(np.abs(vec.T @ vec - np.eye(9))) < 1e-13
