@@ -5,6 +5,9 @@ Host-side restatement of the caller of ``edc_green_proj`` in the reference's ``a
 
 * ``spectral_kpath`` (:59-77), ``spectral_window`` (:175-188), ``spectral_unfold`` (:190-198), ``spectral_dressing``
   (:200-229) with ``augn_basis`` (src/asr_augcls.f90:73-91);
+* ``spectral_structure_ok`` / ``spectral_origin_classes`` (:83-148): every sublattice one space-group orbit, and the
+  basis sites grouped into origin classes by pure translations and inversions (with the sign of the mapping and the site
+  fraction of each class);
 * ``bloch_spectral`` -- one origin class (a Bravais sublattice whose sites are related by translations or inversion):
   the D2h-reduced operator with the target sites within rmax, one projected chain per (spin, central component, start
   orbital, energy) on the device (``chains_proj``), the averaged off-site elements <G_{0L, RL}> = sum_c x_c gp, the
@@ -18,8 +21,8 @@ import numpy as np
 
 from .chains import ChainSpec, chains_proj
 
-__all__ = ["spectral_kpath", "spectral_window", "spectral_unfold", "augn_basis", "spectral_dressing", "spectral_elements",
-           "spectral_sum", "bloch_spectral"]
+__all__ = ["spectral_kpath", "spectral_window", "spectral_unfold", "augn_basis", "spectral_dressing", "spectral_structure_ok",
+           "spectral_origin_classes", "spectral_elements", "spectral_sum", "bloch_spectral"]
 
 ORB_L = np.array([0, 1, 1, 1, 2, 2, 2, 2, 2])
 
@@ -100,6 +103,49 @@ def spectral_dressing(dc, dl, spc, conc, frozen: bool, nsm: int | None = None) -
         for j, s in enumerate(sup):
             tau[:, k] += conc[s] * np.sqrt(dc / dl[:, spc[s] - 1]) * phi[k, j]
     return tau
+
+
+def spectral_structure_ok(s) -> bool:
+    """True if every sublattice of the structure is a single orbit of its space group (labels kept): one set of
+    component potentials per sublattice needs every site of it equivalent to its first site."""
+    from .crystal import space_group
+    ops = space_group(s)
+    for kap in range(1, s.nlabel + 1):
+        sites = np.nonzero(s.label == kap)[0]
+        if sites.size == 0:
+            continue
+        b0 = int(sites[0])
+        reach = {int(o.perm[b0]) for o in ops}
+        if any(int(b) not in reach for b in sites):
+            return False
+    return True
+
+
+def spectral_origin_classes(s, ops=None):
+    """Basis sites grouped by pure translations (rot = +I) and inversions (rot = -I) of the space group, sublattice by
+    sublattice.  Returns bclass (nb, 1-based class), orig_b (1-based representative basis sites), orig_sign (nb: +1 when a
+    translation maps the site onto its representative, -1 when an inversion does) and orig_w (site fraction per class)."""
+    from .crystal import space_group
+    ops = space_group(s) if ops is None else ops
+    nb = s.nb
+    bclass = np.zeros(nb, dtype=np.int64)
+    sign = np.ones(nb, dtype=np.int64)
+    orig = []
+    eye = np.eye(3)
+    for kap in range(1, s.nlabel + 1):
+        for b in range(nb):
+            if s.label[b] != kap or bclass[b]:
+                continue
+            orig.append(b + 1)
+            bclass[b] = len(orig)
+            for want, sg in ((eye, 1), (-eye, -1)):
+                for b2 in range(b + 1, nb):
+                    if s.label[b2] != kap or bclass[b2]:
+                        continue
+                    if any(o.perm[b2] == b and np.max(np.abs(o.rot - want)) < 1e-7 for o in ops):
+                        bclass[b2], sign[b2] = len(orig), sg
+    w = np.array([np.sum(bclass == g) / nb for g in range(1, len(orig) + 1)])
+    return bclass, np.array(orig, dtype=np.int64), sign, w
 
 
 def spectral_elements(op, tnode, tgop, t0: int, comps, conc, eds, z, nsteps: int, tail: str = "hull", precision: str = "fp64",

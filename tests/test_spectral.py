@@ -128,3 +128,30 @@ def test_projections_in_three_bases(readout, nlev, tol_abs, tol_origin):
             tr = int(np.nonzero(np.all(np.abs(td - pd[:, None]) < 1e-9, axis=0))[0][0])
             erot = max(erot, abs(gp[4][3, t] - gp[3][2, tr]))
         assert erot < 1e-11
+
+
+def test_structure_and_origin_classes():
+    """The reference's checks of spectral_structure_ok and spectral_origin_classes: fcc one origin of weight 1; B2 and
+    hcp accepted, hcp's two sites one origin (inversion, signs +1, -1); NiAs: the cations in two origins, the anions in
+    one, weights 1/4, 1/4, 1/2; L1_2: four origins (corner and three faces) of weight 1/4; a sublattice that merges
+    inequivalent sites is refused."""
+    from asr_b200 import crystal as X
+    s = X.prototype_structure("fcc")
+    assert SP.spectral_structure_ok(s)
+    bcl, ob, osg, ow = SP.spectral_origin_classes(s)
+    assert list(ob) == [1] and abs(ow[0] - 1.0) < 1e-14
+    assert SP.spectral_structure_ok(X.prototype_structure("b2"))
+    s = X.prototype_structure("hcp")
+    assert SP.spectral_structure_ok(s)
+    bcl, ob, osg, ow = SP.spectral_origin_classes(s)
+    assert len(ob) == 1 and list(osg) == [1, -1] and abs(ow[0] - 1.0) < 1e-14
+    s = X.prototype_structure("nias", 1.62)
+    assert SP.spectral_structure_ok(s)
+    bcl, ob, osg, ow = SP.spectral_origin_classes(s)
+    assert list(ob) == [1, 2, 3] and list(osg) == [1, 1, 1, -1] and np.max(np.abs(ow - [0.25, 0.25, 0.5])) < 1e-14
+    l12 = X.Structure(np.eye(3), np.array([[0, 0.5, 0.5, 0], [0, 0.5, 0, 0.5], [0, 0, 0.5, 0.5]]), [1, 2, 2, 2])
+    assert SP.spectral_structure_ok(l12)
+    bcl, ob, osg, ow = SP.spectral_origin_classes(l12)
+    assert len(ob) == 4 and np.max(np.abs(ow - 0.25)) < 1e-14
+    bad = X.Structure(np.diag([1.0, 1.0, 2.0]), np.array([[0, 0, 0], [0, 0, 0], [0, 0.2, 0.5]]), [1, 1, 1])
+    assert not SP.spectral_structure_ok(bad)
