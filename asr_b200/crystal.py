@@ -17,7 +17,10 @@ Host-side restatement of the set-up that feeds ``build_augcls_operator`` in the 
   then x, y, z, neighbour entries 0 (no such bond) and -1 (outside the ball), and the site operations in canonical
   order (monomial first, by axis permutation and row signs);
 * ``sublattice_inputs`` -- the per-sublattice block of class_scf: flippable sites, classes, the class-preserving site
-  group, its orbital groups and reduction group, giving (graph, cls, perm, dmat, flippable, start orbitals, weights).
+  group, its orbital groups and reduction group, giving (graph, cls, perm, dmat, flippable, start orbitals, weights);
+* ``decoration_build`` / ``decoration_classes`` / ``decoration_structure`` -- src/asr_sublattice.f90:26-116: sublattices
+  given by Wyckoff positions of a decoration cell of ``period`` conventional cubes of an sc / bcc / fcc graph with a
+  centering (P, I, F), as classes of graph sites or as a crystal structure.
 
 Everything here runs once per set-up on the host (integer and small dense work); the device build consumes its output.
 """
@@ -32,7 +35,8 @@ from .lattices import Graph, orbital_rep
 
 __all__ = ["Structure", "prototype_structure", "SymOp", "space_group", "site_ops", "basis_orbits", "translation_types",
            "is_monomial", "orbital_matrix", "orbital_groups", "reduction_ops", "CrystalGraph", "crystal_graph", "graph_site",
-           "graph_site_ops", "structure_cluster", "graph_distances", "sublattice_inputs", "GEO_TOL", "RTOL"]
+           "graph_site_ops", "structure_cluster", "graph_distances", "sublattice_inputs", "Decoration", "decoration_build",
+           "decoration_classes", "decoration_structure", "GEO_TOL", "RTOL"]
 
 GEO_TOL = 1.0e-6     # fractional-coordinate tolerance (src/asr_crystal.f90:13)
 RTOL = 1.0e-9        # distance tolerance in alat units (src/asr_crystal_graph.f90:36)
@@ -561,3 +565,95 @@ def sublattice_inputs(s: Structure, ops: list[SymOp], kap: int, rcl: float, leve
     return dict(cg=cg, graph=cg.g, cls=cls, flippable=flip, stype=typ[cg.basis].astype(np.int32),
                 perm=np.asfortranarray(perm[:, [keep[r] for r in red]]), dmat=np.asfortranarray(dgo[:, :, red]),
                 site_group=len(keep), orbital_group=grp, reps=rep, weights=wgt, maxlevel=levels)
+
+
+# --------------------------------------------------------------------------------------------------------- decorations
+def _on_graph(kind: str, h) -> bool:
+    h = np.asarray(h, dtype=np.int64)
+    if kind == "sc":
+        return bool(np.all(h % 2 == 0))
+    if kind == "bcc":
+        return bool(h[0] % 2 == h[1] % 2 == h[2] % 2)
+    if kind == "fcc":
+        return bool(int(np.sum(h)) % 2 == 0)
+    return False
+
+
+@dataclass
+class Decoration:
+    """Sublattices of an sc / bcc / fcc graph in a cell of ``period`` conventional cubes (edge m = 2 period half-lattice
+    units): ``tab`` (m, m, m) the sublattice of every graph point of the cell (0: not a site), ``pts`` (3, nsite) the sites
+    in the order z, y, x (x fastest), ``pcls`` their sublattices, ``rep`` (3, ncls) the first site of each, ``frac`` the
+    site fractions."""
+    lattice: str
+    period: int
+    m: int
+    ncls: int
+    tab: np.ndarray
+    pts: np.ndarray
+    pcls: np.ndarray
+    rep: np.ndarray
+    frac: np.ndarray
+
+
+def decoration_build(lattice: str, period: int, centering: str, pos, owner, ncls: int) -> Decoration:
+    """Sublattices from Wyckoff positions pos (3, k) (fractions of the decoration cell) with owners (k, 1-based) and the
+    centering translations P, I or F.  Every graph site of the cell must belong to exactly one sublattice (ValueError)."""
+    tr = {"P": [[0, 0, 0]], "I": [[0, 0, 0], [0.5, 0.5, 0.5]],
+          "F": [[0, 0, 0], [0, 0.5, 0.5], [0.5, 0, 0.5], [0.5, 0.5, 0]]}.get(centering)
+    if tr is None:
+        raise ValueError("centering must be 'P', 'I' or 'F'")
+    m = 2 * period
+    pos = np.asarray(pos, dtype=float).reshape(3, -1)
+    owner = np.asarray(owner, dtype=np.int64)
+    tab = np.zeros((m, m, m), dtype=np.int64)
+    for k in range(pos.shape[1]):
+        for t in tr:
+            f = np.mod(pos[:, k] + np.asarray(t, float), 1.0) * m
+            h = np.mod(np.rint(f).astype(np.int64), m)
+            if np.max(np.abs(f - np.rint(f))) > 1e-6 or not _on_graph(lattice, h):
+                raise ValueError("a sublattice position is not a site of the graph lattice")
+            if tab[h[0], h[1], h[2]] not in (0, owner[k]):
+                raise ValueError("two sublattices share a site")
+            tab[h[0], h[1], h[2]] = owner[k]
+    pts, pcls = [], []
+    for l in range(m):
+        for j in range(m):
+            for i in range(m):
+                if not _on_graph(lattice, (i, j, l)):
+                    continue
+                if tab[i, j, l] == 0:
+                    raise ValueError("a site of the decoration cell belongs to no sublattice")
+                pts.append((i, j, l))
+                pcls.append(int(tab[i, j, l]))
+    pts = np.array(pts, dtype=np.int64).T
+    pcls = np.array(pcls, dtype=np.int64)
+    rep = -np.ones((3, ncls), dtype=np.int64)
+    frac = np.zeros(ncls)
+    for q in range(pts.shape[1]):
+        c = pcls[q] - 1
+        if rep[0, c] < 0:
+            rep[:, c] = pts[:, q]
+        frac[c] += 1.0
+    if np.any(frac == 0.0):
+        raise ValueError("a sublattice has no site")
+    return Decoration(lattice=lattice, period=period, m=m, ncls=ncls, tab=tab, pts=pts, pcls=pcls, rep=rep,
+                      frac=frac / pts.shape[1])
+
+
+def decoration_classes(dec: Decoration, coord: np.ndarray, mg: int, origin: int) -> np.ndarray:
+    """Classes (1-based) of the graph sites coord (3, n) of a periodic supercell of edge mg half-lattice units, with the
+    representative site of sublattice ``origin`` (1-based) moved to the graph origin."""
+    if mg % dec.m:
+        raise ValueError("decoration_classes: the supercell is not a multiple of the decoration cell")
+    h = np.mod(np.asarray(coord, dtype=np.int64) + dec.rep[:, origin - 1][:, None], dec.m)
+    cls = dec.tab[h[0], h[1], h[2]]
+    if np.any(cls == 0):
+        raise ValueError("decoration_classes: graph site outside the decoration")
+    return cls.astype(np.int32)
+
+
+def decoration_structure(dec: Decoration) -> Structure:
+    """The decoration as a crystal structure: the cell of ``period`` cubes (alat units), every graph site of the cell a
+    basis site in the order of ``pts``, labelled by its sublattice."""
+    return Structure(np.eye(3) * dec.period, dec.pts.astype(float) / dec.m, dec.pcls)

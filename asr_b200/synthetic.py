@@ -379,27 +379,26 @@ def structure_blocks(bvec: np.ndarray, seed: int, ntype: int = 1):
     return block, block0
 
 
-# the reference examples as structures (primitive cells in units of the bcc / fcc cube edge, labels per sublattice);
-# species per class and concentrations as in EXAMPLES
-STRUCTURE_EXAMPLES = {
-    "cuzn_alloy": ("bcc", None, 4),
-    "fe66ni14cr20_fcc": ("fcc", None, 3),
-    "cuzn_b2": ("b2", None, 4),
-    # L2_1 with a = 2 a_bcc: fcc primitive cell of cube edge 2; 8c at (1/4, 1/4, 1/4) and (3/4, 3/4, 3/4) of the
-    # conventional cube (label 1), 4a at the origin (label 2), 4b at (1/2, 1/2, 1/2) (label 3)
-    "co2fe04cr06al_l21": ("l21", None, 4),
+# the structures of the reference examples as their inputs give them: graph lattice, period of the decoration cell in
+# conventional cubes, centering, and the Wyckoff positions (fractions of the decoration cell) of each sublattice, in the
+# order of the examples' sublattices; with the recursion levels of each example
+EXAMPLE_DECORATIONS = {
+    "cuzn_alloy": ("bcc", 1, "I", [[(0.0, 0.0, 0.0)]], 4),
+    "fe66ni14cr20_fcc": ("fcc", 1, "F", [[(0.0, 0.0, 0.0)]], 3),
+    "cuzn_b2": ("bcc", 1, "P", [[(0.0, 0.0, 0.0)], [(0.5, 0.5, 0.5)]], 4),
+    "co2fe04cr06al_l21": ("bcc", 2, "F", [[(0.25, 0.25, 0.25), (0.75, 0.75, 0.75)], [(0.0, 0.0, 0.0)], [(0.5, 0.5, 0.5)]], 4),
 }
 
 
 def example_structure(name: str):
-    """The Structure of reference example ``name``."""
+    """The Structure of reference example ``name``: its decoration cell (``crystal.decoration_build``) as the cell, every
+    graph site of the cell a basis site labelled by its sublattice."""
     from . import crystal as X
-    kind = STRUCTURE_EXAMPLES[name][0]
-    if kind != "l21":
-        return X.prototype_structure(kind)
-    avec = np.array([[0.0, 1.0, 1.0], [1.0, 0.0, 1.0], [1.0, 1.0, 0.0]])
-    cart = np.array([[0.5, 0.5, 0.5], [1.5, 1.5, 1.5], [0.0, 0.0, 0.0], [1.0, 1.0, 1.0]]).T
-    return X.Structure(avec, X.inv3(avec) @ cart, [1, 1, 2, 3])
+    lattice, period, centering, subl, _ = EXAMPLE_DECORATIONS[name]
+    pos = np.array([p for sl in subl for p in sl], dtype=float).T
+    owner = [k + 1 for k, sl in enumerate(subl) for _ in sl]
+    dec = X.decoration_build(lattice, period, centering, pos, owner, len(subl))
+    return X.decoration_structure(dec)
 
 
 def structure_case(name: str, sublattice: int = 1, seed: int = 0, rcl: float = 1.2, levels: int | None = None,
@@ -408,7 +407,7 @@ def structure_case(name: str, sublattice: int = 1, seed: int = 0, rcl: float = 1
     ball about the start site, the class-preserving site group, its start orbitals and weights, and the reduction group.
     Returns the keys of ``example_case`` plus reps, weights, stype and the crystal graph."""
     from . import crystal as X
-    _, _, lev = STRUCTURE_EXAMPLES[name]
+    lev = EXAMPLE_DECORATIONS[name][4]
     levels = lev if levels is None else levels
     spcs, concs = EXAMPLES[name][4], EXAMPLES[name][5]
     s = example_structure(name)

@@ -217,15 +217,46 @@ def test_rmin_and_levels_zero():
 
 
 def test_sublattice_inputs_of_the_l21_cell():
-    """The L2_1 cell from its structure: the 8c site group is T_d (24 operations, class-preserving), the 4a and 4b site
+    """The L2_1 cell from its decoration: the 8c site group is T_d (24 operations, class-preserving), the 4a and 4b site
     groups O_h (48); four start orbitals s, p_z, d_xy, d_3z2 with weights 1, 3, 3, 2 on each, reduction groups of
     order 8 (8c) and 16 (4a, 4b)."""
     from asr_b200 import synthetic as S
     s = S.example_structure("co2fe04cr06al_l21")
     ops = X.space_group(s)
-    assert len(ops) == 48           # Fm-3m on the primitive cell: the centring translations are lattice vectors
+    assert s.nb == 16               # the decoration cell of the example: 2^3 conventional bcc cubes, 16 sites
+    assert len(ops) == 48 * 4       # Fm-3m on that cell: 48 point operations x 4 centring translations
     for kap, nsite, nred in ((1, 24, 8), (2, 48, 16), (3, 48, 16)):
         inp = X.sublattice_inputs(s, ops, kap, 1.2, 1)
         assert inp["site_group"] == nsite and inp["perm"].shape[1] == nred
         assert list(inp["reps"]) == [1, 3, 5, 7] and list(inp["weights"]) == [1, 3, 3, 2]
         assert inp["cls"][0] == kap and inp["flippable"][0] == 0
+
+
+def test_decorations():
+    """Decoration cells (src/asr_sublattice.f90:39-116): the L2_1 cell of its example (16 sites, fractions 1/2, 1/4, 1/4),
+    classes of a periodic supercell with the origin moved to a sublattice, and the input errors."""
+    d = X.decoration_build("bcc", 2, "F", np.array([[0.25, 0.75, 0.0, 0.5]] * 3), [1, 1, 2, 3], 3)
+    assert d.pts.shape[1] == 16 and np.allclose(d.frac, [0.5, 0.25, 0.25])
+    g, coord, _ = lat.periodic_graph_shells("bcc", 4, 4)
+    for origin in (1, 2, 3):
+        cls = X.decoration_classes(d, coord, 8, origin)
+        assert cls[0] == origin and np.allclose(np.bincount(cls)[1:] / cls.size, d.frac)
+    with pytest.raises(ValueError, match="share a site"):
+        X.decoration_build("bcc", 1, "P", np.array([[0.0, 0.0], [0.0, 0.0], [0.0, 0.0]]), [1, 2], 2)
+    with pytest.raises(ValueError, match="no sublattice"):
+        X.decoration_build("bcc", 1, "P", np.zeros((3, 1)), [1], 1)
+    with pytest.raises(ValueError, match="centering"):
+        X.decoration_build("bcc", 1, "C", np.zeros((3, 1)), [1], 1)
+
+
+@pytest.mark.parametrize("kind,sub", [("bcc", 1), ("fcc", 1)])
+def test_decoration_and_primitive_cells_give_the_same_operator_inputs(kind, sub):
+    """A sublattice's operator inputs do not depend on the cell the structure is written in: the conventional cube with
+    its centring sites and the primitive cell give the same ball, classes, group and start orbitals."""
+    d = X.decoration_build(kind, 1, "I" if kind == "bcc" else "F", np.zeros((3, 1)), [1], 1)
+    sd, sp = X.decoration_structure(d), X.prototype_structure(kind)
+    a = X.sublattice_inputs(sd, X.space_group(sd), sub, 1.2, 2)
+    b = X.sublattice_inputs(sp, X.space_group(sp), sub, 1.2, 2)
+    for k in ("cls", "perm", "dmat", "flippable", "stype", "reps", "weights"):
+        assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+    assert np.array_equal(a["graph"].nbr, b["graph"].nbr)
