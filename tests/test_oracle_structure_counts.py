@@ -65,3 +65,44 @@ def test_representatives_carry_their_orbital_groups(name, sub):
         ad, bd = coef["diag", l0]
         assert len(ar) == len(ad) == depth
         assert np.max(np.abs(ar - ad)) < 1e-9 * np.max(np.abs(ar)) and np.max(np.abs(br[:-1] - bd[:-1])) < 1e-9 * np.max(np.abs(br))
+
+
+def test_ball_and_periodic_box_give_the_same_chains():
+    """The ball about the start site and an unwrapped periodic box give the same recursion (the reference's cluster vs
+    box check): plain chains from s, p_z, d_3z2 on the B2 sublattice a, 8 levels, coefficients to 1e-10 (deeper levels
+    differ by the rounding that the two node orders amplify in a chain without reorthogonalisation)."""
+    ball = S.structure_case("cuzn_b2", 1)
+    box = S.example_case("cuzn_b2", 1, l=16)
+    c, d, o, e = S.plain_params(S.draw_species(2, 7))
+    ops = []
+    for case in (ball, box):
+        op = _oracle(case)
+        op.set_params(c, d, o, e)
+        ops.append(op)
+    assert ops[0].nn == ops[1].nn
+    for l0 in (1, 3, 7):
+        coef = []
+        for op in ops:
+            op.set_start(l0)
+            v0 = np.zeros(op.dim)
+            v0[l0 - 1] = 1.0
+            a, b, n = op.lanczos(v0, 8)
+            coef.append((a[:n], b[:n]))
+        assert np.max(np.abs(coef[0][0] - coef[1][0])) < 1e-10 and np.max(np.abs(coef[0][1] - coef[1][1])) < 1e-10
+
+
+def test_chain_greens_is_independent_of_the_thread_count():
+    """The oracle's task-parallel chain_greens gives bit-identical Green functions with 1 and 4 threads (the reference's
+    thread-count test)."""
+    case = S.structure_case("cuzn_b2", 2)
+    op = _oracle(case)
+    sp = S.draw_species(2, 3)
+    groups = []
+    for cen in (1, 2):
+        ed = S.edc_params(sp, cen)
+        groups.append(dict(c=ed["c"], d=ed["d"], o=ed["o"], e=ed["e"], dc=ed["dc"], dl=ed["dl"], enu=ed["enu"]))
+    z = np.linspace(-0.8, 0.4, 12) + 0.05j
+    nlev = np.full((2, 2), 16, np.int32)
+    g1, _ = op.chain_greens(groups, [0, 0], [1, 3], nlev, z, 4, nthreads=1)
+    g4, _ = op.chain_greens(groups, [0, 0], [1, 3], nlev, z, 4, nthreads=4)
+    assert np.array_equal(g1, g4)
