@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <climits>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "op.h"
@@ -426,7 +427,9 @@ __global__ void k_perm_rows(int nn, int w, const int* old_of_new, const int* new
   if (q >= (long)nn * w) return;
   int n = (int)(q / w), k = (int)(q % w);
   T v = in[(size_t)old_of_new[n] * w + k];
-  if (remap && v >= 0) v = (T)new_of_old[(int)v];
+  if constexpr (std::is_signed<T>::value) {   // node indices (signed, -1: none) are renumbered; flags are copied
+    if (remap && v >= 0) v = (T)new_of_old[(int)v];
+  }
   out[q] = v;
 }
 
