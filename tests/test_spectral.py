@@ -155,3 +155,47 @@ def test_structure_and_origin_classes():
     assert len(ob) == 4 and np.max(np.abs(ow - 0.25)) < 1e-14
     bad = X.Structure(np.diag([1.0, 1.0, 2.0]), np.array([[0, 0, 0], [0, 0, 0], [0, 0.2, 0.5]]), [1, 1, 1])
     assert not SP.spectral_structure_ok(bad)
+
+
+def test_unfolded_projections_give_the_band_structure():
+    """An ordered bcc crystal on the 16-site periodic cell (one species, unreduced): the projected chains of the oracle
+    (edc_green_proj, tail none, closed) give every off-site element <G_{0L,RL}>, and their Bloch sum at the commensurate
+    wavevectors equals -Im tr_l (z - H(k))^-1 / pi of the dense H(k) (1e-9)."""
+    from asr_b200 import lattices as lat
+    from asr_b200 import synthetic as S
+    case = S.cubic_case("bcc", 2, 1, [1.0], seed=5, group="identity")
+    g, coord = case["graph"], case["coord"]
+    n = g.n
+    tsite = np.arange(1, n + 1, dtype=np.int32)
+    fl = np.zeros(n, np.int32)
+    op = OracleOp(g, case["model"], case["cls"], case["perm"], case["dmat"], 1, 6, 0, fl, tsite=tsite)
+    assert op.nn == n
+    ed = S.edc_params(S.draw_species(1, 5), 1)
+    op.set_params(ed["c"], ed["d"], ed["o"], ed["e"])
+    dim = 9 * n
+    h = np.zeros((dim, dim))
+    for k in range(dim):
+        x = np.zeros(dim)
+        x[k] = 1.0
+        h[:, k] = op.apply(x)
+    disp = 0.5 * ((coord + 2) % 4 - 2).astype(float)     # minimum-image displacements (alat)
+    tw = np.zeros((9, 1, n))
+    tw[:, 0, :] = 1.0
+    z = 0.15 + 0.1j
+    gdg = np.zeros((9, n), np.complex128)
+    for l0 in range(1, 10):
+        op.set_start(l0)
+        _, gp, _, m = op.edc_green_proj(ed, z, l0, 200, op.tnode, op.tgop, tw, tail="none")
+        gdg[l0 - 1] = gp[l0 - 1]
+    ks = [np.array(v) / 2.0 for v in ((0, 0, 0), (1, 0, 0), (1, 1, 0), (1, 1, 1), (0, 0, 1))]
+    orb_l = S.ORB_L
+    site = op.tables()["site"]                          # the dense H is in node order; node j sits on site site[j]
+    for k in ks:
+        ph = np.exp(2j * np.pi * (k @ disp))
+        hk = sum(ph[site[j] - 1] * h[0:9, 9 * j:9 * j + 9] for j in range(n))
+        gk = np.linalg.inv(z * np.eye(9) - hk)
+        for l in range(3):
+            exact = -np.imag(np.trace(gk[np.ix_(orb_l == l, orb_l == l)])) / np.pi
+            v = -np.imag(np.sum(gdg[orb_l == l], axis=0)) / np.pi
+            unf = SP.spectral_unfold(disp, v, k)
+            assert abs(unf - exact) < 1e-9 * max(1.0, abs(exact)), (k, l, unf, exact)
