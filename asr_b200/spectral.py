@@ -8,6 +8,9 @@ Host-side restatement of the caller of ``edc_green_proj`` in the reference's ``a
 * ``spectral_structure_ok`` / ``spectral_origin_classes`` (:83-148): every sublattice one space-group orbit, and the
   basis sites grouped into origin classes by pure translations and inversions (with the sign of the mapping and the site
   fraction of each class);
+* ``spectral_sum_origins`` -- the Bloch sum over several origin classes (src/asr_class_scf.f90:1566-1590, 1690-1745):
+  the partner of every target in the origin class of the target's own basis site (at -R, or +R through an inversion),
+  the average with it, and the windowed sums weighted by the site fractions of the origin classes;
 * ``bloch_spectral`` -- one origin class (a Bravais sublattice whose sites are related by translations or inversion):
   the D2h-reduced operator with the target sites within rmax, one projected chain per (spin, central component, start
   orbital, energy) on the device (``chains_proj``), the averaged off-site elements <G_{0L, RL}> = sum_c x_c gp, the
@@ -22,7 +25,7 @@ import numpy as np
 from .chains import ChainSpec, chains_proj
 
 __all__ = ["spectral_kpath", "spectral_window", "spectral_unfold", "augn_basis", "spectral_dressing", "spectral_structure_ok",
-           "spectral_origin_classes", "spectral_elements", "spectral_sum", "bloch_spectral"]
+           "spectral_origin_classes", "spectral_elements", "spectral_sum", "spectral_sum_origins", "bloch_spectral"]
 
 ORB_L = np.array([0, 1, 1, 1, 2, 2, 2, 2, 2])
 
@@ -196,6 +199,47 @@ def spectral_sum(gdg, tdisp, kv, rmax: float, window: str = "ball"):
         v = -np.imag(np.sum(gsym[ORB_L == l], axis=0)) / np.pi                # (nt, ne)
         A[:, :, l] = (phase @ (v * w[:, None])).T
     return A, gsym
+
+
+def spectral_sum_origins(gdg: list, tdisp: list, tbase: list, tsign: list, orig_w, kv, rmax: float, window: str = "ball"):
+    """A(k, E) summed over origin classes u with weights orig_w[u] (spectral_final, src/asr_class_scf.f90:1588-1601
+    partners, :1693-1701 symmetrisation, :1725-1746 the weighted Bloch sum).  gdg[u] (9, nt_u, ne) are the elements of
+    origin u, tdisp[u] (3, nt_u) the target displacements (alat), tbase[u] (nt_u, 0-based) the origin class of each
+    target's basis site and tsign[u] (nt_u) the sign of the operation that maps that site onto its class representative.
+    The partner of target t of origin u is the target j of origin u2 = tbase[u][t] with tbase[u2][j] == u and
+    tdisp[u2][:, j] = -tsign[u][t] tdisp[u][:, t]; without one it is target t of origin u2.  Every element whose partner is
+    not itself is averaged with it.  Returns (A (ne, nk, 3) per orbital l, parts (norig, ne, nk) the part of each origin
+    summed over l, the symmetrised elements)."""
+    nor = len(gdg)
+    mir = []
+    for u in range(nor):
+        mu = []
+        for t in range(tdisp[u].shape[1]):
+            u2 = int(tbase[u][t])
+            hit = [j for j in range(tdisp[u2].shape[1]) if int(tbase[u2][j]) == u
+                   and np.max(np.abs(tdisp[u2][:, j] + tsign[u][t] * tdisp[u][:, t])) < 1e-9]
+            mu.append((u2, hit[0] if hit else t))
+        mir.append(mu)
+    sym = []
+    for u in range(nor):
+        g = np.array(gdg[u], copy=True)
+        for t, (u2, j) in enumerate(mir[u]):
+            if (u2, j) != (u, t):
+                g[:, t] = 0.5 * (gdg[u][:, t] + gdg[u2][:, j])
+        sym.append(g)
+    kv = np.asarray(kv, dtype=float).reshape(3, -1)
+    ne = sym[0].shape[2]
+    A = np.zeros((ne, kv.shape[1], 3))
+    parts = np.zeros((nor, ne, kv.shape[1]))
+    for u in range(nor):
+        w = np.array([spectral_window(window, float(np.linalg.norm(tdisp[u][:, t])), rmax) for t in range(tdisp[u].shape[1])])
+        phase = np.cos(2.0 * np.pi * (kv.T @ tdisp[u]))
+        for l in range(3):
+            v = -np.imag(np.sum(sym[u][ORB_L == l], axis=0)) / np.pi
+            a = orig_w[u] * (phase @ (v * w[:, None])).T
+            A[:, :, l] += a
+            parts[u] += a
+    return A, parts, sym
 
 
 def bloch_spectral(op, tnode, tgop, tdisp, t0: int, comps, conc, eds, z, kv, nsteps: int, rmax: float, window: str = "ball",

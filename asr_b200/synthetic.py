@@ -339,9 +339,8 @@ def example_case(name: str, sublattice: int = 1, seed: int = 0, l: int | None = 
     g, coord, bvec = lat.periodic_graph_shells(kind, l, 4)
     cname = cnames[sublattice - 1]
     cls = _example_classes(cname, coord, _EXAMPLE_SHIFT[cname])
-    if cname.startswith("b2"):
-        # classes of the example: 1 = sublattice a, 2 = sublattice b; with the shift, site 1 carries the start class
-        cls = np.where(cls == 1, sublattice, 3 - sublattice).astype(np.int32)
+    # the shift puts site 1 on the start sublattice; the classes keep the example's labels (B2: 1 = cube corners a,
+    # 2 = cube centres b)
     perm, mats = lat.class_ops(coord, 2 * l, cls)
     dmat = lat.orbital_rep(mats)
     block, block0 = sk_blocks(bvec, seed)

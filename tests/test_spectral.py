@@ -199,3 +199,59 @@ def test_unfolded_projections_give_the_band_structure():
             v = -np.imag(np.sum(gdg[orb_l == l], axis=0)) / np.pi
             unf = SP.spectral_unfold(disp, v, k)
             assert abs(unf - exact) < 1e-9 * max(1.0, abs(exact)), (k, l, unf, exact)
+
+
+def test_multi_origin_sum_on_an_ordered_b2_crystal():
+    """Two origin classes (the two sublattices of an ordered B2 crystal on the 16-site periodic cell, species with equal
+    Delta and d and different c): the projected elements of each origin's operator, the partner average and the
+    weighted Bloch sum equal (1/N) sum_ij cos(2 pi k.(r_j - r_i)) (-Im G_ij / pi) of the dense G at commensurate k."""
+    from asr_b200 import lattices as lat
+    from asr_b200 import synthetic as S
+    sp = S.draw_species(2, 12)
+    sp.d[1] = sp.d[0]
+    sp.delta[1] = sp.delta[0]
+    z = 0.1 + 0.12j
+    gdg, tdisp, tbase, tsign, dense = [], [], [], [], None
+    for u in (1, 2):
+        case = S.example_case("cuzn_b2", u, l=2)
+        g, coord, cls = case["graph"], case["coord"], case["cls"]
+        n = g.n
+        perm, dmat = lat.identity_group(n)
+        op = OracleOp(g, case["model"], cls, perm, dmat, 1, 6, 0, np.zeros(n, np.int32), tsite=np.arange(1, n + 1, dtype=np.int32))
+        ed = S.edc_params(sp, u)
+        op.set_params(ed["c"], ed["d"], ed["o"], ed["e"])
+        op.freeze_site(1, u)
+        tw = np.zeros((9, 1, n))
+        tw[:, 0, :] = 1.0
+        gu = np.zeros((9, n, 1), np.complex128)
+        for l0 in range(1, 10):
+            op.set_start(l0)
+            _, gp, _, _ = op.edc_green_proj(ed, z, l0, 200, op.tnode, op.tgop, tw, tail="none")
+            gu[l0 - 1, :, 0] = gp[l0 - 1]
+        gdg.append(gu)
+        tdisp.append(0.5 * ((coord + 2) % 4 - 2).astype(float))
+        tbase.append(np.asarray(cls) - 1)
+        tsign.append(np.ones(n))
+        if u == 1:                                        # the dense G of the whole cell, in site order
+            dim = 9 * n
+            h = np.zeros((dim, dim))
+            for k in range(dim):
+                x = np.zeros(dim)
+                x[k] = 1.0
+                h[:, k] = op.apply(x)
+            site = op.tables()["site"] - 1
+            pidx = np.concatenate([9 * np.argsort(site)[s_] + np.arange(9) for s_ in range(n)])
+            gd = np.linalg.inv(z * np.eye(dim) - h)[np.ix_(pidx, pidx)]
+            dense = (gd, 0.5 * coord.astype(float), n)
+    ks = np.array([[0, 0, 0], [0.5, 0, 0], [0.5, 0.5, 0], [0.5, 0.5, 0.5]]).T
+    A, parts, _ = SP.spectral_sum_origins(gdg, tdisp, tbase, tsign, [0.5, 0.5], ks, 2.0, "sharp")
+    assert np.allclose(parts.sum(axis=0), A.sum(axis=2), rtol=0, atol=1e-13)
+    gd, r, n = dense
+    orb_l = S.ORB_L
+    for q in range(ks.shape[1]):
+        k = ks[:, q]
+        c = np.cos(2 * np.pi * (k @ (r[:, None, :] - r[:, :, None]).reshape(3, -1))).reshape(n, n)
+        for l in range(3):
+            v = sum(-np.imag(gd[o::9, o::9]) / np.pi for o in np.nonzero(orb_l == l)[0])
+            exact = float(np.sum(c * v)) / n
+            assert abs(A[0, q, l] - exact) < 1e-9 * max(1.0, abs(exact)), (k, l, A[0, q, l], exact)
