@@ -331,8 +331,9 @@ def _example_classes(kind: str, coord: np.ndarray, shift) -> np.ndarray:
 
 
 def example_case(name: str, sublattice: int = 1, seed: int = 0, l: int | None = None):
-    """Operator inputs of the reference example ``name`` with the start site on ``sublattice`` (1-based), the classes
-    relabelled so that the class list is that of the example; returns the case dict of ``cubic_case`` plus maxlevel.
+    """Operator inputs of the reference example ``name`` with the start site on ``sublattice`` (1-based): the cluster is
+    shifted so that site 1 lies on that sublattice and every site keeps the class of its sublattice in the example's
+    class list; returns the case dict of ``cubic_case`` plus maxlevel.
     ``l`` overrides the periodic cluster (the examples' own: the supercell their published runs used)."""
     kind, l0, levels, cnames, spcs, concs = EXAMPLES[name]
     l = l0 if l is None else l
