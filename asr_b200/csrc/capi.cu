@@ -910,20 +910,17 @@ int asr_chains_run(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int 
                    double depth_tol, int tail, int precision, int project, double* g, double* a, double* b, int* mused) {
   if (!ctx || !z || !g) { set_error("asr_chains_run: null argument"); return ASR_EINVAL; }
   ASR_TRY(set_device(ctx));
+  if (nz < 0 || ngroup < 1) { set_error("asr_chains_run: bad argument"); return ASR_EINVAL; }
   cudaStream_t s = ctx->stream;
-  const size_t ng = mode == ASR_MODE_EDC ? (size_t)nz * ngroup : (size_t)nz * ngroup;
-  double2 *d_z = nullptr, *d_g = nullptr;
-  ASR_CUDA(cudaMalloc(&d_z, std::max(nz, 1) * sizeof(double2)));
-  ASR_CUDA(cudaMalloc(&d_g, std::max<size_t>(ng, 1) * sizeof(double2)));
-  ASR_CUDA(cudaMemcpyAsync(d_z, z, nz * sizeof(double2), cudaMemcpyHostToDevice, s));
-  int rc = chains_common(ctx, op, groups, ngroup, d_z, nz, mode, depth_tol, tail, precision, project, d_g, a, b, mused);
-  if (rc == ASR_OK) {
-    cudaMemcpyAsync(g, d_g, ng * sizeof(double2), cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) { set_error("asr_chains_run: copy back failed"); rc = ASR_ECUDA; }
-  }
-  cudaFree(d_z);
-  cudaFree(d_g);
-  return rc;
+  const size_t ng = (size_t)nz * ngroup;
+  Dev<double2> d_z, d_g;   // freed on every return path
+  ASR_TRY(d_z.alloc(nz));
+  ASR_TRY(d_g.alloc(ng));
+  ASR_CUDA(cudaMemcpyAsync(d_z.p, z, nz * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_TRY(chains_common(ctx, op, groups, ngroup, d_z.p, nz, mode, depth_tol, tail, precision, project, d_g.p, a, b, mused));
+  ASR_CUDA(cudaMemcpyAsync(g, d_g.p, ng * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  return ASR_OK;
 }
 
 // edc_green_proj (src/asr_edc.f90:174-232) for every (group, energy): all nlev steps (no depth test), g (nz, ngroup),
