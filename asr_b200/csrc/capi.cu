@@ -610,14 +610,12 @@ static int chains_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups
     std::vector<int> lg(nlane);
     for (int q = 0; q < ngroup; ++q)
       for (int j = 0; j < nz; ++j) lg[(size_t)q * nz + j] = q;
-    double2* d_lz = nullptr;
-    ASR_CUDA(cudaMalloc(&d_lz, std::max(nlane, 1) * sizeof(double2)));
+    Dev<double2> d_lz;
+    ASR_TRY(d_lz.alloc(nlane));
     for (int q = 0; q < ngroup; ++q)
-      cudaMemcpyAsync(d_lz + (size_t)q * nz, d_z, nz * sizeof(double2), cudaMemcpyDeviceToDevice, s);
-    int rc = run_lanes(ctx, op, gi, blob, GL, lg, d_lz, nlane, opt, d_g, want_ab ? &ha : nullptr, want_ab ? &hb : nullptr, &hm,
-                       &nfall, &nsteps);
-    cudaFree(d_lz);
-    if (rc != ASR_OK) return rc;
+      ASR_CUDA(cudaMemcpyAsync(d_lz.p + (size_t)q * nz, d_z, nz * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+    ASR_TRY(run_lanes(ctx, op, gi, blob, GL, lg, d_lz.p, nlane, opt, d_g, want_ab ? &ha : nullptr, want_ab ? &hb : nullptr, &hm,
+                      &nfall, &nsteps));
     for (int L = 0; L < nlane; ++L) {
       if (mused) mused[L] = hm[L];
       for (int k = 0; k < nlevmax; ++k) {
@@ -631,12 +629,10 @@ static int chains_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups
     // plain: one real chain per group, then the terminated fraction at every energy
     std::vector<int> lg(ngroup);
     for (int q = 0; q < ngroup; ++q) lg[q] = q;
-    double2* d_lz = nullptr;
-    ASR_CUDA(cudaMalloc(&d_lz, ngroup * sizeof(double2)));
-    ASR_CUDA(cudaMemsetAsync(d_lz, 0, ngroup * sizeof(double2), s));
-    int rc = run_lanes(ctx, op, gi, blob, GL, lg, d_lz, ngroup, opt, nullptr, &ha, &hb, &hm, &nfall, &nsteps);
-    cudaFree(d_lz);
-    if (rc != ASR_OK) return rc;
+    Dev<double2> d_lz;
+    ASR_TRY(d_lz.alloc(ngroup));
+    ASR_CUDA(cudaMemsetAsync(d_lz.p, 0, ngroup * sizeof(double2), s));
+    ASR_TRY(run_lanes(ctx, op, gi, blob, GL, lg, d_lz.p, ngroup, opt, nullptr, &ha, &hb, &hm, &nfall, &nsteps));
     // plain lanczos returns n levels with b(n) (src/reference/asr_recursion.f90:57)
     std::vector<double> ra((size_t)ngroup * NLMAX), rb((size_t)ngroup * NLMAX);
     std::vector<int> rn(ngroup);
@@ -651,43 +647,39 @@ static int chains_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups
       }
     }
     if (d_g && nz > 0) {
-      double *d_a = nullptr, *d_b = nullptr, *d_ai = nullptr, *d_bi = nullptr;
-      int* d_n = nullptr;
-      ASR_CUDA(cudaMalloc(&d_a, ra.size() * sizeof(double)));
-      ASR_CUDA(cudaMalloc(&d_b, rb.size() * sizeof(double)));
-      ASR_CUDA(cudaMalloc(&d_ai, ngroup * sizeof(double)));
-      ASR_CUDA(cudaMalloc(&d_bi, ngroup * sizeof(double)));
-      ASR_CUDA(cudaMalloc(&d_n, ngroup * sizeof(int)));
-      ASR_CUDA(cudaMemcpyAsync(d_a, ra.data(), ra.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-      ASR_CUDA(cudaMemcpyAsync(d_b, rb.data(), rb.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-      ASR_CUDA(cudaMemcpyAsync(d_n, rn.data(), ngroup * sizeof(int), cudaMemcpyHostToDevice, s));
+      Dev<double> d_a, d_b, d_ai, d_bi;   // freed on every return path
+      Dev<int> d_n;
+      ASR_TRY(d_a.alloc(ra.size())); ASR_TRY(d_b.alloc(rb.size())); ASR_TRY(d_ai.alloc(ngroup)); ASR_TRY(d_bi.alloc(ngroup));
+      ASR_TRY(d_n.alloc(ngroup));
+      ASR_CUDA(cudaMemcpyAsync(d_a.p, ra.data(), ra.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+      ASR_CUDA(cudaMemcpyAsync(d_b.p, rb.data(), rb.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+      ASR_CUDA(cudaMemcpyAsync(d_n.p, rn.data(), ngroup * sizeof(int), cudaMemcpyHostToDevice, s));
       if (tail == ASR_TAIL_HULL) {
         // the complex cf_species hull tail on the real chain
         std::vector<double2> ca((size_t)ngroup * NLMAX), cb((size_t)ngroup * NLMAX);
         for (size_t q = 0; q < ca.size(); ++q) { ca[q] = make_double2(ra[q], 0.0); cb[q] = make_double2(rb[q], 0.0); }
-        double2 *d_ca = nullptr, *d_cb = nullptr, *d_zz = nullptr;
-        int* d_nf = nullptr;
-        ASR_CUDA(cudaMalloc(&d_ca, ca.size() * sizeof(double2)));
-        ASR_CUDA(cudaMalloc(&d_cb, cb.size() * sizeof(double2)));
-        ASR_CUDA(cudaMalloc(&d_zz, (size_t)nz * ngroup * sizeof(double2)));
-        ASR_CUDA(cudaMalloc(&d_nf, sizeof(int)));
-        ASR_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(int), s));
-        ASR_CUDA(cudaMemcpyAsync(d_ca, ca.data(), ca.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
-        ASR_CUDA(cudaMemcpyAsync(d_cb, cb.data(), cb.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+        Dev<double2> d_ca, d_cb, d_zz;
+        Dev<int> d_nf;
+        ASR_TRY(d_ca.alloc(ca.size())); ASR_TRY(d_cb.alloc(cb.size())); ASR_TRY(d_zz.alloc((size_t)nz * ngroup));
+        ASR_TRY(d_nf.alloc(1));
+        ASR_CUDA(cudaMemsetAsync(d_nf.p, 0, sizeof(int), s));
+        ASR_CUDA(cudaMemcpyAsync(d_ca.p, ca.data(), ca.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
+        ASR_CUDA(cudaMemcpyAsync(d_cb.p, cb.data(), cb.size() * sizeof(double2), cudaMemcpyHostToDevice, s));
         for (int q = 0; q < ngroup; ++q)
-          ASR_CUDA(cudaMemcpyAsync(d_zz + (size_t)q * nz, d_z, nz * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+          ASR_CUDA(cudaMemcpyAsync(d_zz.p + (size_t)q * nz, d_z, nz * sizeof(double2), cudaMemcpyDeviceToDevice, s));
         long nt = (long)nz * ngroup;
-        k_cf_eval<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(d_ca, d_cb, d_n, NLMAX, ngroup, d_zz, nz, tail, d_g, nullptr, d_nf);
+        k_cf_eval<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(d_ca.p, d_cb.p, d_n.p, NLMAX, ngroup, d_zz.p, nz, tail, d_g, nullptr,
+                                                               d_nf.p);
+        ASR_CUDA(cudaGetLastError());
         ASR_CUDA(cudaStreamSynchronize(s));
-        cudaFree(d_ca); cudaFree(d_cb); cudaFree(d_zz); cudaFree(d_nf);
       } else {
-        k_real_tail<<<(ngroup + 63) / 64, 64, 0, s>>>(d_a, d_b, d_n, NLMAX, ngroup, tail, d_ai, d_bi);
+        k_real_tail<<<(ngroup + 63) / 64, 64, 0, s>>>(d_a.p, d_b.p, d_n.p, NLMAX, ngroup, tail, d_ai.p, d_bi.p);
         long nt = (long)nz * ngroup;
-        k_real_green<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(d_a, d_b, d_n, NLMAX, ngroup, d_ai, d_bi, tail, d_z, nz, d_g);
+        k_real_green<<<(unsigned)((nt + 127) / 128), 128, 0, s>>>(d_a.p, d_b.p, d_n.p, NLMAX, ngroup, d_ai.p, d_bi.p, tail, d_z, nz,
+                                                                   d_g);
+        ASR_CUDA(cudaGetLastError());
         ASR_CUDA(cudaStreamSynchronize(s));
       }
-      ASR_CUDA(cudaGetLastError());
-      cudaFree(d_a); cudaFree(d_b); cudaFree(d_ai); cudaFree(d_bi); cudaFree(d_n);
     }
     ctx->nchain += ngroup;
   }
@@ -1072,31 +1064,26 @@ int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, in
   ASR_TRY(set_device(ctx));
   cudaStream_t s = ctx->stream;
   size_t nab = (size_t)ld * nchain, nzz = (size_t)nz * nchain;
-  double2 *d_a, *d_b, *d_z, *d_g, *d_e = nullptr;
-  int *d_m, *d_nf;
-  ASR_CUDA(cudaMalloc(&d_a, nab * sizeof(double2)));
-  ASR_CUDA(cudaMalloc(&d_b, nab * sizeof(double2)));
-  ASR_CUDA(cudaMalloc(&d_z, nzz * sizeof(double2)));
-  ASR_CUDA(cudaMalloc(&d_g, nzz * sizeof(double2)));
-  ASR_CUDA(cudaMalloc(&d_m, nchain * sizeof(int)));
-  ASR_CUDA(cudaMalloc(&d_nf, sizeof(int)));
-  if (edges) ASR_CUDA(cudaMalloc(&d_e, 2 * nzz * sizeof(double2)));
-  ASR_CUDA(cudaMemcpyAsync(d_a, a, nab * sizeof(double2), cudaMemcpyHostToDevice, s));
-  ASR_CUDA(cudaMemcpyAsync(d_b, b, nab * sizeof(double2), cudaMemcpyHostToDevice, s));
-  ASR_CUDA(cudaMemcpyAsync(d_z, z, nzz * sizeof(double2), cudaMemcpyHostToDevice, s));
-  ASR_CUDA(cudaMemcpyAsync(d_m, m, nchain * sizeof(int), cudaMemcpyHostToDevice, s));
-  ASR_CUDA(cudaMemsetAsync(d_nf, 0, sizeof(int), s));
-  k_cf_eval<<<(unsigned)((nzz + 127) / 128), 128, 0, s>>>(d_a, d_b, d_m, ld, nchain, d_z, nz, tail, d_g, d_e, d_nf);
+  Dev<double2> d_a, d_b, d_z, d_g, d_e;   // freed on every return path
+  Dev<int> d_m, d_nf;
+  ASR_TRY(d_a.alloc(nab)); ASR_TRY(d_b.alloc(nab)); ASR_TRY(d_z.alloc(nzz)); ASR_TRY(d_g.alloc(nzz));
+  ASR_TRY(d_m.alloc(nchain)); ASR_TRY(d_nf.alloc(1));
+  if (edges) ASR_TRY(d_e.alloc(2 * nzz));
+  ASR_CUDA(cudaMemcpyAsync(d_a.p, a, nab * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_b.p, b, nab * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_z.p, z, nzz * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemcpyAsync(d_m.p, m, nchain * sizeof(int), cudaMemcpyHostToDevice, s));
+  ASR_CUDA(cudaMemsetAsync(d_nf.p, 0, sizeof(int), s));
+  k_cf_eval<<<(unsigned)((nzz + 127) / 128), 128, 0, s>>>(d_a.p, d_b.p, d_m.p, ld, nchain, d_z.p, nz, tail, d_g.p,
+                                                          edges ? d_e.p : nullptr, d_nf.p);
   int nf = 0;
   ASR_CUDA(cudaGetLastError());
-  ASR_CUDA(cudaMemcpyAsync(g, d_g, nzz * sizeof(double2), cudaMemcpyDeviceToHost, s));
-  if (edges) ASR_CUDA(cudaMemcpyAsync(edges, d_e, 2 * nzz * sizeof(double2), cudaMemcpyDeviceToHost, s));
-  ASR_CUDA(cudaMemcpyAsync(&nf, d_nf, sizeof(int), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(g, d_g.p, nzz * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  if (edges) ASR_CUDA(cudaMemcpyAsync(edges, d_e.p, 2 * nzz * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(&nf, d_nf.p, sizeof(int), cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaStreamSynchronize(s));
   if (nfall) *nfall = nf;
   ctx->nfall += nf;
-  cudaFree(d_a); cudaFree(d_b); cudaFree(d_z); cudaFree(d_g); cudaFree(d_m); cudaFree(d_nf);
-  if (d_e) cudaFree(d_e);
   return ASR_OK;
 }
 
