@@ -32,7 +32,7 @@ EXPORTS = ["asr_version", "asr_last_error", "asr_ctx_create", "asr_ctx_destroy",
     "asr_chains_adjoint", "asr_cf_eval_noalloc", "asr_ed3_blocks", "asr_supercell_build", "asr_supercell_free",
            "asr_supercell_apply", "asr_kpm_moments", "asr_kpm_dos", "asr_sro_layout", "asr_gauss_legendre", "asr_contour_nodes",
            "asr_contour_nodes_closed", "asr_contour_nodes_fermi", "asr_contour_moment", "asr_op_build_targets",
-           "asr_chains_proj", "asr_epi_blocks", "asr_autotune"]
+           "asr_chains_proj", "asr_epi_blocks", "asr_autotune", "asr_op_tuning", "asr_op_set_tuning"]
 
 
 class ChainGroup(C.Structure):
@@ -100,6 +100,8 @@ def lib():
     L.asr_epi_blocks.argtypes = [vp, vp, C.POINTER(ChainGroup), d_p, d_p, C.c_int, d_p, C.c_int, C.c_int, C.c_int, C.c_int, d_p,
                                  i_p]
     L.asr_autotune.argtypes = [vp, vp, C.POINTER(ChainGroup), C.c_int, d_p, C.c_int, C.c_int, C.c_int, i_p, i_p, d_p]
+    L.asr_op_tuning.argtypes = [vp, C.c_int, i_p, i_p, i_p, d_p]
+    L.asr_op_set_tuning.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.asr_ed3_blocks.argtypes = [vp, vp, C.POINTER(Ed3Group), C.c_int, d_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, d_p,
                                  i_p, d_p, d_p, d_p]
     L.asr_supercell_build.argtypes = [vp, C.c_int, C.c_int, i_p, i_p, C.c_int, d_p, d_p, d_p, d_p, d_p, d_p, C.POINTER(vp)]

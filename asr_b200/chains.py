@@ -202,15 +202,39 @@ def edc_green_proj(op: AugclsOp, ed: dict, z, iv: int, nlev: int, tnode, tgop, t
 def autotune(op: AugclsOp, specs, z, precision: str = "fp64", levels: int = 8) -> dict:
     """Choose the batch shape (tiles per batch, nodes per warp) of the chains on this operator by timing the given groups
     (depth capped at ``levels``, at most 64 energies); a candidate must beat the built-in default by 3 %.  Later calls in
-    this precision use the choice.  Returns dict(tiles_per_batch,
-    nodes_per_warp, ms_tiles (4, 8, 16, 32 tiles at 4 nodes per warp), ms_npw (1, 2, 4, 8 nodes per warp))."""
+    this precision use the choice; at that shape the step kernel with fixed-offset link gathers (the same bits) is kept
+    when it is 3 % faster than the general one.  Returns dict(tiles_per_batch, nodes_per_warp, ms_tiles (4, 8, 16, 32
+    tiles at 4 nodes per warp), ms_npw (1, 2, 4, 8 nodes per warp), link_gather ("fixed-offset" or "general"),
+    ms_link (general, fixed-offset step at the chosen shape))."""
     z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
     arr, keep = _groups(specs)
     tpb, npw = C.c_int(), C.c_int()
     times = np.zeros(8)
     check(lib().asr_autotune(op.ctx.h, op.h, arr, len(specs), _pd(z), z.shape[0], PREC[precision], int(levels), C.byref(tpb),
                              C.byref(npw), _pd(times)))
-    return dict(tiles_per_batch=tpb.value, nodes_per_warp=npw.value, ms_tiles=times[:4].tolist(), ms_npw=times[4:].tolist())
+    st = tuning(op, precision)
+    return dict(tiles_per_batch=tpb.value, nodes_per_warp=npw.value, ms_tiles=times[:4].tolist(), ms_npw=times[4:].tolist(),
+                link_gather=st["link_gather"], ms_link=st["ms_link"])
+
+
+def tuning(op: AugclsOp, precision: str = "fp64") -> dict:
+    """The operator's tuned state in this precision (``asr_op_tuning``): tiles_per_batch and nodes_per_warp (0: never
+    tuned), link_gather, ms_link."""
+    tpb, npw, link = C.c_int(), C.c_int(), C.c_int()
+    ms = np.zeros(2)
+    check(lib().asr_op_tuning(op.h, PREC[precision], C.byref(tpb), C.byref(npw), C.byref(link), _pd(ms)))
+    return dict(tiles_per_batch=tpb.value, nodes_per_warp=npw.value,
+                link_gather="fixed-offset" if link.value == 1 else "general", ms_link=ms.tolist())
+
+
+def set_tuning(op: AugclsOp, precision: str = "fp64", tiles_per_batch: int = 0, nodes_per_warp: int = 0,
+               link_gather: str = "general"):
+    """Pin the tuned state in this precision (``asr_op_set_tuning``): 0 restores the built-in shape defaults;
+    link_gather "general" or "fixed-offset" (the same results)."""
+    if link_gather not in ("general", "fixed-offset"):
+        raise ValueError(link_gather)
+    check(lib().asr_op_set_tuning(op.h, PREC[precision], int(tiles_per_batch), int(nodes_per_warp),
+                                  1 if link_gather == "fixed-offset" else 0))
 
 
 def lanczos(op: AugclsOp, l0: int, nmax: int, precision: str = "fp64"):

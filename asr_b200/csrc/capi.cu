@@ -1027,6 +1027,7 @@ int asr_autotune(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ng
     }
     return ASR_OK;
   };
+  op->tuned_link[pix] = 0;   // the shapes are timed with the general step kernel
   const int tpbs[4] = {4, 8, 16, 32}, npws[4] = {1, 2, 4, 8};
   double tab[8];
   for (double& t : tab) t = -1.0;
@@ -1050,9 +1051,40 @@ int asr_autotune(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ng
     if (tab[4 + c] < margin * best) { best = tab[4 + c]; best_n = npws[c]; }
   op->tuned_tpb[pix] = best_t;
   op->tuned_npw[pix] = best_n;
+  // then the step kernel with fixed-offset link gathers at that shape (the same bits; kept when it is 3 % faster)
+  double t_gen = 0.0, t_link = 0.0;
+  ASR_TRY(timed(best_t, best_n, t_gen));
+  op->tuned_link[pix] = 1;
+  int rc = timed(best_t, best_n, t_link);
+  op->tuned_link[pix] = (rc == ASR_OK && t_link < margin * t_gen) ? 1 : 0;
+  if (rc != ASR_OK) return rc;
+  op->tuned_link_ms[pix][0] = t_gen;
+  op->tuned_link_ms[pix][1] = t_link;
   if (tpb_out) *tpb_out = best_t;
   if (npw_out) *npw_out = best_n;
   if (times) for (int c = 0; c < 8; ++c) times[c] = tab[c];
+  return ASR_OK;
+}
+
+int asr_op_tuning(const asr_op* op, int precision, int* tpb, int* npw, int* link, double* ms) {
+  if (!op || (precision != ASR_FP64 && precision != ASR_FP32)) { set_error("asr_op_tuning: bad argument"); return ASR_EINVAL; }
+  const int pix = precision == ASR_FP64 ? 0 : 1;
+  if (tpb) *tpb = op->tuned_tpb[pix];
+  if (npw) *npw = op->tuned_npw[pix];
+  if (link) *link = op->tuned_link[pix];
+  if (ms) { ms[0] = op->tuned_link_ms[pix][0]; ms[1] = op->tuned_link_ms[pix][1]; }
+  return ASR_OK;
+}
+
+int asr_op_set_tuning(asr_op* op, int precision, int tpb, int npw, int link) {
+  if (!op || (precision != ASR_FP64 && precision != ASR_FP32)) { set_error("asr_op_set_tuning: bad argument"); return ASR_EINVAL; }
+  if (!(tpb == 0 || tpb == 4 || tpb == 8 || tpb == 16 || tpb == 32)) { set_error("asr_op_set_tuning: tiles per batch %d", tpb); return ASR_EINVAL; }
+  if (!(npw == 0 || npw == 1 || npw == 2 || npw == 4 || npw == 8)) { set_error("asr_op_set_tuning: nodes per warp %d", npw); return ASR_EINVAL; }
+  if (link != 0 && link != 1) { set_error("asr_op_set_tuning: link must be 0 or 1"); return ASR_EINVAL; }
+  const int pix = precision == ASR_FP64 ? 0 : 1;
+  op->tuned_tpb[pix] = tpb;
+  op->tuned_npw[pix] = npw;
+  op->tuned_link[pix] = link;
   return ASR_OK;
 }
 

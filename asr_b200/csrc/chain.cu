@@ -154,6 +154,7 @@ template <> struct Pair<float> { typedef float2 T; };
 constexpr int RW = 12;   // padded row of a shared-memory block (16-byte aligned pairs for FP64 and FP32)
 // packed orbital operation of the identity: permutation pi(l) = l in bits 4l..4l+3, no signs (bits 40..48)
 constexpr unsigned long long PW_IDENTITY = 0x876543210ull;
+constexpr unsigned long long PW_PERM_MASK = 0xFFFFFFFFFull;   // the nine 4-bit orbital indices
 
 // the output of one node of the S application: t2 (unscaled), or with FINAL y = s (d t2 + (c + e + X(z)) U) and the
 // node's share of the dot sum norb (s U) . y
@@ -201,7 +202,10 @@ __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView&
 // FUSE_D: t1 = d o U is folded into the shared-memory blocks (the tile's d per orbital; d is invariant under the orbital
 // permutations of the group).  FINAL (needs FUSE_D, o = 0): y = s (d o S d o U + (c + e + X(z)) U) and the partial dot
 // sum_i norb_i (s U_i) . y_i (normalised-coordinate bilinear form).  Group data are per tile (single-group tiles).
-template <typename ST, bool FUSE_D, bool FINAL>
+// LINK_ID: links whose orbital operation keeps the orbital order (the identity, and the pure sign changes of diagonal
+// groups such as D2h) gather their nine rows at fixed offsets, without the per-orbital index and sign decoding; the
+// products and their order are those of the general path, so both instantiations give the same bits.
+template <typename ST, bool FUSE_D, bool FINAL, bool LINK_ID>
 __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, const ST* __restrict__ blocks,
                                                    const typename St2<ST>::T* __restrict__ in,
                                                    typename St2<ST>::T* __restrict__ out, double2* part, int npw) {
@@ -285,9 +289,16 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
       const unsigned long long pw = piw[gk];
       const T2* src = in + vix(it.tile, bv.nn, r, 0) + lane;
       T2 v[9];
-      for (int lp = 0; lp < 9; ++lp) {
-        int p = (int)((pw >> (4 * lp)) & 15ull);
-        v[lp] = flip_if(src[p * TL], (uint32_t)((pw >> (40 + lp)) & 1ull));
+      if (LINK_ID && pw == PW_IDENTITY) {                                        // warp-uniform: one node, one slot
+        for (int lp = 0; lp < 9; ++lp) v[lp] = src[lp * TL];
+      } else if (LINK_ID && (pw & PW_PERM_MASK) == PW_IDENTITY) {               // signs only
+        const uint32_t sg = (uint32_t)(pw >> 40);
+        for (int lp = 0; lp < 9; ++lp) v[lp] = flip_if(src[lp * TL], (sg >> lp) & 1u);
+      } else {
+        for (int lp = 0; lp < 9; ++lp) {
+          int p = (int)((pw >> (4 * lp)) & 15ull);
+          v[lp] = flip_if(src[p * TL], (uint32_t)((pw >> (40 + lp)) & 1ull));
+        }
       }
       const ST* Bk = B + (size_t)(k + 1) * 9 * RW;
       for (int l = 0; l < 9; ++l) {
@@ -858,10 +869,13 @@ template <typename ST, bool FUSE_D, bool FINAL>
 void launch_smul(asr_op* op, const BatchView& bv, const ST* blk, const typename St2<ST>::T* in, typename St2<ST>::T* out,
                  double2* part, int npw, int grid, cudaStream_t s) {
   OpView ov = op->view();
+  const int pix = std::is_same<ST, double>::value ? 0 : 1;
   if (smul_bulk_enabled())
     k_smul_bulk<ST, FUSE_D, FINAL><<<grid, WPB * TL, smul_bulk_smem<ST>(op), s>>>(ov, bv, blk, in, out, part, npw, op->ctx->d_err);
+  else if (op->tuned_link[pix] == 1)
+    k_smul<ST, FUSE_D, FINAL, true><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
   else
-    k_smul<ST, FUSE_D, FINAL><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
+    k_smul<ST, FUSE_D, FINAL, false><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
 }
 
 // a bounded wait of the staged kernels that ran out (the device error word), as a status
@@ -2283,12 +2297,18 @@ static void smem_attrs() {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64 || done[dev]) return;
-  cudaFuncSetAttribute(k_smul<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-  cudaFuncSetAttribute(k_smul<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-  cudaFuncSetAttribute(k_smul<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-  cudaFuncSetAttribute(k_smul<float, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-  cudaFuncSetAttribute(k_smul<float, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-  cudaFuncSetAttribute(k_smul<float, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, true, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, false, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   cudaFuncSetAttribute(k_smul_bulk<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_smul_bulk<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_smul_bulk<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

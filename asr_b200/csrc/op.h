@@ -57,6 +57,8 @@ struct asr_op {
   int start_l = 1;
   // batch shape chosen by asr_autotune per precision (index 0 FP64, 1 FP32); 0: the built-in defaults
   int tuned_tpb[2] = {0, 0}, tuned_npw[2] = {0, 0};
+  int tuned_link[2] = {0, 0};             // 1: the step kernel's fixed-offset link gathers (chosen by asr_autotune)
+  double tuned_link_ms[2][2] = {{-1.0, -1.0}, {-1.0, -1.0}};   // device ms of the general / fixed-offset step at the tuned shape
   // host copies of the model and group
   std::vector<int> nsc, spc;       // spc(ldspc, ncls)
   int ldspc = 1;

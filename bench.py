@@ -542,7 +542,8 @@ def main():
 
     # batch shape (tiles per batch, nodes per warp) chosen by timing on this operator (asr_autotune), outside the timed region
     tune = (A.autotune(op, specs, z_all[:nzs], args.precision) if args.autotune else
-            {"tiles_per_batch": 16 if args.precision == "fp64" else 8, "nodes_per_warp": 4, "ms_tiles": None, "ms_npw": None})
+            {"tiles_per_batch": 16 if args.precision == "fp64" else 8, "nodes_per_warp": 4, "ms_tiles": None, "ms_npw": None,
+             "link_gather": "general", "ms_link": None})
 
     def slice_of(it):
         # each rank walks its own slices (weak scaling); rank r starts r slices further
@@ -639,7 +640,8 @@ def main():
                        "l2": "inputs larger than L2 (one 32-lane vector is %.0f MB)" % (op.nn * 9 * 32 * 16 / 1e6),
                        "parallelism": f"chain tasks over {world} GPU(s)", "operator_build_s": build_s,
                        "batch_shape": {"tiles_per_batch": tune["tiles_per_batch"], "nodes_per_warp": tune["nodes_per_warp"],
-                                       "autotune_ms_tiles_4_8_16_32": tune["ms_tiles"], "autotune_ms_npw_1_2_4_8": tune["ms_npw"]},
+                                       "autotune_ms_tiles_4_8_16_32": tune["ms_tiles"], "autotune_ms_npw_1_2_4_8": tune["ms_npw"],
+                                       "link_gather": tune["link_gather"], "autotune_ms_link_general_fixed": tune["ms_link"]},
                        "precision": args.precision},
             "e2e": {"value": e2e, "unit": "chain-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,

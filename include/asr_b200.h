@@ -161,9 +161,21 @@ int asr_epi_blocks(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, cons
  * at 4 nodes per warp, by 3 %) on the operator for this precision; later calls that leave the shape
  * automatic use it.  The shape does not change results beyond the order of the per-block partial sums (rounding).
  * Each candidate is timed on the device (CUDA events around its batches, allocations excluded, best of two runs).
+ * At the chosen shape it then times the step kernel with fixed-offset link gathers (links whose orbital operation keeps
+ * the orbital order read their nine rows without index decoding; the same bits) against the general one and keeps it
+ * when it is 3 % faster.
  * tpb, npw: the chosen shape; times(8) the device times in ms (-1: skipped) or NULL. */
 int asr_autotune(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz, int precision,
                  int levels, int* tpb, int* npw, double* times);
+
+/* The operator's tuned state for a precision: tpb, npw (0: never tuned, the built-in defaults apply), link = 1 when the
+ * fixed-offset link gathers are in use, ms(2) the device times of the general and the fixed-offset step at the tuned shape
+ * (-1: not timed).  Any pointer may be NULL.  No counterpart in the reference. */
+int asr_op_tuning(const asr_op* op, int precision, int* tpb, int* npw, int* link, double* ms);
+/* Set the tuned state for a precision (a shape saved from an earlier asr_autotune, or a pinned one): tpb in {4, 8, 16, 32}
+ * or 0 (built-in default), npw in {1, 2, 4, 8} or 0, link 0 (general gathers) or 1 (fixed-offset).  Results do not depend
+ * on link; the shape changes only the order of the per-block partial sums. */
+int asr_op_set_tuning(asr_op* op, int precision, int tpb, int npw, int link);
 
 /* ---- route ed3 (src/asr_ed3.f90): chains on z - K'(z), K' = et - h' + u h' + h' u - h' Qt h', h' = g + d S d ---------- */
 typedef struct asr_ed3_group {

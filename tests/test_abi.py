@@ -87,6 +87,13 @@ def test_fermi_contour_occupation():
         assert abs(occ - f) < 1e-6, (eps, occ, f)
 
 
+def test_tuning_entry_points_check_their_arguments():
+    L = asr_b200.lib()
+    assert L.asr_op_set_tuning(None, _lib.FP64, 16, 4, 0) == _lib.ASR_EINVAL
+    assert "asr_op_set_tuning" in _lib.last_error()
+    assert L.asr_op_tuning(None, _lib.FP64, None, None, None, None) == _lib.ASR_EINVAL
+
+
 def test_missing_library_fails_loudly(monkeypatch):
     monkeypatch.setattr(_lib, "_LIB", None)
     monkeypatch.setattr(_lib, "LIB_PATH", "/nonexistent/libasr_b200.so")

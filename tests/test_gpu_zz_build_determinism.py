@@ -39,3 +39,29 @@ def test_repeated_device_builds_and_chains_are_identical():
     go, mo, _, _ = oop.edc_green_blk(ed, zs, 5, 24, depth_tol=0.0, tail="hull")
     assert np.array_equal(ma, mo)
     assert np.max(np.abs(ga - go) / np.abs(go)) < 1e-8
+
+
+@pytest.mark.parametrize("group", ["d2h", "d4h"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_fixed_offset_link_gathers_give_the_same_bits(group, precision):
+    """The step kernel with fixed-offset link gathers (identity and sign-only orbital operations read their rows without
+    index decoding) gives the same Green functions bit for bit as the general kernel at the same batch shape: D2h links
+    are identities or sign changes, D4h links also permute orbitals (the general path inside the same kernel)."""
+    from asr_b200 import chains as CH
+    case = K.cubic("fcc", 3, 3, (0.66, 0.14, 0.2), group=group, maxlevel=3, maxrank=1)
+    op = A.build_augcls_operator(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, case["maxlevel"],
+                                 maxrank=case["maxrank"], flippable=case["flippable"])
+    sp = S.draw_species(3, 2)
+    specs = []
+    for cen in (1, 2, 3):
+        ed = S.edc_params(sp, cen)
+        for l0 in (1, 3, 7):
+            specs.append(CH.ChainSpec(c=ed["c"], d=ed["d"], o=ed["o"], e=ed["e"], pa=ed["pa"], pb=ed["pb"], frozen_sp=cen,
+                                      start_orb=l0, nlev=14))
+    z = np.linspace(-1.0, 0.5, 70) + 0.02j
+    out = {}
+    for link in ("general", "fixed-offset"):
+        A.set_tuning(op, precision, 16 if precision == "fp64" else 8, 4, link)
+        assert A.tuning(op, precision)["link_gather"] == link
+        out[link] = CH.chains_run(op, specs, z, "edc", 0.0, "hull", precision)["g"]
+    assert np.array_equal(out["general"], out["fixed-offset"])
