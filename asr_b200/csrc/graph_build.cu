@@ -440,8 +440,13 @@ int permute_rows(cudaStream_t s, int nn, int w, const int* d_oon, const int* d_n
   ASR_CUDA(cudaMalloc(&q, std::max<size_t>((size_t)nn * w, 1) * sizeof(T)));
   long n = (long)nn * w;
   k_perm_rows<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(nn, w, d_oon, d_noo, p, q, remap);
-  ASR_CUDA(cudaGetLastError());
-  ASR_CUDA(cudaStreamSynchronize(s));
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    cudaFree(q);
+    set_error("permute_rows: %s", cudaGetErrorString(e));
+    return ASR_ECUDA;
+  }
   cudaFree(p);
   p = q;
   return ASR_OK;
@@ -514,10 +519,14 @@ int reorder_nodes(asr_ctx* ctx, asr_op* op) {
   std::vector<int> oon = rcm_order(nn, ns, hr), noo(nn);
   for (int n = 0; n < nn; ++n) noo[oon[n]] = n;
   int *d_oon = nullptr, *d_noo = nullptr;
-  ASR_CUDA(cudaMalloc(&d_oon, nn * sizeof(int)));
-  ASR_CUDA(cudaMalloc(&d_noo, nn * sizeof(int)));
-  ASR_CUDA(cudaMemcpyAsync(d_oon, oon.data(), nn * sizeof(int), cudaMemcpyHostToDevice, s));
-  ASR_CUDA(cudaMemcpyAsync(d_noo, noo.data(), nn * sizeof(int), cudaMemcpyHostToDevice, s));
+  if (cudaMalloc(&d_oon, nn * sizeof(int)) != cudaSuccess || cudaMalloc(&d_noo, nn * sizeof(int)) != cudaSuccess ||
+      cudaMemcpyAsync(d_oon, oon.data(), nn * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+      cudaMemcpyAsync(d_noo, noo.data(), nn * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+    cudaFree(d_oon);
+    cudaFree(d_noo);
+    set_error("reorder_nodes: device allocation or copy of the node order failed");
+    return ASR_ENOMEM;
+  }
   int rc = ASR_OK;
   auto run = [&](int r) { if (rc == ASR_OK) rc = r; };
   run(permute_rows<int>(s, nn, 1, d_oon, d_noo, op->d_site, false));
