@@ -1,7 +1,6 @@
 """Golden node counts of the reference's shipped examples ("nodes / sublattice" in example/reference/*/asr.out): the
 oracle's restatement of build_augcls_operator (src/asr_augcls.f90:596-823) on the examples' graphs and reduction groups
 gives the reference's production node sets."""
-import numpy as np
 import pytest
 
 from asr_b200 import synthetic as S
