@@ -5,8 +5,10 @@
 // calls this file.  Every routine cites the reference Fortran it restates (paths relative to the asr project root).
 //
 // Parity pins: the golden complex chains and known-answer tests of test/test_terminators.f90 (tests/golden/), the
-// exact-enumeration toy models of test_slow/test_augcls.f90 (ring; dense numpy solve) and the reduced == unreduced
-// dense-solve check of test/test_augcls_project.f90.  LAPACK zgeev / dsterf (external, no pinned version; MKL or
+// exact-enumeration toy models of test_slow/test_augcls.f90 (ring; dense numpy solve), the reduced == unreduced
+// dense-solve check of test/test_augcls_project.f90, the node counts the reference prints for its shipped examples
+// (example/reference/*/asr.out), the task-count invariance of test/test_augcls_threads.f90, and the sc-band contour
+// moments of test/test_contour.f90 against exact band integrals.  LAPACK zgeev / dsterf (external, no pinned version; MKL or
 // OpenBLAS) are replaced by published algorithms: shifted complex Hessenberg QR (Golub & Van Loan, Alg. 7.5.1 with
 // Wilkinson shifts) and Sturm-sequence bisection (Wilkinson 1965); tests check both against scipy's LAPACK.
 //
