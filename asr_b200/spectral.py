@@ -8,7 +8,9 @@ Host-side restatement of the caller of ``edc_green_proj`` in the reference's ``a
 * ``spectral_structure_ok`` / ``spectral_origin_classes`` (:83-148): every sublattice one space-group orbit, and the
   basis sites grouped into origin classes by pure translations and inversions (with the sign of the mapping and the site
   fraction of each class);
-* ``spectral_sum_origins`` -- the Bloch sum over several origin classes (src/asr_class_scf.f90:1566-1590, 1690-1745):
+* ``spectral_targets`` -- the targets of one origin class (src/asr_class_scf.f90:1562-1586): cluster sites within rmax,
+  with the origin class and mapping sign of each target's basis site;
+* ``spectral_sum_origins`` -- the Bloch sum over several origin classes (src/asr_class_scf.f90:1588-1601, 1693-1746):
   the partner of every target in the origin class of the target's own basis site (at -R, or +R through an inversion),
   the average with it, and the windowed sums weighted by the site fractions of the origin classes;
 * ``bloch_spectral`` -- one origin class (a Bravais sublattice whose sites are related by translations or inversion):
@@ -25,7 +27,8 @@ import numpy as np
 from .chains import ChainSpec, chains_proj
 
 __all__ = ["spectral_kpath", "spectral_window", "spectral_unfold", "augn_basis", "spectral_dressing", "spectral_structure_ok",
-           "spectral_origin_classes", "spectral_elements", "spectral_sum", "spectral_sum_origins", "bloch_spectral"]
+           "spectral_origin_classes", "spectral_targets", "spectral_elements", "spectral_sum", "spectral_sum_origins",
+           "bloch_spectral"]
 
 ORB_L = np.array([0, 1, 1, 1, 2, 2, 2, 2, 2])
 
@@ -149,6 +152,23 @@ def spectral_origin_classes(s, ops=None):
                         bclass[b2], sign[b2] = len(orig), sg
     w = np.array([np.sum(bclass == g) / nb for g in range(1, len(orig) + 1)])
     return bclass, np.array(orig, dtype=np.int64), sign, w
+
+
+def spectral_targets(cg, bclass, orig_sign, rmax: float) -> dict:
+    """Targets of one origin class (spectral_final, src/asr_class_scf.f90:1562-1586): the sites of the origin's crystal
+    graph ``cg`` (``crystal.crystal_graph`` started on the origin's representative basis site) within rmax (alat) of the
+    origin, in cluster order.  bclass (nb, 1-based) and orig_sign (nb) come from ``spectral_origin_classes``.  Returns
+    dict(tsite (nt,) 1-based graph sites for ``asr_op_build_targets``, tdisp (3, nt), tbase (nt,) the 0-based origin class
+    of each target's basis site, tsign (nt,), t0 the index of the origin among the targets)."""
+    disp = np.asarray(cg.disp, dtype=float)
+    r2 = 4.0 * np.sum(disp * disp, axis=0)
+    sel = np.nonzero(r2 <= 4.0 * rmax * rmax + 1.0e-9)[0]
+    if sel.size == 0 or sel[0] != 0:
+        raise ValueError("spectral_targets: the origin is not a spectral target")
+    basis = np.asarray(cg.basis)[sel]
+    return dict(tsite=(sel + 1).astype(np.int32), tdisp=disp[:, sel].copy(),
+                tbase=(np.asarray(bclass)[basis] - 1).astype(np.int64), tsign=np.asarray(orig_sign)[basis].astype(float),
+                t0=0)
 
 
 def spectral_elements(op, tnode, tgop, t0: int, comps, conc, eds, z, nsteps: int, tail: str = "hull", precision: str = "fp64",

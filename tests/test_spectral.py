@@ -255,3 +255,39 @@ def test_multi_origin_sum_on_an_ordered_b2_crystal():
             v = sum(-np.imag(gd[o::9, o::9]) / np.pi for o in np.nonzero(orb_l == l)[0])
             exact = float(np.sum(c * v)) / n
             assert abs(A[0, q, l] - exact) < 1e-9 * max(1.0, abs(exact)), (k, l, A[0, q, l], exact)
+
+
+def test_targets_per_origin_class_and_their_partners():
+    """Targets of every origin class (spectral_final, src/asr_class_scf.f90:1562-1601) for the ordered B2 cell (two
+    classes, translations only) and hcp (one class, the second site by inversion): the origin comes first, every target
+    lies within rmax, tbase / tsign follow the basis site, and every target of B2 finds its partner at -R in its own
+    origin class's list (so the partner average of spectral_sum_origins never falls back)."""
+    from asr_b200 import crystal as CR
+    for name, ca, rmax, nor in (("b2", None, 1.01, 2), ("hcp", None, 1.5, 1)):
+        s = CR.prototype_structure(name, ca)
+        ops = CR.space_group(s)
+        bclass, orig_b, orig_sign, orig_w = SP.spectral_origin_classes(s, ops)
+        assert len(orig_b) == nor and abs(np.sum(orig_w) - 1.0) < 1e-12
+        tg = []
+        for u in range(nor):
+            cg = CR.crystal_graph(s, ops, 1.0, 2, start=int(orig_b[u]) - 1, rmin=rmax)
+            t = SP.spectral_targets(cg, bclass, orig_sign, rmax)
+            assert t["t0"] == 0 and np.all(t["tdisp"][:, 0] == 0.0)
+            assert np.all(np.linalg.norm(t["tdisp"], axis=0) <= rmax + 1e-9)
+            assert np.array_equal(t["tbase"], bclass[cg.basis[t["tsite"] - 1]] - 1)
+            assert t["tbase"][0] == u
+            tg.append(t)
+        if name == "b2":
+            assert all(np.all(t["tsign"] == 1.0) for t in tg)
+            for u in range(nor):
+                for j in range(tg[u]["tsite"].shape[0]):
+                    u2 = tg[u]["tbase"][j]
+                    d = tg[u2]["tdisp"] + tg[u]["tsign"][j] * tg[u]["tdisp"][:, j:j + 1]
+                    hit = (tg[u2]["tbase"] == u) & (np.max(np.abs(d), axis=0) < 1e-9)
+                    assert hit.sum() == 1
+            # NN shell of the other sublattice, NNN shell of the own one
+            r = np.linalg.norm(tg[0]["tdisp"], axis=0)
+            assert set(tg[0]["tbase"][np.abs(r - np.sqrt(0.75)) < 1e-9]) == {1}
+            assert set(tg[0]["tbase"][np.abs(r - 1.0) < 1e-9]) == {0}
+        else:
+            assert sorted(set(tg[0]["tsign"])) == [-1.0, 1.0]
