@@ -115,3 +115,19 @@ def test_fortran_binding_matches_the_header():
     for name, args in found:
         assert name in protos, name
         assert len([a for a in args.split(",") if a.strip()]) == len(protos[name]), name
+
+
+def test_ctypes_argtypes_match_the_header():
+    """The ctypes binding declares, for every entry point, as many arguments as its C prototype."""
+    src = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "asr_b200.h")).read(), flags=re.S)
+    protos = {m.group(1): [a for a in m.group(2).split(",") if a.strip() and a.strip() != "void"]
+              for m in re.finditer(r"int\s+(asr_\w+)\s*\(([^)]*)\)\s*;", src)}
+    L = asr_b200.lib()
+    checked = 0
+    for name in _lib.EXPORTS:
+        f = getattr(L, name)
+        if f.argtypes is None:
+            continue
+        assert len(f.argtypes) == len(protos[name]), name
+        checked += 1
+    assert checked >= 30
