@@ -3,7 +3,8 @@ binary with flippable sites, class operations, levels 4, rank 2 (65,972 nodes he
 same node set and every table bit for bit, equal to the oracle's (the parallel closure claims each new node by the
 smallest candidate position, so the numbering does not depend on the schedule); (C) the edc chains from orbital 5 with
 the start site frozen, depth 24, hull tail, no depth test, give bitwise the same G on repeated calls (fixed-order
-reductions, no floating-point atomics) and the oracle's G."""
+reductions, no floating-point atomics) and the oracle's G.  Also: the step kernel's two link-gather instantiations give
+the same bits."""
 import numpy as np
 import pytest
 
