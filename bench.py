@@ -650,7 +650,7 @@ def main():
                        "precision": args.precision},
             "e2e": {"value": e2e, "unit": "chain-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "traffic": traffic, "kernel": "chain step operator (k_smul, fused S + diagonal + dot)",
+                         "traffic": traffic, "kernel": "chain step operator (k_smul, fused S + diagonal + dot; %s link gathers)" % tune["link_gather"],
                          "per_launch_ms": per_launch_ms, "launches": ks["launches"], "fp64_tflops": tflops,
                          "share_of_step": ks["ms"] / ms, "peak_source": peak_source,
                          "fp64_frac": (tflops / legs["fp64_peak_tflops"]) if legs else None,
