@@ -179,7 +179,8 @@ def space_group(s: Structure) -> list[SymOp]:
     (src/asr_crystal_symmetry.f90:50-116)."""
     g = s.avec.T @ s.avec
     ainv = inv3(s.avec)
-    # anchor: the first site of the label with the fewest sites
+    # every operation must carry some site onto a site of the same label; trying the translations only from one site of
+    # the rarest label keeps the candidate list shortest (ties: the lowest label number, then the first such site)
     i0, nlab = 0, s.nb + 1
     for lab in range(1, s.nlabel + 1):
         n = int(np.sum(s.label == lab))
@@ -217,7 +218,9 @@ def space_group(s: Structure) -> list[SymOp]:
     if not ident:
         raise RuntimeError("space_group: the identity was not found")
     k = ident[0]
-    ops[0], ops[k] = ops[k], ops[0]           # a swap, as the reference does: the rest keep their search order
+    # the identity goes first by exchanging two entries (not by a shift of the list), so that the site groups and the
+    # canonical representatives built from this order see the operations in the order the search found them
+    ops[0], ops[k] = ops[k], ops[0]
     return ops
 
 

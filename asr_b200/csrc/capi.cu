@@ -203,11 +203,6 @@ void free_op(asr_op* op) {
   delete op;
 }
 
-int set_device(asr_ctx* ctx) {
-  ASR_CUDA(cudaSetDevice(ctx->device));
-  return ASR_OK;
-}
-
 }  // namespace
 }  // namespace asrb
 
@@ -230,7 +225,7 @@ int asr_ctx_create(int device, asr_ctx** out) {
   int ndev = 0;
   ASR_CUDA(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) { set_error("asr_ctx_create: device %d of %d", device, ndev); return ASR_EINVAL; }
-  ASR_CUDA(cudaSetDevice(device));
+  ASR_ON_DEVICE(device);
   asr_ctx* c = new asr_ctx();
   c->device = device;
   cudaDeviceProp prop;
@@ -250,7 +245,8 @@ int asr_ctx_create(int device, asr_ctx** out) {
 
 int asr_ctx_destroy(asr_ctx* ctx) {
   if (!ctx) return ASR_OK;
-  cudaSetDevice(ctx->device);
+  DeviceGuard dg;
+  dg.set(ctx->device);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   if (ctx->d_err) cudaFree(ctx->d_err);
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
@@ -301,7 +297,7 @@ int asr_ctx_kernel_stats(asr_ctx* ctx, double* ms, int64_t* launches, double* by
 }
 
 int asr_ctx_sync(asr_ctx* ctx) {
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   ASR_CUDA(cudaStreamSynchronize(ctx->stream));
   return ASR_OK;
 }
@@ -324,7 +320,7 @@ static int op_build(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int* nbr,
   }
   *out = nullptr;
   if (nsite < 1 || ncls < 1 || nop < 1 || nsp < 1 || ldspc < 1) { set_error("asr_op_build: empty input"); return ASR_EINVAL; }
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   for (int k = 0; k < ncls; ++k) {
     if (nsc[k] < 1 || nsc[k] > ldspc) { set_error("asr_op_build: species count of class %d", k + 1); return ASR_EINVAL; }
     double sum = 0.0;
@@ -389,7 +385,8 @@ int asr_op_build_targets(asr_ctx* ctx, int nsite, const int* nbr_ptr, const int*
 
 int asr_op_free(asr_op* op) {
   if (!op) return ASR_OK;
-  cudaSetDevice(op->ctx->device);
+  DeviceGuard dg;
+  dg.set(op->ctx->device);
   free_op(op);
   return ASR_OK;
 }
@@ -405,7 +402,7 @@ int asr_op_export_tables(const asr_op* op, int* flipr, int* flipg, int* hopr, in
                          double* norb, double* sq, int* stab_ptr, int* stab) {
   if (!op) { set_error("asr_op_export_tables: null operator"); return ASR_EINVAL; }
   asr_ctx* ctx = op->ctx;
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   cudaStream_t s = ctx->stream;
   const size_t nn = op->nn, nsm = op->nsmax, ns = op->nslot;
   std::vector<int> fr(nsm * nn), hr(ns * nn), sp(nn + 1), st(nn), lv(nn), ob(nn);
@@ -467,7 +464,7 @@ int asr_op_set_params(asr_op* op, const double* c, const double* d, const double
 int asr_op_freeze_site(asr_op* op, int site, int sp) {
   if (!op) { set_error("augcls_freeze_site: null operator"); return ASR_EINVAL; }
   if (sp < 1 || sp > op->nsp) { set_error("augcls_freeze_any: species index out of range"); return ASR_EINVAL; }
-  ASR_TRY(set_device(op->ctx));
+  ASR_ON_DEVICE(op->ctx->device);
   cudaStream_t s = op->ctx->stream;
   const size_t nn = op->nn, nsm = op->nsmax;
   std::vector<int> st(nn), fr(nsm * nn);
@@ -490,7 +487,7 @@ int asr_op_freeze_site(asr_op* op, int site, int sp) {
 
 int asr_op_unfreeze(asr_op* op) {
   if (!op) { set_error("asr_op_unfreeze: null operator"); return ASR_EINVAL; }
-  ASR_TRY(set_device(op->ctx));
+  ASR_ON_DEVICE(op->ctx->device);
   std::fill(op->frozen_h.begin(), op->frozen_h.end(), 0);
   ASR_CUDA(cudaMemsetAsync(op->d_frozen, 0, op->nn, op->ctx->stream));
   ASR_CUDA(cudaStreamSynchronize(op->ctx->stream));
@@ -544,7 +541,7 @@ static int op_group(asr_op* op, const GroupLayout& GL, const double* pa, const d
 
 int asr_op_apply(asr_op* op, const double* x, double* y, int nvec) {
   if (!op || !x || !y || nvec < 1) { set_error("augcls_apply: bad argument"); return ASR_EINVAL; }
-  ASR_TRY(set_device(op->ctx));
+  ASR_ON_DEVICE(op->ctx->device);
   GroupLayout GL = layout(op);
   std::vector<double> blob;
   std::vector<GroupInfo> gi;
@@ -554,7 +551,7 @@ int asr_op_apply(asr_op* op, const double* x, double* y, int nvec) {
 
 int asr_op_rand_c(asr_op* op, const double* par, const double* x, double* w, int nvec) {
   if (!op || !par || !x || !w || nvec < 1) { set_error("augcls_rand_c: bad argument"); return ASR_EINVAL; }
-  ASR_TRY(set_device(op->ctx));
+  ASR_ON_DEVICE(op->ctx->device);
   GroupLayout GL = layout(op);
   const int np = 9 * op->nsp;
   std::vector<double> pr(np), pim(np);
@@ -567,7 +564,7 @@ int asr_op_rand_c(asr_op* op, const double* par, const double* x, double* w, int
 
 int asr_op_project_c(asr_op* op, double* x, int nvec) {
   if (!op || !x || nvec < 1) { set_error("augcls_project_c: bad argument"); return ASR_EINVAL; }
-  ASR_TRY(set_device(op->ctx));
+  ASR_ON_DEVICE(op->ctx->device);
   GroupLayout GL = layout(op);
   std::vector<double> blob;
   std::vector<GroupInfo> gi;
@@ -581,7 +578,7 @@ static int chains_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups
   if (!ctx || !op || !groups || ngroup < 1 || nz < 0) { set_error("asr_chains_run: bad argument"); return ASR_EINVAL; }
   if (mode != ASR_MODE_PLAIN && mode != ASR_MODE_EDC) { set_error("asr_chains_run: unknown mode"); return ASR_EINVAL; }
   if (tail < 0 || tail > 3) { set_error("asr_chains_run: unknown tail"); return ASR_EINVAL; }
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   cudaStream_t s = ctx->stream;
   GroupLayout GL = layout(op);
   std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
@@ -696,7 +693,7 @@ int asr_epi_blocks(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, cons
                    const double* z, int nz, int tail, int precision, int project, double* x, int* mused) {
   if (!ctx || !op || !groups || !v9 || !chi || ngroup < 1 || nz < 1 || !z || !x) { set_error("asr_epi_blocks: bad argument"); return ASR_EINVAL; }
   if (tail < 0 || tail > 3) { set_error("asr_epi_blocks: unknown tail"); return ASR_EINVAL; }
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   GroupLayout GL = layout(op);
   std::vector<double> blob((size_t)GL.stride * ngroup, 0.0), vv(9 * (size_t)ngroup);
   std::vector<GroupInfo> gi(ngroup);
@@ -748,7 +745,7 @@ int asr_ed3_blocks(asr_ctx* ctx, asr_op* op, const asr_ed3_group* groups, int ng
                    int tail, int precision, int project, double* bk, int* mused, double* a, double* b, double* c) {
   if (!ctx || !op || !groups || ngroup < 1 || nz < 1 || !z || !bk) { set_error("asr_ed3_blocks: bad argument"); return ASR_EINVAL; }
   if (tail < 0 || tail > 3) { set_error("asr_ed3_blocks: unknown tail"); return ASR_EINVAL; }
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   const int nsp = op->nsp, np = 9 * nsp;
   GroupLayout GL = layout(op);
   std::vector<double> blob((size_t)GL.stride * ngroup, 0.0), oc(ngroup);
@@ -828,7 +825,7 @@ int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
     set_error("asr_chains_adjoint: tail must be none, hull or avg2");
     return ASR_EINVAL;
   }
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   GroupLayout GL = layout(op);
   std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
   std::vector<GroupInfo> gi(ngroup);
@@ -901,7 +898,7 @@ int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
 int asr_chains_run(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz, int mode,
                    double depth_tol, int tail, int precision, int project, double* g, double* a, double* b, int* mused) {
   if (!ctx || !z || !g) { set_error("asr_chains_run: null argument"); return ASR_EINVAL; }
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   if (nz < 0 || ngroup < 1) { set_error("asr_chains_run: bad argument"); return ASR_EINVAL; }
   cudaStream_t s = ctx->stream;
   const size_t ng = (size_t)nz * ngroup;
@@ -934,7 +931,7 @@ int asr_chains_proj(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int
     tn[q] = tnode[q] > 0 ? op->dev_node(tnode[q] - 1) : -1;   // reference numbering -> the device's node order
     tg[q] = tnode[q] > 0 ? tgop[q] - 1 : 0;
   }
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   cudaStream_t s = ctx->stream;
   GroupLayout GL = layout(op);
   std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
@@ -993,7 +990,7 @@ int asr_autotune(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ng
                  int levels, int* tpb_out, int* npw_out, double* times) {
   if (!ctx || !op || !groups || ngroup < 1 || !z || nz < 1 || levels < 1) { set_error("asr_autotune: bad argument"); return ASR_EINVAL; }
   if (precision != ASR_FP64 && precision != ASR_FP32) { set_error("asr_autotune: unknown precision"); return ASR_EINVAL; }
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   GroupLayout GL = layout(op);
   std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
   std::vector<GroupInfo> gi(ngroup);
@@ -1027,6 +1024,16 @@ int asr_autotune(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ng
     }
     return ASR_OK;
   };
+  // the tuned state is only replaced when every timing succeeded: a failed timing leaves the operator's previous (or
+  // pinned) shape and link choice in place
+  struct Restore {
+    asr_op* op;
+    int pix, tpb, npw, link;
+    bool done = false;
+    ~Restore() {
+      if (!done) { op->tuned_tpb[pix] = tpb; op->tuned_npw[pix] = npw; op->tuned_link[pix] = link; }
+    }
+  } keep{op, pix, op->tuned_tpb[pix], op->tuned_npw[pix], op->tuned_link[pix]};
   op->tuned_link[pix] = 0;   // the shapes are timed with the general step kernel
   const int tpbs[4] = {4, 8, 16, 32}, npws[4] = {1, 2, 4, 8};
   double tab[8];
@@ -1056,8 +1063,9 @@ int asr_autotune(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ng
   ASR_TRY(timed(best_t, best_n, t_gen));
   op->tuned_link[pix] = 1;
   int rc = timed(best_t, best_n, t_link);
-  op->tuned_link[pix] = (rc == ASR_OK && t_link < margin * t_gen) ? 1 : 0;
   if (rc != ASR_OK) return rc;
+  op->tuned_link[pix] = t_link < margin * t_gen ? 1 : 0;
+  keep.done = true;
   op->tuned_link_ms[pix][0] = t_gen;
   op->tuned_link_ms[pix][1] = t_link;
   if (tpb_out) *tpb_out = best_t;
@@ -1093,7 +1101,7 @@ int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, in
   if (!ctx || !a || !b || !m || !z || !g || ld < 1 || nchain < 1 || nz < 1) { set_error("asr_cf_eval: bad argument"); return ASR_EINVAL; }
   for (int c = 0; c < nchain; ++c)
     if (m[c] < 1 || m[c] > ld || m[c] > CF_NMAX) { set_error("asr_cf_eval: depth of chain %d out of range", c + 1); return ASR_EINVAL; }
-  ASR_TRY(set_device(ctx));
+  ASR_ON_DEVICE(ctx->device);
   cudaStream_t s = ctx->stream;
   size_t nab = (size_t)ld * nchain, nzz = (size_t)nz * nchain;
   Dev<double2> d_a, d_b, d_z, d_g, d_e;   // freed on every return path
@@ -1110,6 +1118,7 @@ int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, in
                                                           edges ? d_e.p : nullptr, d_nf.p);
   int nf = 0;
   ASR_CUDA(cudaGetLastError());
+  ctx->launches += 1;
   ASR_CUDA(cudaMemcpyAsync(g, d_g.p, nzz * sizeof(double2), cudaMemcpyDeviceToHost, s));
   if (edges) ASR_CUDA(cudaMemcpyAsync(edges, d_e.p, 2 * nzz * sizeof(double2), cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaMemcpyAsync(&nf, d_nf.p, sizeof(int), cudaMemcpyDeviceToHost, s));

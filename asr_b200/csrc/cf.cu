@@ -72,27 +72,25 @@ __global__ void k_real_green(const double* a, const double* b, const int* n, int
 namespace asrb {
 namespace {
 
-constexpr int kMaxDevices = 64;
 __device__ __align__(256) unsigned char g_cf_scratch[ASR_CF_NOALLOC_BYTES];
 std::mutex g_cf_mu;
-unsigned char* g_cf_ptr[kMaxDevices] = {};
 
 size_t up256(size_t n) { return (n + 255) & ~(size_t)255; }
 
-// device address of the scratch on the current device, resolved once per device (the device must be current)
-int cf_scratch(int dev, unsigned char** out) {
-  if (dev < 0 || dev >= kMaxDevices) { set_error("asr_cf_eval_noalloc: device %d out of range", dev); return ASR_EINVAL; }
+// device address of the scratch on the context's device, resolved on the first call with that device current and kept
+// with the context (a context, like every device address it holds, does not outlive a reset of its device)
+int cf_scratch(asr_ctx* ctx, unsigned char** out) {
   std::lock_guard<std::mutex> lk(g_cf_mu);
-  if (!g_cf_ptr[dev]) {
+  if (!ctx->cf_scratch) {
     void* p = nullptr;
     cudaError_t rc = cudaGetSymbolAddress(&p, g_cf_scratch);
     if (rc != cudaSuccess || !p) {
-      set_error("asr_cf_eval_noalloc: cudaGetSymbolAddress failed on device %d: %s", dev, cudaGetErrorString(rc));
+      set_error("asr_cf_eval_noalloc: cudaGetSymbolAddress failed on device %d: %s", ctx->device, cudaGetErrorString(rc));
       return ASR_ECUDA;
     }
-    g_cf_ptr[dev] = (unsigned char*)p;
+    ctx->cf_scratch = (unsigned char*)p;
   }
-  *out = g_cf_ptr[dev];
+  *out = ctx->cf_scratch;
   return ASR_OK;
 }
 
@@ -117,9 +115,9 @@ extern "C" int asr_cf_eval_noalloc(asr_ctx* ctx, const double* a, const double* 
               (size_t)ASR_CF_NOALLOC_BYTES);
     return ASR_EINVAL;
   }
-  ASR_CUDA(cudaSetDevice(ctx->device));
+  ASR_ON_DEVICE(ctx->device);
   unsigned char* base = nullptr;
-  ASR_TRY(cf_scratch(ctx->device, &base));
+  ASR_TRY(cf_scratch(ctx, &base));
   cudaStream_t s = ctx->stream;
   double2* d_a = (double2*)base;
   double2* d_b = (double2*)(base + o_b);

@@ -28,6 +28,31 @@ const char* get_error();
     if (s_ != ASR_OK) return s_;    \
   } while (0)
 
+// Makes a device current for the rest of a scope and makes the caller's device current again at its end, so that an
+// entry point leaves the calling thread's current device as it found it.
+struct DeviceGuard {
+  int prev = -1;
+  int set(int dev) {
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) cur = -1;
+    if (cur != dev) {
+      cudaError_t e = cudaSetDevice(dev);
+      if (e != cudaSuccess) {
+        set_error("cudaSetDevice(%d): %s", dev, cudaGetErrorString(e));
+        return ASR_ECUDA;
+      }
+      prev = cur;
+    }
+    return ASR_OK;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+#define ASR_ON_DEVICE(dev)       \
+  ::asrb::DeviceGuard dguard_;   \
+  ASR_TRY(dguard_.set(dev))
+
 // device error codes written into a flag word (the first error wins)
 enum DevErr : int {
   DERR_NONE = 0,

@@ -462,7 +462,7 @@ int asr_supercell_build(asr_ctx* ctx, int nsite, int nslot, const int* nbr, cons
     if (spc[i] < 1 || spc[i] > nsp) { set_error("asr_supercell_build: species index out of range"); return ASR_EINVAL; }
     sp[i] = (uint8_t)(spc[i] - 1);
   }
-  ASR_CUDA(cudaSetDevice(ctx->device));
+  ASR_ON_DEVICE(ctx->device);
   asr_supercell* sc = new asr_supercell();
   sc->ctx = ctx; sc->n = nsite; sc->ns = nslot; sc->nsp = nsp;
   std::vector<int> nb((size_t)nslot * nsite);
@@ -502,7 +502,8 @@ int asr_supercell_build(asr_ctx* ctx, int nsite, int nslot, const int* nbr, cons
 
 int asr_supercell_free(asr_supercell* sc) {
   if (!sc) return ASR_OK;
-  cudaSetDevice(sc->ctx->device);
+  DeviceGuard dg;
+  dg.set(sc->ctx->device);
   cudaFree(sc->d_nbr); cudaFree(sc->d_spc); cudaFree(sc->d_par); cudaFree(sc->d_blocks); cudaFree(sc->d_blocks_f);
   delete sc;
   return ASR_OK;
@@ -511,7 +512,7 @@ int asr_supercell_free(asr_supercell* sc) {
 int asr_supercell_apply(asr_supercell* sc, const double* x, double* y, int nvec) {
   if (!sc || !x || !y || nvec < 1) { set_error("asr_supercell_apply: bad argument"); return ASR_EINVAL; }
   asr_ctx* ctx = sc->ctx;
-  ASR_CUDA(cudaSetDevice(ctx->device));
+  ASR_ON_DEVICE(ctx->device);
   cudaStream_t s = ctx->stream;
   const int n = sc->n;
   const size_t nel = (size_t)n * 9 * KV;
@@ -553,7 +554,7 @@ int asr_supercell_apply(asr_supercell* sc, const double* x, double* y, int nvec)
 int asr_kpm_moments(asr_ctx* ctx, asr_supercell* sc, double cen, double scl, int nmom, int v0, int nvec, uint64_t seed,
                     int precision, int doubling, double* mu) {
   if (!ctx || !sc || !mu || nmom < 1 || nvec < 1 || !(scl > 0.0)) { set_error("kpm_moments: bad argument"); return ASR_EINVAL; }
-  ASR_CUDA(cudaSetDevice(ctx->device));
+  ASR_ON_DEVICE(ctx->device);
   if (precision == ASR_FP32) return kpm_run<float>(ctx, sc, cen, scl, nmom, v0, nvec, seed, doubling != 0, mu);
   return kpm_run<double>(ctx, sc, cen, scl, nmom, v0, nvec, seed, doubling != 0, mu);
 }

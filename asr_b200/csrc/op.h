@@ -21,6 +21,7 @@ struct asr_ctx {
   int64_t prof_launches = 0;
   std::vector<cudaEvent_t> ev_pool;   // pairs (start, end) of the timed launches
   int ev_used = 0;                    // pairs recorded and not yet read
+  unsigned char* cf_scratch = nullptr;   // device address of asr_cf_eval_noalloc's static array (resolved on first use)
 };
 
 namespace asrb {

@@ -26,7 +26,7 @@ sys.path.insert(0, ROOT)
 
 NZ_SLICE = 192
 # DRAM bytes (read + write) per launch of the step kernel from one ncu capture of a 16-tile launch, and the algorithmic
-# bytes of that launch (profiles/k_smul_fcc_ternary_edc.md); traffic is scaled to the bench's mean launch
+# bytes of that launch; traffic is scaled to the bench's mean launch
 NCU_STEP_TRAFFIC = {"fp64": (3.30e9, 16 * 20969 * (2 * 4608.0 + 18 * 5 + 3 * 5 + 20))}
 
 
@@ -650,7 +650,10 @@ def main():
                        "precision": args.precision},
             "e2e": {"value": e2e, "unit": "chain-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "traffic": traffic, "kernel": "chain step operator (k_smul, fused S + diagonal + dot; %s link gathers)" % tune["link_gather"],
+                         "traffic": traffic,
+                         "traffic_source": "ncu capture of the general-link k_smul<double,1,1> at 16 tiles, scaled to the "
+                                           "mean launch" if traffic is not None else None,
+                         "kernel": "chain step operator (k_smul, fused S + diagonal + dot; %s link gathers)" % tune["link_gather"],
                          "per_launch_ms": per_launch_ms, "launches": ks["launches"], "fp64_tflops": tflops,
                          "share_of_step": ks["ms"] / ms, "peak_source": peak_source,
                          "fp64_frac": (tflops / legs["fp64_peak_tflops"]) if legs else None,

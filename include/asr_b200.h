@@ -213,9 +213,10 @@ int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, in
 /* asr_cf_eval without device allocation (no edges), for callers that may not call cudaMalloc / cudaFree (they
  * synchronise the device, or device memory belongs to another allocator).  No counterpart in the reference.  The
  * operands go through one static device array of ASR_CF_NOALLOC_BYTES per device; calls whose operands need more
- * (32 ld nchain + 32 nz nchain + 4 nchain + 4 bytes, each part rounded up to 256) return ASR_EINVAL.  The first call on
- * a device resolves the array's address; make it before capturing the context's stream.  Calls that overlap in time
- * on one device share the array and race: serialise them. */
+ * (32 ld nchain + 32 nz nchain + 4 nchain + 4 bytes, each part rounded up to 256) return ASR_EINVAL.  The call is
+ * synchronous: it copies the operands from host memory and returns after g and nfall are back on the host.  The first
+ * call on a context resolves the array's device address and keeps it with the context; make that first call before any
+ * stream capture on the device.  Calls that overlap in time on one device share the array and race: serialise them. */
 #define ASR_CF_NOALLOC_BYTES (8u << 20)
 int asr_cf_eval_noalloc(asr_ctx* ctx, const double* a, const double* b, const int* m, int ld, int nchain, const double* z,
                         int nz, int tail, double* g, int64_t* nfall);

@@ -102,14 +102,12 @@ def test_missing_library_fails_loudly(monkeypatch):
 
 
 def test_fortran_binding_matches_the_header():
-    """Every interface of the iso_c_binding module in INTEGRATION.md names a declared entry point with the same number of
-    arguments as its C prototype."""
+    """Every interface of the iso_c_binding module include/asr_b200.f90 names a declared entry point with the same number
+    of arguments as its C prototype."""
     src = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "asr_b200.h")).read(), flags=re.S)
     protos = {m.group(1): [a for a in m.group(2).split(",") if a.strip() and a.strip() != "void"]
               for m in re.finditer(r"int\s+(asr_\w+)\s*\(([^)]*)\)\s*;", src)}
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    block = doc[doc.index("```fortran"):]
-    block = block[:block.index("```", 10)].replace("&\n", "")
+    block = open(os.path.join(ROOT, "include", "asr_b200.f90")).read().replace("&\n", "")
     found = re.findall(r"function\s+(asr_\w+)\s*\(([^)]*)\)", block)
     assert len(found) >= 15
     for name, args in found:
