@@ -265,6 +265,34 @@ def cubic_case(kind: str, l: int, nsp: int, conc, seed: int, group: str = "d2h",
                 dmat=np.asfortranarray(dmat), model=mdl)
 
 
+def batched_ternary_workload():
+    """The batched, uneven-depth configuration: fcc ternary Fe0.66Ni0.14Cr0.20-like random alloy on a 5^3-cell periodic
+    cluster (NN + NNN Slater-Koster blocks, 18 slots), one site class, D2h reduction (the operator is built from start
+    site 1 to 3 levels at rank 1, the start site not flippable); 2 spins x 3 central species x 9 start orbitals = 54 chain
+    groups in the edc form (``edc_params``) with depths drawn from U{16..28} (seed 1); energies: the 48-point
+    Gauss-Legendre semicircle over [-1.2, 0.3] (the node rule of contour_nodes, src/asr_contour.f90:17-34) followed by
+    4096 real-axis energies on [-1.5, 1.0] + 0.005i.  Returns (case, flippable, groups, z), groups as dicts of ed, cen,
+    l0, nlev in the order (spin, central species, start orbital)."""
+    case = cubic_case("fcc", 5, 3, [0.66, 0.14, 0.20], seed=1, group="d2h")
+    fl = np.ones(case["graph"].n, np.int32)
+    fl[0] = 0
+    rng = np.random.default_rng(1)
+    depths = rng.integers(16, 29, size=54)
+    groups = []
+    for spin in range(2):
+        sp = draw_species(3, seed=1 + spin)
+        for cen in (1, 2, 3):
+            ed = edc_params(sp, cen)
+            for l0 in range(1, 10):
+                groups.append(dict(ed=ed, cen=cen, l0=l0, nlev=int(depths[len(groups)]), spin=spin))
+    ebot, ef = -1.2, 0.3
+    x, _ = np.polynomial.legendre.leggauss(48)
+    th = 0.5 * np.pi * (1.0 - x)
+    zc = 0.5 * (ebot + ef) + 0.5 * (ef - ebot) * np.exp(1j * th)
+    zr = np.linspace(-1.5, 1.0, 4096) + 0.005j
+    return case, fl, groups, np.concatenate([zc, zr])
+
+
 # L2_1 (Heusler-like) decoration of bcc: four fcc sublattices.  Sites of the bcc grid have i, j, k all even or all odd
 # (half-lattice units); even sites split by (i + j + k) / 2 mod 2, odd sites by (i + j + k - 3) / 2 mod 2.
 HEUSLER_SHIFT = ((0, 0, 0), (2, 0, 0), (1, 1, 1), (3, 1, 1))   # a site of sublattice 1..4 relative to sublattice 1

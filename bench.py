@@ -43,34 +43,18 @@ def parse():
     p.add_argument("--scf", type=int, default=0,
                    help="SCF leg: 0 none, 1 two timed iterations at full size + convergence on a small cluster, 2 converge at full size")
     p.add_argument("--autotune", type=int, default=1, help="choose the batch shape by timing first (1) or use the defaults (0)")
-    p.add_argument("--legs", type=int, default=1,
-                   help="also measure the mixed-precision leg with its DOS error and the adjoint leg (1) or not (0)")
+    p.add_argument("--legs", default="1",
+                   help="1: measure every leg (mixed precision with its DOS error, adjoint, KPM, plain, example, spectral, "
+                        "EPI), 0: none, or a comma list of leg names")
+    p.add_argument("--link", default="auto", choices=["auto", "general", "fixed"],
+                   help="step-kernel link gathers: the autotuner's choice (auto; general without --autotune), or pinned")
     return p.parse_args()
 
 
 def workload():
     """Synthetic inputs of the configuration (host arrays only)."""
     from asr_b200 import synthetic as S
-    case = S.cubic_case("fcc", 5, 3, [0.66, 0.14, 0.20], seed=1, group="d2h")
-    fl = np.ones(case["graph"].n, np.int32)
-    fl[0] = 0
-    rng = np.random.default_rng(1)
-    depths = rng.integers(16, 29, size=54)
-    groups = []
-    for spin in range(2):
-        sp = S.draw_species(3, seed=1 + spin)
-        for cen in (1, 2, 3):
-            ed = S.edc_params(sp, cen)
-            for l0 in range(1, 10):
-                groups.append(dict(ed=ed, cen=cen, l0=l0, nlev=int(depths[len(groups)])))
-    # energies: contour_nodes (src/asr_contour.f90:17-34) on [ebot, ef] + real axis
-    ebot, ef = -1.2, 0.3
-    x, _ = np.polynomial.legendre.leggauss(48)
-    th = 0.5 * np.pi * (1.0 - x)
-    zc = 0.5 * (ebot + ef) + 0.5 * (ef - ebot) * np.exp(1j * th)
-    zr = np.linspace(-1.5, 1.0, 4096) + 0.005j
-    z = np.concatenate([zc, zr])
-    return case, fl, groups, z
+    return S.batched_ternary_workload()
 
 
 def specs_of(groups):
@@ -437,14 +421,25 @@ def scf_leg(torch, full: bool):
     return out
 
 
-def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
-    """The mixed-precision leg (FP32 matvec and vectors, FP64 coefficients and fractions) with its DOS and charge error
-    against the FP64 run, and the adjoint leg (forward plus reverse sweep) on the contour energies."""
+LEGS = ("mixed", "adjoint", "kpm", "plain", "example", "spectral", "epi")
+
+
+def contour_weights(z_all):
+    """dz weights of the 48-point semicircle (the first 48 energies of the workload) for the contour charge M_0."""
+    ebot, ef = -1.2, 0.3
+    x, wgl = np.polynomial.legendre.leggauss(48)
+    th = 0.5 * np.pi * (1.0 - x)
+    return z_all[:48], 0.5 * np.pi * wgl * 0.5j * (ef - ebot) * np.exp(1j * th)
+
+
+def mixed_leg(args, A, op, specs, groups, z_all, step, stream, world):
+    """The mixed-precision form (FP32 vectors and matvec, FP64 coefficients and fractions): chain-steps/s on the timed
+    slices, and its DOS error against the FP64 run over the whole real axis (every fourth of the 4096 energies, all 54
+    groups) and the error of the contour charge M_0 per group."""
     import torch
     nzs = args.nz_slice
     depth = np.array([g["nlev"] for g in groups])
-    out = {}
-    out["fp32_batch_shape"] = A.autotune(op, specs, z_all[:nzs], "fp32")
+    out = {"fp32_batch_shape": A.autotune(op, specs, z_all[:nzs], "fp32")}
     step(0, "fp32")
     torch.cuda.synchronize()
     nsteps = max(1, min(args.steps, 3))
@@ -456,51 +451,77 @@ def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
     torch.cuda.synchronize()
     ms32 = e0.elapsed_time(e1)
     mixed = {"value": int(depth.sum()) * nzs * nsteps * world / (ms32 / 1000.0), "unit": "chain-steps/s", "steps": nsteps}
-    # error against FP64: DOS -Im G / pi on 192 real-axis energies, and the contour charge M_0 over the 48 contour nodes
-    zr = z_all[48:48 + 192]
+    zr = z_all[48::4]
     g64 = A.chains_run(op, specs, zr, "edc", 0.0, "hull", "fp64")["g"]
     g32 = A.chains_run(op, specs, zr, "edc", 0.0, "hull", "fp32")["g"]
     dos64, dos32 = -g64.imag / np.pi, -g32.imag / np.pi
     mixed["dos_error"] = float(np.max(np.abs(dos32 - dos64)) / np.max(np.abs(dos64)))
-    ebot, ef = -1.2, 0.3
-    x, wgl = np.polynomial.legendre.leggauss(48)
-    th = 0.5 * np.pi * (1.0 - x)
-    zc = z_all[:48]
-    wc = 0.5 * np.pi * wgl * 0.5j * (ef - ebot) * np.exp(1j * th)   # dz along the semicircle
+    zc, wc = contour_weights(z_all)
     c64 = A.chains_run(op, specs, zc, "edc", 0.0, "hull", "fp64")["g"]
     c32 = A.chains_run(op, specs, zc, "edc", 0.0, "hull", "fp32")["g"]
     q64 = -np.imag(np.sum(wc[:, None] * c64, axis=0)) / np.pi
     q32 = -np.imag(np.sum(wc[:, None] * c32, axis=0)) / np.pi
     mixed["charge_error"] = float(np.max(np.abs(q32 - q64)))
-    mixed["error_basis"] = ("max |DOS32 - DOS64| / max DOS64 over 54 groups x 192 real-axis energies; max |M0_32 - M0_64| "
-                            "of the 48-node contour charge per group")
+    mixed["error_basis"] = ("max |DOS32 - DOS64| / max DOS64 over 54 groups x 1024 real-axis energies (every fourth of the "
+                            "4096, the whole band); max |M0_32 - M0_64| of the 48-node contour charge per group")
     out["mixed"] = mixed
-    # adjoint: forward + reverse sweep of all groups over the 48 contour energies, seeds = contour charge weights
+    return out
+
+
+def adjoint_leg(args, A, op, specs, groups, z_all, stream):
+    """Forward plus reverse sweep of all 54 groups over the 48 contour energies (seeds: the contour charge weights), in
+    FP64 and in the mixed form, against the forward alone on the same energies; the mixed gradient's error against FP64."""
+    import torch
+    depth = np.array([g["nlev"] for g in groups])
+    zc, wc = contour_weights(z_all)
     w = np.repeat(wc[:, None], len(specs), axis=1)
-    A.chains_adjoint(op, specs, zc[:8], w[:8], "hull", "fp64", True)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    _, grad = A.chains_adjoint(op, specs, zc, w, "hull", "fp64", True)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    msa = e0.elapsed_time(e1)
-    e0.record(stream)
-    A.chains_run(op, specs, zc, "edc", 0.0, "hull", "fp64")
-    e1.record(stream)
-    torch.cuda.synchronize()
-    msf = e0.elapsed_time(e1)
     steps_adj = int(depth.sum()) * zc.shape[0]
-    out["adjoint"] = {"value": steps_adj / (msa / 1000.0), "unit": "chain-steps/s (forward + reverse, checkpoints every "
-                      "sqrt(depth) levels)", "forward_same_energies": steps_adj / (msf / 1000.0),
-                      "adjoint_over_forward_time": msa / msf, "energies": int(zc.shape[0]), "groups": len(specs),
-                      "gradient_norm": float(np.linalg.norm(grad))}
+    out, grads = {}, {}
+    for prec in ("fp64", "fp32"):
+        A.chains_adjoint(op, specs, zc[:8], w[:8], "hull", prec, True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, grads[prec] = A.chains_adjoint(op, specs, zc, w, "hull", prec, True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        msa = e0.elapsed_time(e1)
+        e0.record(stream)
+        A.chains_run(op, specs, zc, "edc", 0.0, "hull", prec)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        msf = e0.elapsed_time(e1)
+        out[prec] = {"value": steps_adj / (msa / 1000.0), "forward_same_energies": steps_adj / (msf / 1000.0),
+                     "adjoint_over_forward_time": msa / msf, "gradient_norm": float(np.linalg.norm(grads[prec]))}
+    out["unit"] = "chain-steps/s (forward + reverse, checkpoints every sqrt(depth) levels)"
+    out["energies"], out["groups"] = int(zc.shape[0]), len(specs)
+    out["fp32_gradient_error"] = float(np.max(np.abs(grads["fp32"] - grads["fp64"])) / np.max(np.abs(grads["fp64"])))
+    # the FP64 entries under their former names
+    out["value"], out["forward_same_energies"] = out["fp64"]["value"], out["fp64"]["forward_same_energies"]
+    out["adjoint_over_forward_time"] = out["fp64"]["adjoint_over_forward_time"]
+    return out
+
+
+def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
+    """The legs chosen by --legs (all by default), each a dict in the JSON line's ``legs``."""
+    import torch
+    want = set(LEGS) if args.legs == "1" else set(x.strip() for x in args.legs.split(",") if x.strip())
+    out = {}
+    if "mixed" in want:
+        out.update(mixed_leg(args, A, op, specs, groups, z_all, step, stream, world))
+    if "adjoint" in want:
+        out["adjoint"] = adjoint_leg(args, A, op, specs, groups, z_all, stream)
     out["fp64_peak_tflops"] = fp64_peak_tflops(torch)
-    out["kpm"] = kpm_leg(torch)
-    out["plain"] = plain_leg(torch)
-    out["example_cuzn"] = example_leg(torch)
-    out["spectral"] = spectral_leg(torch)
-    out["epi"] = epi_leg(torch)
+    if "kpm" in want:
+        out["kpm"] = kpm_leg(torch)
+    if "plain" in want:
+        out["plain"] = plain_leg(torch)
+    if "example" in want:
+        out["example_cuzn"] = example_leg(torch)
+    if "spectral" in want:
+        out["spectral"] = spectral_leg(torch)
+    if "epi" in want:
+        out["epi"] = epi_leg(torch)
     if args.scf:
         out["scf"] = scf_leg(torch, args.scf == 2)
     return out
@@ -544,6 +565,9 @@ def main():
     tune = (A.autotune(op, specs, z_all[:nzs], args.precision) if args.autotune else
             {"tiles_per_batch": 16 if args.precision == "fp64" else 8, "nodes_per_warp": 4, "ms_tiles": None, "ms_npw": None,
              "link_gather": "general", "ms_link": None})
+    if args.link != "auto":
+        tune["link_gather"] = "fixed-offset" if args.link == "fixed" else "general"
+        A.set_tuning(op, args.precision, tune["tiles_per_batch"], tune["nodes_per_warp"], tune["link_gather"])
 
     def slice_of(it):
         # each rank walks its own slices (weak scaling); rank r starts r slices further
@@ -610,7 +634,7 @@ def main():
         ms_e2e = float(t.item())
     e2e = total_steps / (ms_e2e / 1000.0)
     # the legs measure single-GPU kernels and configurations: one GPU only (every rank skips them alike)
-    legs = run_legs(args, A, op, specs, groups, z_all, step, stream, world) if args.legs and world == 1 else None
+    legs = run_legs(args, A, op, specs, groups, z_all, step, stream, world) if args.legs != "0" and world == 1 else None
     nsp = 3
     h2d = nzs * 16 + len(specs) * 6 * 9 * nsp * 8
     d2h = len(specs) * nzs * (16 + 4)

@@ -1556,10 +1556,11 @@ extern "C" int orc_ed3_blocks(void* h, int ns, const double* dc, const double* d
 // (the copy-on-write of lop(kp) = cop(kp)%op), its frozen start site and its start orbital.
 // params: per (comp, spin) group q: c,d,o,e (9, nsp) each, then edn dc(9), del(9,nsp), enu(9,nsp); group layout
 // [c|d|o|e|dc|del|enu] with sizes 4*9*nsp + 9 + 2*9*nsp.  gcomp(q): central species (frozen at the start site).
-// iorb(o): start orbital index (1..9).  nlevq(q, o): chain depth.  Output gz(nz, norb, ngroup) complex.
+// iorb(o): start orbital index (1..9).  nlevq(q, o): chain depth.  Output gz(nz, norb, ngroup) complex; optional (NULL:
+// not wanted) the chain coefficients a, b (ldab, nz, norb, ngroup) complex and the depths used mz(nz, norb, ngroup).
 extern "C" int orc_chain_greens(void* h, int ngroup, const double* params, const int* gcomp, int norb, const int* iorb,
                                 const int* nlevq, const double* zs, int nz, int nbe, double depth_tol, int tail, int project,
-                                int nthreads, double* gz, long* nchainsteps) {
+                                int nthreads, double* gz, long* nchainsteps, int ldab, double* az, double* bz, int* mz) {
   Op& op0 = *(Op*)h;
   const int nsp = op0.nsp;
   const size_t gstride = 4 * 9 * (size_t)nsp + 9 + 2 * 9 * (size_t)nsp;
@@ -1576,7 +1577,7 @@ extern "C" int orc_chain_greens(void* h, int ngroup, const double* params, const
     BlkWork wk;
     wk.init(nbe, 9 * (size_t)op.nn);
     int curq = -1, curo = -1;
-    std::vector<cd> gb(nbe);
+    std::vector<cd> gb(nbe), ab, bb;
     std::vector<int> mu(nbe);
 #pragma omp for schedule(dynamic)
     for (long t = 0; t < ntask; ++t) {
@@ -1594,12 +1595,22 @@ extern "C" int orc_chain_greens(void* h, int ngroup, const double* params, const
              std::vector<double>(P + 36 * nsp + 9 + 9 * nsp, P + 36 * nsp + 9 + 18 * nsp)};
       int j1 = jb * nbe, j2 = std::min(nz, j1 + nbe);
       int nlev = nlevq[q + (size_t)ngroup * o];
+      const bool want_ab = az && bz && nlev <= ldab;
+      if (want_ab) { ab.assign((size_t)nlev * nbe, cd(0.0)); bb.assign((size_t)nlev * nbe, cd(0.0)); }
       edc_green_blk(op, wk, ed, (const cd*)zs + j1, j2 - j1, iorb[o], nlev, depth_tol, tail, project != 0, gb.data(), mu.data(),
-                    nullptr, nullptr, nullptr);
+                    want_ab ? ab.data() : nullptr, want_ab ? bb.data() : nullptr, nullptr);
       for (int j = j1; j < j2; ++j) {
         size_t dst = (size_t)j + (size_t)nz * (o + (size_t)norb * q);
         gz[2 * dst] = gb[j - j1].real(); gz[2 * dst + 1] = gb[j - j1].imag();
         steps += mu[j - j1];
+        if (mz) mz[dst] = mu[j - j1];
+        if (want_ab)
+          for (int k = 0; k < nlev; ++k) {
+            az[2 * (dst * ldab + k)] = ab[(size_t)(j - j1) * nlev + k].real();
+            az[2 * (dst * ldab + k) + 1] = ab[(size_t)(j - j1) * nlev + k].imag();
+            bz[2 * (dst * ldab + k)] = bb[(size_t)(j - j1) * nlev + k].real();
+            bz[2 * (dst * ldab + k) + 1] = bb[(size_t)(j - j1) * nlev + k].imag();
+          }
       }
     }
   }

@@ -69,7 +69,7 @@ def lib():
         L.orc_edc_green_blk.argtypes = [C.c_void_p, C.c_int, _d, _d, _d, _d, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int,
                                         C.c_int, _d, _i, _d, _d, _l]
         L.orc_chain_greens.argtypes = [C.c_void_p, C.c_int, _d, _i, C.c_int, _i, _i, _d, C.c_int, C.c_int, C.c_double,
-                                       C.c_int, C.c_int, C.c_int, _d, _l]
+                                       C.c_int, C.c_int, C.c_int, _d, _l, C.c_int, _d, _d, _i]
         L.orc_ed3_blocks.argtypes = [C.c_void_p, C.c_int, _d, _d, _d, _d, _d, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                                      C.c_double, C.c_int, C.c_int, _d, _i, _d, _d, _d, _l]
         L.orc_gauss_legendre.argtypes = [C.c_int, _d, _d]
@@ -297,9 +297,12 @@ class OracleOp:
                                         _pd(c[j]), C.byref(nf)))
         return bk.T, m.T, a, b, c
 
-    def chain_greens(self, groups, gcomp, iorb, nlevq, zs, nbe, depth_tol=0.0, tail="hull", project=True, nthreads=0):
+    def chain_greens(self, groups, gcomp, iorb, nlevq, zs, nbe, depth_tol=0.0, tail="hull", project=True, nthreads=0,
+                     coefs=False):
         """``chain_greens`` (src/asr_class_scf.f90:966-1160): groups is a list of dicts with c, d, o, e, dc, dl, enu;
-        gcomp the central species (0: none frozen); iorb the start orbitals; nlevq (ngroup, norb) depths."""
+        gcomp the central species (0: none frozen); iorb the start orbitals; nlevq (ngroup, norb) depths.  Returns
+        (gz (nz, norb, ngroup), chain-steps); with coefs also dict(a, b = (nlevmax, nz, norb, ngroup), m = (nz, norb,
+        ngroup)) of every chain."""
         nsp = self.nsp
         P = np.concatenate([np.concatenate([_f64(gq[k]).ravel(order="F") for k in ("c", "d", "o", "e", "dc", "dl", "enu")])
                             for gq in groups])
@@ -310,10 +313,18 @@ class OracleOp:
         gz = np.zeros((len(groups), len(iorb), nz), np.complex128)   # memory order of Fortran gz(nz, norb, ngroup)
         steps = C.c_long(0)
         assert P.shape[0] == len(groups) * (4 * 9 * nsp + 9 + 18 * nsp)
+        ld = int(np.max(nlevq)) if coefs else 1
+        az = np.zeros((len(groups), len(iorb), nz, ld), np.complex128) if coefs else None
+        bz = np.zeros_like(az) if coefs else None
+        mz = np.zeros((len(groups), len(iorb), nz), np.int32) if coefs else None
         _check(lib().orc_chain_greens(self.h, len(groups), _pd(P), _pi(gcomp), len(iorb), _pi(iorb), _pi(nlevq),
                                       _pd(zs), nz, nbe, depth_tol, TAILS[tail], int(project), nthreads,
-                                      _pd(gz), C.byref(steps)))
-        return gz.transpose(2, 1, 0), steps.value
+                                      _pd(gz), C.byref(steps), ld, _pd(az) if coefs else None, _pd(bz) if coefs else None,
+                                      _pi(mz) if coefs else None))
+        if not coefs:
+            return gz.transpose(2, 1, 0), steps.value
+        return gz.transpose(2, 1, 0), steps.value, dict(a=az.transpose(3, 2, 1, 0), b=bz.transpose(3, 2, 1, 0),
+                                                        m=mz.transpose(2, 1, 0))
 
 
 # ---------------------------------------------------------------------------------------------- free functions
