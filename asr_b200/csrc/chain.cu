@@ -163,6 +163,7 @@ __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView&
                                               int gflags, int gfrozen, const unsigned long long* piw, const T2* __restrict__ in,
                                               T2* __restrict__ out, const A2* acc, double2& dot) {
   if (!FINAL) {
+#pragma unroll
     for (int l = 0; l < 9; ++l) stv(out + vix(tile, bv.nn, i, l) + lane, make_double2(acc[l].x, acc[l].y));
   } else {
     // y_l = s (d_l t2_l + P_l(U)),  P = c + e + X(z) (src/asr_augblk.f90:219-250), orbital by orbital
@@ -173,6 +174,7 @@ __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView&
     const double norb = op.sq[i] * op.sq[i];
     const int fs = (op.start[i] && gfrozen > 0) ? gfrozen : (int)op.frozen[i];
     const int nsm = op.nsmax, kap = op.ncl[i], l0 = op.lst[i], nk = op.nsc[kap];
+#pragma unroll
     for (int l = 0; l < 9; ++l) {
       double2 ui = ld(in + vix(tile, bv.nn, i, l) + lane);
       double2 pt;
