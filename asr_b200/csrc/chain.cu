@@ -138,6 +138,86 @@ __device__ __forceinline__ void block_reduce_store(double2 v, double2* part, int
   }
 }
 
+// Ticket of a finished block: true in every thread of the block of `tile` that stored its partials last, once all bpt
+// blocks of the tile have stored theirs (no block waits on another).  The last block resets the ticket for the next
+// launch.  Every thread of the block calls it, after block_reduce_store.
+__device__ __forceinline__ bool last_block_of_tile(int* tick, int tile, int bpt) {
+  __shared__ int s_last;
+  __threadfence();   // the partials this block stored, before its ticket
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int t = atomicAdd(tick + tile, 1);
+    s_last = t == bpt - 1;
+    if (s_last) tick[tile] = 0;
+  }
+  __syncthreads();
+  if (s_last) __threadfence();
+  return s_last != 0;
+}
+
+// a_k = sum of the partials (fixed order) for one lane of a tile; depth test every 4 levels from 8
+// (src/asr_edc.f90:121-127) when DEPTH (without it the caller guarantees that no depth test is due at level k)
+template <bool DEPTH>
+__device__ __forceinline__ void reduce_a_lane(const BatchView& bv, const double2* part, int bpt, int k, int tile, int lane) {
+  int L = tile * TL + lane;
+  int grp = bv.lane_group[L];
+  bv.lane_wact[L] = 0;
+  if (grp < 0 || !bv.lane_act[L]) return;
+  double2 a = make_double2(0, 0);
+  for (int q = 0; q < bpt; ++q) a = cadd(a, __ldcg(part + ((size_t)tile * bpt + q) * TL + lane));
+  bv.acur[L] = a;
+  bv.acoef[(size_t)L * NLMAX + k - 1] = a;
+  bv.lane_m[L] = k;
+  int nlev = bv.ginfo[grp].nlev;
+  bool go = true;
+  if (k == nlev) {
+    go = false;   // edc exits before b_k (src/asr_edc.f90:120); the plain chain still forms b_n (asr_recursion.f90:50-57)
+    if (bv.mode == ASR_MODE_PLAIN) bv.lane_wact[L] = 1;
+  } else if (DEPTH && bv.depth_tol > 0.0 && k >= 8 && k % 4 == 0 && bv.mode == ASR_MODE_EDC) {
+    double2 wd[NLMAX], we[NLMAX];
+    int nf = 0;
+    double2 gtry = cf_species_dev(bv.acoef + (size_t)L * NLMAX, bv.bcoef + (size_t)L * NLMAX, k, bv.lane_z[L], bv.tail, wd, we,
+                                  &nf, nullptr);
+    if (nf) atomicAdd(bv.nfall, nf);
+    if (k > 8 && cmag(csub(gtry, bv.gprev[L])) <= bv.depth_tol * cmag(gtry)) go = false;   // :123-125
+    bv.gprev[L] = gtry;
+  }
+  if (go) bv.lane_wact[L] = 1;
+  else bv.lane_act[L] = 0;
+}
+
+// b_k = sqrt(w . w); |b| < tol ends the chain; scales of the next step (u <- w / b, up <- u).  One full warp per tile.
+__device__ __forceinline__ void reduce_b_lane(const BatchView& bv, const double2* part, int bpt, int k, double btol, int tile,
+                                              int lane, bool tile_live) {
+  int L = tile * TL + lane;
+  int grp = bv.lane_group[L];
+  bool act = false;
+  if (tile_live && grp >= 0 && bv.lane_wact[L]) {
+    double2 ww = make_double2(0, 0);
+    for (int q = 0; q < bpt; ++q) ww = cadd(ww, __ldcg(part + ((size_t)tile * bpt + q) * TL + lane));
+    double2 b = bv.mode == ASR_MODE_PLAIN ? make_double2(sqrt(ww.x), 0.0) : csqrt_p(ww);
+    bv.bcoef[(size_t)L * NLMAX + k - 1] = b;
+    bool ok = bv.mode == ASR_MODE_PLAIN ? (b.x >= btol) : (cmag(b) >= btol);   // |b| < 1e-12 ends the chain
+    if (!bv.lane_act[L]) ok = false;   // plain chain at its last level: b_n stored, chain done
+    else if (!ok && bv.lane_closed) bv.lane_closed[L] = 1;   // the Krylov space is exhausted
+    if (ok) {
+      bv.sup[L] = bv.su[L];
+      bv.su[L] = cdiv(make_double2(1.0, 0.0), b);
+      bv.bprev[L] = b;
+      act = true;
+    } else {
+      bv.lane_act[L] = 0;
+    }
+  }
+  if (!act) {
+    bv.su[L] = make_double2(0, 0);
+    bv.sup[L] = make_double2(0, 0);
+  }
+  // tile activity for the next step (a warp vote over the lanes)
+  unsigned any = __ballot_sync(0xffffffffu, act);
+  if (lane == 0) bv.tile_act[tile] = any != 0;
+}
+
 // sign flip of a complex value by the sign bit (no floating-point operation)
 __device__ __forceinline__ double2 flip_if(double2 x, uint32_t bit) {
   unsigned long long m = (unsigned long long)bit << 63;
@@ -318,7 +398,11 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
     }
     smul_node_out<ST, FINAL>(op, bv, it.tile, i, lane, L, grp, gflags, gfrozen, piw, in, out, acc, dot);
   }
-  if (FINAL) block_reduce_store(dot, part, it.tile, bpt);
+  if (FINAL) {
+    block_reduce_store(dot, part, it.tile, bpt);
+    if (bv.tick && last_block_of_tile(bv.tick, it.tile, bpt) && threadIdx.x < TL)
+      reduce_a_lane<false>(bv, part, bpt, bv.kstep, it.tile, threadIdx.x);
+  }
 }
 
 // ------------------------------------------------------------------------------------------------ staged S application
@@ -602,17 +686,25 @@ __device__ __forceinline__ void project_node(const OpView& op, int i, unsigned l
   int ns = s1 - s0;
   if (ns <= 1) return;
   double2 acc[9];
+#pragma unroll
   for (int l = 0; l < 9; ++l) acc[l] = make_double2(0, 0);
   for (int j = s0; j < s1; ++j) {
     int g = op.stab[j];
     bool neg = (chimask >> g) & 1ull;
     uint32_t sgm = op.sgm[g];
+#pragma unroll
     for (int l = 0; l < 9; ++l) {
-      double2 v = x[op.pi[g * 9 + l]];
+      // x[pi(l)] by selection over fixed indices: the node's values stay in registers (no dynamically indexed array)
+      const int p = op.pi[g * 9 + l];
+      double2 v = x[0];
+#pragma unroll
+      for (int q = 1; q < 9; ++q)
+        if (q == p) v = x[q];
       if (((sgm >> l) & 1u) ^ (neg ? 1u : 0u)) v = make_double2(-v.x, -v.y);
       acc[l] = cadd(acc[l], v);
     }
   }
+#pragma unroll
   for (int l = 0; l < 9; ++l) x[l] = cscale(acc[l], 1.0 / (double)ns);
 }
 
@@ -650,6 +742,8 @@ __global__ void __launch_bounds__(WPB * TL) k_lanczos_w(OpView op, BatchView bv,
     for (int l = 0; l < 9; ++l) stv(y + vix(it.tile, bv.nn, i, l) + lane, x[l]);
   }
   block_reduce_store(dot, part, it.tile, bpt);
+  if (bv.tick && last_block_of_tile(bv.tick, it.tile, bpt) && threadIdx.x < TL)
+    reduce_b_lane(bv, part, bpt, bv.kstep, 1.0e-12, it.tile, threadIdx.x, true);
 }
 
 // in-place projection of a batch vector (asr_op_project_c)
@@ -674,68 +768,16 @@ __global__ void __launch_bounds__(WPB * TL) k_project(OpView op, BatchView bv, t
 }
 
 // ------------------------------------------------------------------------------------------------ per-lane scalars
-// a_k = sum of the partials (fixed order); depth test every 4 levels from 8 (src/asr_edc.f90:121-127)
 __global__ void k_reduce_a(BatchView bv, const double2* part, int bpt, int k) {
   int tile = blockIdx.x, lane = threadIdx.x;
   if (tile >= bv.ntile || !bv.tile_act[tile]) return;
-  int L = tile * TL + lane;
-  int grp = bv.lane_group[L];
-  bv.lane_wact[L] = 0;
-  if (grp < 0 || !bv.lane_act[L]) return;
-  double2 a = make_double2(0, 0);
-  for (int q = 0; q < bpt; ++q) a = cadd(a, part[((size_t)tile * bpt + q) * TL + lane]);
-  bv.acur[L] = a;
-  bv.acoef[(size_t)L * NLMAX + k - 1] = a;
-  bv.lane_m[L] = k;
-  int nlev = bv.ginfo[grp].nlev;
-  bool go = true;
-  if (k == nlev) {
-    go = false;   // edc exits before b_k (src/asr_edc.f90:120); the plain chain still forms b_n (asr_recursion.f90:50-57)
-    if (bv.mode == ASR_MODE_PLAIN) bv.lane_wact[L] = 1;
-  } else if (bv.depth_tol > 0.0 && k >= 8 && k % 4 == 0 && bv.mode == ASR_MODE_EDC) {
-    double2 wd[NLMAX], we[NLMAX];
-    int nf = 0;
-    double2 gtry = cf_species_dev(bv.acoef + (size_t)L * NLMAX, bv.bcoef + (size_t)L * NLMAX, k, bv.lane_z[L], bv.tail, wd, we,
-                                  &nf, nullptr);
-    if (nf) atomicAdd(bv.nfall, nf);
-    if (k > 8 && cmag(csub(gtry, bv.gprev[L])) <= bv.depth_tol * cmag(gtry)) go = false;   // :123-125
-    bv.gprev[L] = gtry;
-  }
-  if (go) bv.lane_wact[L] = 1;
-  else bv.lane_act[L] = 0;
+  reduce_a_lane<true>(bv, part, bpt, k, tile, lane);
 }
 
-// b_k = sqrt(w . w); |b| < tol ends the chain; scales of the next step (u <- w / b, up <- u)
 __global__ void k_reduce_b(BatchView bv, const double2* part, int bpt, int k, double btol) {
   int tile = blockIdx.x, lane = threadIdx.x;
   if (tile >= bv.ntile) return;
-  int L = tile * TL + lane;
-  int grp = bv.lane_group[L];
-  bool act = false;
-  if (bv.tile_act[tile] && grp >= 0 && bv.lane_wact[L]) {
-    double2 ww = make_double2(0, 0);
-    for (int q = 0; q < bpt; ++q) ww = cadd(ww, part[((size_t)tile * bpt + q) * TL + lane]);
-    double2 b = bv.mode == ASR_MODE_PLAIN ? make_double2(sqrt(ww.x), 0.0) : csqrt_p(ww);
-    bv.bcoef[(size_t)L * NLMAX + k - 1] = b;
-    bool ok = bv.mode == ASR_MODE_PLAIN ? (b.x >= btol) : (cmag(b) >= btol);   // |b| < 1e-12 ends the chain
-    if (!bv.lane_act[L]) ok = false;   // plain chain at its last level: b_n stored, chain done
-    else if (!ok && bv.lane_closed) bv.lane_closed[L] = 1;   // the Krylov space is exhausted
-    if (ok) {
-      bv.sup[L] = bv.su[L];
-      bv.su[L] = cdiv(make_double2(1.0, 0.0), b);
-      bv.bprev[L] = b;
-      act = true;
-    } else {
-      bv.lane_act[L] = 0;
-    }
-  }
-  if (!act) {
-    bv.su[L] = make_double2(0, 0);
-    bv.sup[L] = make_double2(0, 0);
-  }
-  // tile activity for the next step (a warp vote over the lanes)
-  unsigned any = __ballot_sync(0xffffffffu, act);
-  if (lane == 0) bv.tile_act[tile] = any != 0;
+  reduce_b_lane(bv, part, bpt, k, btol, tile, lane, bv.tile_act[tile] != 0);
 }
 
 // final fraction of every lane: cf_species with the chosen tail (edc mode); lmap: batch lane -> output lane (-1: none)
@@ -983,10 +1025,10 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   ASR_CUDA(cudaMemcpyAsync(d_gblob.p, gblob.data(), gblob.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   ASR_CUDA(cudaMemcpyAsync(d_ginfo.p, ginfo.data(), ginfo.size() * sizeof(GroupInfo), cudaMemcpyHostToDevice, s));
   const int nlp = tpb * TL;
-  Dev<int> d_lgroup, d_act, d_wact, d_m, d_tact, d_nfall, d_tgroup;
+  Dev<int> d_lgroup, d_act, d_wact, d_m, d_tact, d_nfall, d_tgroup, d_tick;
   Dev<double2> d_a, d_b, d_gprev, d_acur, d_bprev, d_su, d_sup, d_part, d_z;
   ASR_TRY(d_lgroup.alloc(nlp)); ASR_TRY(d_act.alloc(nlp)); ASR_TRY(d_wact.alloc(nlp)); ASR_TRY(d_m.alloc(nlp));
-  ASR_TRY(d_tact.alloc(tpb)); ASR_TRY(d_nfall.alloc(1)); ASR_TRY(d_tgroup.alloc(tpb));
+  ASR_TRY(d_tact.alloc(tpb)); ASR_TRY(d_nfall.alloc(1)); ASR_TRY(d_tgroup.alloc(tpb)); ASR_TRY(d_tick.alloc(tpb));
   ASR_TRY(d_a.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_b.alloc((size_t)nlp * NLMAX));
   ASR_TRY(d_gprev.alloc(nlp)); ASR_TRY(d_acur.alloc(nlp)); ASR_TRY(d_bprev.alloc(nlp)); ASR_TRY(d_su.alloc(nlp));
   ASR_TRY(d_sup.alloc(nlp)); ASR_TRY(d_part.alloc((size_t)tpb * bpt * TL)); ASR_TRY(d_z.alloc(nlp));
@@ -1040,6 +1082,7 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
     ASR_CUDA(cudaMemcpyAsync(d_act.p, ones.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemcpyAsync(d_tact.p, tact.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemsetAsync(d_wact.p, 0, nlp * sizeof(int), s));
+    ASR_CUDA(cudaMemsetAsync(d_tick.p, 0, tpb * sizeof(int), s));
     ASR_CUDA(cudaMemsetAsync(d_m.p, 0, nlp * sizeof(int), s));
     ASR_CUDA(cudaMemsetAsync(d_a.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
     ASR_CUDA(cudaMemsetAsync(d_b.p, 0, (size_t)nlp * NLMAX * sizeof(double2), s));
@@ -1071,8 +1114,14 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
         k_proj_gather<ST><<<(unsigned)((nwarp * TL + 255) / 256), 256, 0, s>>>(op->view(), bv, U, PV, k);
         ctx->launches += 1;
       }
+      // the fused step reduces a_k in its epilogue (the tile's last block), except at the levels of the depth test, whose
+      // fraction evaluation runs in the separate reduction kernel; k_lanczos_w always reduces b_k in its epilogue
+      const bool depth_due = opt.depth_tol > 0.0 && opt.mode == ASR_MODE_EDC && k >= 8 && k % 4 == 0;
+      const bool a_in_step = fused && !depth_due;
+      BatchView bvs = bv;
+      bvs.tick = a_in_step ? d_tick.p : nullptr;
       if (ctx->profile) ASR_CUDA(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used], s));
-      ASR_TRY(step_apply<ST>(ctx, op, bv, fused, any_o, all_dunif, U, Y, nvec > 3 ? V[3].p : nullptr, nvec > 3 ? V[4].p : nullptr,
+      ASR_TRY(step_apply<ST>(ctx, op, bvs, fused, any_o, all_dunif, U, Y, nvec > 3 ? V[3].p : nullptr, nvec > 3 ? V[4].p : nullptr,
                              nvec > 5 ? V[5].p : nullptr, nvec > 5 ? V[6].p : nullptr, d_part.p, npw, gridb));
       if (ctx->profile) {
         ASR_CUDA(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used + 1], s));
@@ -1083,10 +1132,11 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
         ctx->prof_flops += (double)nt * nn * TL * (op->nslot + 1) * 81.0 * 4.0;
         ctx->prof_launches += 1;
       }
-      k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
-      k_lanczos_w<ST><<<gridb, WPB * TL, 0, s>>>(op->view(), bv, Y, U, UP, d_part.p, npw);
-      k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
-      ctx->launches += 3 + (fused ? 1 : (any_o ? 7 : (all_dunif ? 2 : 3)));
+      if (!a_in_step) k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+      BatchView bvw = bv;
+      bvw.tick = d_tick.p;
+      k_lanczos_w<ST><<<gridb, WPB * TL, 0, s>>>(op->view(), bvw, Y, U, UP, d_part.p, npw);
+      ctx->launches += (a_in_step ? 1 : 2) + (fused ? 1 : (any_o ? 7 : (all_dunif ? 2 : 3)));
     }
     ASR_CUDA(cudaGetLastError());
     if (opt.mode == ASR_MODE_EDC && d_g_out) {

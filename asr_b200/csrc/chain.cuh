@@ -53,6 +53,8 @@ struct BatchView {
   int* tile_act;           // tile has an active lane
   int* nfall;
   int* lane_closed;        // optional: 1 where |b| < 1e-12 ended the chain
+  int* tick;               // optional (ntile): per-tile tickets; set, the step and Lanczos kernels reduce a and b in the
+                           // epilogue of the tile's last block instead of separate reduction launches
 };
 
 struct RunOptions {
