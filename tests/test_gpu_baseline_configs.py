@@ -7,8 +7,8 @@
   (``chain_greens`` / ``edc_green_blk``, src/asr_class_scf.f90:966-1160, src/asr_edc.f90:237-316) evaluates a sample of
   8 energies per group that touches every 32-lane tile of the run: 2 contour nodes and 6 real energies from the band
   bottom to the top.  FP64: a and b within 1e-9 relative, G within 1e-8, equal depths.  FP32 vectors and matvec with
-  FP64 coefficients and fractions: DOS within 1e-6 of the oracle's (relative to the largest DOS of the sample), and
-  within 1e-6 of the FP64 device DOS on 1024 real energies across the band for every group.
+  FP64 coefficients and fractions: DOS within 1e-6 of the oracle's on the sample and of the FP64 device DOS at all 4096
+  real energies for every group, both relative to the largest DOS on the real axis.
 * Plain configuration (bcc A0.5B0.5, levels 4, D2h, 9 real chains of depth 12, Beer-Pettifor tail, 2000 energies): the
   DOS of every start orbital against the oracle's lanczos + terminated fraction (src/reference/asr_recursion.f90:17-58,
   src/reference/asr_terminator.f90) within 1e-8.
@@ -81,20 +81,23 @@ def test_batched_workload_fp64_matches_oracle(batched):
 
 
 def test_batched_workload_fp32_dos_within_1e6(batched):
+    """DOS errors relative to the largest DOS on the real axis (all 54 groups, all 4096 real energies of the FP64 device
+    run, which the FP64 test pins to the oracle): the FP32 form against the oracle on the sampled energies, and against
+    the FP64 device run at every real energy."""
     op, specs, sel = batched["op"], batched["specs"], batched["sel"]
-    g32 = A.chains_run(op, specs, batched["z"], "edc", 0.0, "hull", "fp32")["g"]
-    nr = len(CONTOUR_SAMPLE)
-    dos32, doso = -g32[sel[nr:]].imag / np.pi, -batched["go"][nr:].imag / np.pi
-    err_oracle = np.max(np.abs(dos32 - doso)) / np.max(np.abs(doso))
-    assert err_oracle <= 1e-6, err_oracle
-    # the whole band: every fourth energy of the 4096-point real axis, all 54 groups, FP32 against FP64 on the device
     _, _, _, z_all = S.batched_ternary_workload()
-    zr = z_all[48::4]
+    zr = z_all[48:]
     g64 = A.chains_run(op, specs, zr, "edc", 0.0, "hull", "fp64")["g"]
     g32 = A.chains_run(op, specs, zr, "edc", 0.0, "hull", "fp32")["g"]
     d64, d32 = -g64.imag / np.pi, -g32.imag / np.pi
-    err_band = np.max(np.abs(d32 - d64)) / np.max(np.abs(d64))
+    dmax = np.max(np.abs(d64))
+    err_band = np.max(np.abs(d32 - d64)) / dmax
     assert err_band <= 1e-6, err_band
+    g32s = A.chains_run(op, specs, batched["z"], "edc", 0.0, "hull", "fp32")["g"]
+    nr = len(CONTOUR_SAMPLE)
+    dos32, doso = -g32s[sel[nr:]].imag / np.pi, -batched["go"][nr:].imag / np.pi
+    err_oracle = np.max(np.abs(dos32 - doso)) / dmax
+    assert err_oracle <= 1e-6, err_oracle
 
 
 def test_plain_configuration_dos_matches_oracle():
