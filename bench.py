@@ -434,7 +434,8 @@ def contour_weights(z_all):
 
 def mixed_leg(args, A, op, specs, groups, z_all, step, stream, world):
     """The mixed-precision form (FP32 vectors and matvec, FP64 coefficients and fractions): chain-steps/s on the timed
-    slices, and its DOS error against the FP64 run over the whole real axis (all 4096 energies, all 54 groups) and the error of the contour charge M_0 per group."""
+    slices, and its DOS error against the FP64 run over the whole real axis (all 4096 energies, all 54 groups) and the
+    error of the contour charge M_0 per group."""
     import torch
     nzs = args.nz_slice
     depth = np.array([g["nlev"] for g in groups])
