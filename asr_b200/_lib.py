@@ -25,14 +25,15 @@ FP64, FP32 = 0, 1
 
 # names of every exported entry point declared in include/asr_b200.h
 EXPORTS = ["asr_version", "asr_last_error", "asr_ctx_create", "asr_ctx_destroy", "asr_ctx_sync", "asr_ctx_stats",
-           "asr_ctx_set_stream", "asr_ctx_profile", "asr_ctx_kernel_stats", "asr_ctx_launches", "asr_op_build",
-           "asr_op_free", "asr_op_dims", "asr_op_export_tables", "asr_op_set_params", "asr_op_freeze_site", "asr_op_unfreeze",
-           "asr_op_set_start", "asr_op_set_chi", "asr_op_set_class_conc", "asr_op_apply", "asr_op_rand_c", "asr_op_project_c",
-           "asr_chains_run", "asr_chains_run_dev", "asr_cf_eval", "asr_cf_adjoint",
-    "asr_chains_adjoint", "asr_cf_eval_noalloc", "asr_ed3_blocks", "asr_supercell_build", "asr_supercell_free",
-           "asr_supercell_apply", "asr_kpm_moments", "asr_kpm_dos", "asr_sro_layout", "asr_gauss_legendre", "asr_contour_nodes",
-           "asr_contour_nodes_closed", "asr_contour_nodes_fermi", "asr_contour_moment", "asr_op_build_targets",
-           "asr_chains_proj", "asr_epi_blocks", "asr_autotune", "asr_op_tuning", "asr_op_set_tuning"]
+           "asr_ctx_set_stream", "asr_ctx_profile", "asr_ctx_kernel_stats", "asr_ctx_kernel_stats_kind",
+           "asr_ctx_launches", "asr_op_build", "asr_op_free", "asr_op_dims", "asr_op_export_tables",
+           "asr_op_set_params", "asr_op_freeze_site", "asr_op_unfreeze", "asr_op_set_start", "asr_op_set_chi",
+           "asr_op_set_class_conc", "asr_op_apply", "asr_op_rand_c", "asr_op_project_c", "asr_chains_run",
+           "asr_chains_run_dev", "asr_cf_eval", "asr_cf_adjoint", "asr_chains_adjoint", "asr_cf_eval_noalloc",
+           "asr_ed3_blocks", "asr_supercell_build", "asr_supercell_free", "asr_supercell_apply", "asr_kpm_moments",
+           "asr_kpm_dos", "asr_sro_layout", "asr_gauss_legendre", "asr_contour_nodes", "asr_contour_nodes_closed",
+           "asr_contour_nodes_fermi", "asr_contour_moment", "asr_op_build_targets", "asr_chains_proj",
+           "asr_epi_blocks", "asr_autotune", "asr_op_tuning", "asr_op_set_tuning"]
 
 
 class ChainGroup(C.Structure):
@@ -70,6 +71,7 @@ def lib():
     L.asr_ctx_set_stream.argtypes = [vp, vp]
     L.asr_ctx_profile.argtypes = [vp, C.c_int]
     L.asr_ctx_kernel_stats.argtypes = [vp, d_p, i64_p, d_p, d_p]
+    L.asr_ctx_kernel_stats_kind.argtypes = [vp, C.c_int, d_p, i64_p, d_p, d_p]
     L.asr_ctx_launches.argtypes = [vp, i64_p]
     L.asr_op_build.argtypes = [vp, C.c_int, i_p, i_p, C.c_int, i_p, i_p, C.c_int, d_p, C.c_int, i_p, i_p, C.c_int, d_p, C.c_int,
                                C.c_int, C.c_int, i_p, i_p, d_p, C.c_int, C.c_int, d_p, C.POINTER(vp)]

@@ -61,13 +61,18 @@ class Context:
         """Run on the caller's CUDA stream (e.g. ``torch.cuda.current_stream().cuda_stream``); None: the own stream."""
         check(lib().asr_ctx_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
+    KERNEL_KINDS = {"step": 0, "lanczos": 1, "kpm": 2, "adjoint": 3}
+
     def profile(self, on: bool):
-        """Start (and clear) or stop the per-launch event timing of the chain step kernel."""
+        """Start (and clear) or stop the per-launch event timing of the hot kernels."""
         check(lib().asr_ctx_profile(self.h, int(bool(on))))
 
-    def kernel_stats(self) -> dict:
+    def kernel_stats(self, kind: str = "step") -> dict:
+        """Summed device time, launches and algorithmic bytes and flops of one kernel kind since ``profile(True)``:
+        'step' (chain step operator), 'lanczos' (Lanczos update), 'kpm' (Chebyshev step), 'adjoint' (reverse level)."""
         ms, n, by, fl = C.c_double(), C.c_int64(), C.c_double(), C.c_double()
-        check(lib().asr_ctx_kernel_stats(self.h, C.byref(ms), C.byref(n), C.byref(by), C.byref(fl)))
+        check(lib().asr_ctx_kernel_stats_kind(self.h, self.KERNEL_KINDS[kind], C.byref(ms), C.byref(n), C.byref(by),
+                                              C.byref(fl)))
         return dict(ms=ms.value, launches=n.value, bytes=by.value, flops=fl.value)
 
     def launches(self) -> int:

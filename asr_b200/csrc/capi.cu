@@ -266,7 +266,7 @@ static int drain_events(asr_ctx* ctx) {
   for (int q = 0; q < ctx->ev_used; ++q) {
     float ms = 0.f;
     ASR_CUDA(cudaEventElapsedTime(&ms, ctx->ev_pool[2 * q], ctx->ev_pool[2 * q + 1]));
-    ctx->prof_ms += ms;
+    ctx->prof[ctx->ev_kind[q]].ms += ms;
   }
   ctx->ev_used = 0;
   return ASR_OK;
@@ -276,7 +276,8 @@ int asr_ctx_profile(asr_ctx* ctx, int on) {
   if (!ctx) { set_error("asr_ctx_profile: null context"); return ASR_EINVAL; }
   ASR_TRY(drain_events(ctx));
   ctx->profile = on;
-  if (on) { ctx->prof_ms = 0.0; ctx->prof_bytes = 0.0; ctx->prof_flops = 0.0; ctx->prof_launches = 0; }
+  if (on)
+    for (auto& p : ctx->prof) p = asr_ctx::ProfStat();
   return ASR_OK;
 }
 
@@ -286,14 +287,20 @@ int asr_ctx_launches(asr_ctx* ctx, int64_t* launches) {
   return ASR_OK;
 }
 
-int asr_ctx_kernel_stats(asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops) {
+int asr_ctx_kernel_stats_kind(asr_ctx* ctx, int kind, double* ms, int64_t* launches, double* bytes, double* flops) {
   if (!ctx) { set_error("asr_ctx_kernel_stats: null context"); return ASR_EINVAL; }
+  if (kind < 0 || kind >= ASR_KERNEL_KINDS) { set_error("asr_ctx_kernel_stats_kind: kind %d", kind); return ASR_EINVAL; }
   ASR_TRY(drain_events(ctx));
-  if (ms) *ms = ctx->prof_ms;
-  if (launches) *launches = ctx->prof_launches;
-  if (bytes) *bytes = ctx->prof_bytes;
-  if (flops) *flops = ctx->prof_flops;
+  const asr_ctx::ProfStat& p = ctx->prof[kind];
+  if (ms) *ms = p.ms;
+  if (launches) *launches = p.launches;
+  if (bytes) *bytes = p.bytes;
+  if (flops) *flops = p.flops;
   return ASR_OK;
+}
+
+int asr_ctx_kernel_stats(asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops) {
+  return asr_ctx_kernel_stats_kind(ctx, ASR_KERNEL_STEP, ms, launches, bytes, flops);
 }
 
 int asr_ctx_sync(asr_ctx* ctx) {

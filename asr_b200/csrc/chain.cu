@@ -1097,13 +1097,6 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
     k_init<ST><<<std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256), 256, 0, s>>>(bv, V[1].p, V[0].p);
     ctx->launches += 2;
     const int gridb = nt * bpt;
-    if (ctx->profile) {   // event pairs stay pending until asr_ctx_kernel_stats reads them (no synchronisation here)
-      while ((int)ctx->ev_pool.size() < 2 * (ctx->ev_used + kmax)) {
-        cudaEvent_t e;
-        ASR_CUDA(cudaEventCreate(&e));
-        ctx->ev_pool.push_back(e);
-      }
-    }
     for (int k = 1; k <= kmax; ++k) {
       bv.kstep = k;
       T2* U = V[k % 3].p;
@@ -1120,22 +1113,22 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
       const bool a_in_step = fused && !depth_due;
       BatchView bvs = bv;
       bvs.tick = a_in_step ? d_tick.p : nullptr;
-      if (ctx->profile) ASR_CUDA(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used], s));
+      // timed regions (asr_ctx_profile): event pairs stay pending until the statistics are read (no synchronisation)
+      int ps = ctx->prof_start(s);
       ASR_TRY(step_apply<ST>(ctx, op, bvs, fused, any_o, all_dunif, U, Y, nvec > 3 ? V[3].p : nullptr, nvec > 3 ? V[4].p : nullptr,
                              nvec > 5 ? V[5].p : nullptr, nvec > 5 ? V[6].p : nullptr, d_part.p, npw, gridb));
-      if (ctx->profile) {
-        ASR_CUDA(cudaEventRecord(ctx->ev_pool[2 * ctx->ev_used + 1], s));
-        ++ctx->ev_used;
-        // algorithmic traffic of one operator pass: read U and write Y per (node, lane), plus the node tables per tile
+      {   // algorithmic traffic of one operator pass: read U and write Y per (node, lane), plus the node tables per tile
         const double tab = (double)op->nslot * 5 + (double)op->nsmax * 5 + 8 + 8 + 4;
-        ctx->prof_bytes += (double)nt * nn * (2.0 * 9 * TL * sizeof(T2) + tab);
-        ctx->prof_flops += (double)nt * nn * TL * (op->nslot + 1) * 81.0 * 4.0;
-        ctx->prof_launches += 1;
+        ctx->prof_stop(s, ps, ASR_KERNEL_STEP, (double)nt * nn * (2.0 * 9 * TL * sizeof(T2) + tab),
+                       (double)nt * nn * TL * (op->nslot + 1) * 81.0 * 4.0);
       }
       if (!a_in_step) k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
       BatchView bvw = bv;
       bvw.tick = d_tick.p;
+      ps = ctx->prof_start(s);
       k_lanczos_w<ST><<<gridb, WPB * TL, 0, s>>>(op->view(), bvw, Y, U, UP, d_part.p, npw);
+      // read y, u, u', write w per (node, lane); about 30 flops per complex element (scaled updates, projection, dot)
+      ctx->prof_stop(s, ps, ASR_KERNEL_LANCZOS, (double)nt * nn * 4.0 * 9 * TL * sizeof(T2), (double)nt * nn * TL * 9 * 30.0);
       ctx->launches += (a_in_step ? 1 : 2) + (fused ? 1 : (any_o ? 7 : (all_dunif ? 2 : 3)));
     }
     ASR_CUDA(cudaGetLastError());
@@ -1689,6 +1682,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         T2* ubn = UB[(k + 1) % 3];
         T2* ubk = UB[k % 3];
         T2* ubp = UB[(k + 2) % 3];
+        const int ps = ctx->prof_start(s);
         k_dot<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, ubn, XS(q + 2), d_part.p, npw);
         k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d1.p);
         k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 0);
@@ -1706,6 +1700,10 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
                                                       d_gpart.p);
         k_adj_gsum<<<nt, 128, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
         ASR_CUDA(cudaMemsetAsync(ubn, 0, cpy, s));   // becomes ubar_{k-2}
+        // one reverse level: 26 vector streams per (node, lane) over its kernels (dot 2, w-bar 5, y-bar 4, S application
+        // 2, combine 3, u-bar 5, parameter gradient 4, clear 1); flops of its one S application
+        ctx->prof_stop(s, ps, ASR_KERNEL_ADJOINT, (double)nt * nn * 26.0 * 9 * TL * sizeof(T2),
+                       (double)nt * nn * TL * (op->nslot + 1) * 81.0 * 4.0);
       }
     }
     ASR_CUDA(cudaGetLastError());

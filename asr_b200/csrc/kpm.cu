@@ -393,6 +393,7 @@ int kpm_run(asr_ctx* ctx, asr_supercell* sc, double cen, double scl, int nmom, i
       const ST* tin = (k == 0) ? ta : tb;
       const ST* told = (k == 0) ? nullptr : ta;
       ST* tout = (k == 0) ? tb : tc;
+      const int ps = ctx->prof_start(s);
       if (scaled) {
         // <r|t> is needed for every step without doubling, and for mu_1 (step 0) with it
         if (!doubling || k == 0)
@@ -406,6 +407,13 @@ int kpm_run(asr_ctx* ctx, asr_supercell* sc, double cen, double scl, int nmom, i
         k_h<ST><<<grid, KSITES * KV, smem, s>>>(S, blocks, tin, true, W2.p);    // o h t
         k_h<ST><<<grid, KSITES * KV, smem, s>>>(S, blocks, W2.p, false, W3.p);
         k_cheb_comb<ST><<<grid, KSITES * KV, 0, s>>>(S, tin, W1.p, W3.p, told, tout, cen, isc, k == 0, seed, v0 + vb, part.p);
+      }
+      {   // algorithmic work of one Chebyshev step: read t_k and t_{k-1}, write t_{k+1}, one species byte per site; flops
+          // 2 x 81 x (1 + slots) per site and vector per S application (one for o = 0, three for the general operator)
+        const double sapp = general ? 3.0 : 1.0;
+        const double streams = general ? 9.0 : 3.0;
+        ctx->prof_stop(s, ps, ASR_KERNEL_KPM, (double)n * (KV * streams * 9 * sizeof(ST) + 1.0),
+                       sapp * (double)n * KV * 2.0 * 81.0 * (1 + sc->ns));
       }
       k_kpm_reduce<<<1, KV, 0, s>>>(part.p, grid, red.p + (size_t)k * KV * 3);
       if (k > 0) { ST* t_ = ta; ta = tb; tb = tc; tc = t_; }

@@ -15,12 +15,38 @@ struct asr_ctx {
   int64_t nchain = 0, nlev = 0, nfall = 0;
   int64_t launches = 0;   // kernels launched by this context
   int* d_err = nullptr;   // device error word
-  // kernel timing (asr_ctx_profile)
+  // kernel timing (asr_ctx_profile): device time, launches and algorithmic work per kernel kind (ASR_KERNEL_*)
+  struct ProfStat {
+    double ms = 0.0, bytes = 0.0, flops = 0.0;
+    int64_t launches = 0;
+  };
   int profile = 0;
-  double prof_ms = 0.0, prof_bytes = 0.0, prof_flops = 0.0;
-  int64_t prof_launches = 0;
+  ProfStat prof[ASR_KERNEL_KINDS];
   std::vector<cudaEvent_t> ev_pool;   // pairs (start, end) of the timed launches
+  std::vector<int> ev_kind;           // kernel kind of every recorded pair
   int ev_used = 0;                    // pairs recorded and not yet read
+  // starts a timed region on stream s (returns its pair index, -1 when profiling is off); no synchronisation
+  int prof_start(cudaStream_t s) {
+    if (!profile) return -1;
+    while ((int)ev_pool.size() < 2 * (ev_used + 1)) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+      ev_pool.push_back(e);
+    }
+    if ((int)ev_kind.size() < ev_used + 1) ev_kind.resize(ev_used + 1);
+    if (cudaEventRecord(ev_pool[2 * ev_used], s) != cudaSuccess) return -1;
+    return ev_used;
+  }
+  // ends the region `slot` of prof_start as one launch of `kind` with the given algorithmic bytes and flops
+  void prof_stop(cudaStream_t s, int slot, int kind, double bytes, double flops) {
+    if (slot < 0 || slot != ev_used) return;
+    if (cudaEventRecord(ev_pool[2 * slot + 1], s) != cudaSuccess) return;
+    ev_kind[slot] = kind;
+    ++ev_used;
+    prof[kind].bytes += bytes;
+    prof[kind].flops += flops;
+    prof[kind].launches += 1;
+  }
   unsigned char* cf_scratch = nullptr;   // device address of asr_cf_eval_noalloc's static array (resolved on first use)
 };
 

@@ -25,9 +25,40 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NZ_SLICE = 192
-# DRAM bytes (read + write) per launch of the step kernel from one ncu capture of a 16-tile launch, and the algorithmic
-# bytes of that launch; traffic is scaled to the bench's mean launch
-NCU_STEP_TRAFFIC = {"fp64": (3.30e9, 16 * 20969 * (2 * 4608.0 + 18 * 5 + 3 * 5 + 20))}
+# DRAM bytes (read + write) per launch of the step kernel from one ncu capture (64-energy slice of this workload), the
+# algorithmic bytes of that launch and what was captured, per (precision, link-gather variant); traffic is scaled to the
+# bench's mean launch
+_TAB = 18 * 5 + 3 * 5 + 20
+NCU_STEP_TRAFFIC = {
+    ("fp64", "fixed-offset"): (3.171e9, 16 * 20969 * (2 * 4608.0 + _TAB),
+                               "ncu capture of k_smul<double,1,1,1> (fixed-offset link gathers, a_k epilogue) at 16 tiles"),
+    ("fp32", "fixed-offset"): (0.770e9, 8 * 20969 * (2 * 2304.0 + _TAB),
+                               "ncu capture of k_smul<float,1,1,1> (fixed-offset link gathers, a_k epilogue) at 8 tiles"),
+    ("fp64", "general"): (3.30e9, 16 * 20969 * (2 * 4608.0 + _TAB),
+                          "ncu capture of the general-link k_smul<double,1,1,0> at 16 tiles (before the a_k epilogue)"),
+}
+
+
+def roof(st, hbm_peak, pipe_peak=None):
+    """Roofline entry of one kernel kind from its CUDA-event statistics: achieved algorithmic GB/s per launch and its
+    fraction of the HBM peak, TFLOP/s and its fraction of the matching measured pipe peak."""
+    if not st or st["launches"] == 0:
+        return None
+    per = st["ms"] / st["launches"]
+    gbs = st["bytes"] / st["launches"] / (per / 1e3) / 1e9
+    tf = st["flops"] / st["launches"] / (per / 1e3) / 1e12
+    return {"launches": st["launches"], "per_launch_ms": per, "achieved_gbs": gbs, "hbm_frac": gbs / hbm_peak,
+            "tflops": tf, "pipe_frac": (tf / pipe_peak) if pipe_peak else None}
+
+
+def hbm_peak_of():
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        peaks = {}
+    if "hbm_gbs" in peaks:
+        return float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    return 6650.0, "fallback 6650 GB/s (an earlier B200 copy measurement; no MEASURED_PEAKS.json)"
 
 
 def parse():
@@ -159,12 +190,20 @@ def run_reference(args):
     print(json.dumps(line))
 
 
-def fp64_peak_tflops(torch):
+def fp32_peak_tflops(torch):
+    """Measured FP32 matrix throughput (cuBLAS SGEMM 8192^3 without TF32, best of 3), the denominator of the FP32 pipe
+    fractions."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    return fp64_peak_tflops(torch, torch.float32)
+
+
+def fp64_peak_tflops(torch, dtype=None):
     """Measured FP64 matrix throughput of this GPU (cuBLAS DGEMM 8192^3, best of 3), the denominator of the FP64
     fraction of the chain step."""
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    dtype = dtype or torch.float64
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
     c = a @ b
     best = 1e30
     for _ in range(3):
@@ -199,16 +238,21 @@ def kpm_leg(torch):
            "alpha1_achieved": float(aout[0, 1])}
     sc.kpm_moments(cen, scl, 64, nvec, seed=5, precision="fp32")
     torch.cuda.synchronize()
+    stats = {}
     for prec in ("fp32", "fp64"):
+        sc.ctx.profile(True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         mu = sc.kpm_moments(cen, scl, nmom, nvec, seed=5, precision=prec)
         e1.record()
         torch.cuda.synchronize()
+        sc.ctx.profile(False)
+        stats[prec] = sc.ctx.kernel_stats("kpm")
         ms = e0.elapsed_time(e1)
         out[prec] = {"ms": ms, "matvec_rows_per_s": (nmom // 2) * nvec * sc.dim / (ms / 1000.0),
                      "tflops": (nmom // 2) * nvec * sc.n * 2.0 * 81 * (1 + sc.ns) / (ms / 1000.0) / 1e12}
         out["mu_" + prec] = mu
+    out["kernel_stats"] = stats
     m32, m64 = out.pop("mu_fp32"), out.pop("mu_fp64")
     egrid = np.linspace(cen - 0.99 * scl, cen + 0.99 * scl, 2000)
     r32, r64 = kpm.kpm_dos(m32, cen, scl, egrid), kpm.kpm_dos(m64, cen, scl, egrid)
@@ -480,11 +524,14 @@ def adjoint_leg(args, A, op, specs, groups, z_all, stream):
     for prec in ("fp64", "fp32"):
         A.chains_adjoint(op, specs, zc[:8], w[:8], "hull", prec, True)
         torch.cuda.synchronize()
+        op.ctx.profile(True)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         _, grads[prec] = A.chains_adjoint(op, specs, zc, w, "hull", prec, True)
         e1.record(stream)
         torch.cuda.synchronize()
+        op.ctx.profile(False)
+        kst = op.ctx.kernel_stats("adjoint")
         msa = e0.elapsed_time(e1)
         e0.record(stream)
         A.chains_run(op, specs, zc, "edc", 0.0, "hull", prec)
@@ -492,7 +539,8 @@ def adjoint_leg(args, A, op, specs, groups, z_all, stream):
         torch.cuda.synchronize()
         msf = e0.elapsed_time(e1)
         out[prec] = {"value": steps_adj / (msa / 1000.0), "forward_same_energies": steps_adj / (msf / 1000.0),
-                     "adjoint_over_forward_time": msa / msf, "gradient_norm": float(np.linalg.norm(grads[prec]))}
+                     "adjoint_over_forward_time": msa / msf, "gradient_norm": float(np.linalg.norm(grads[prec])),
+                     "reverse_level_stats": kst, "reverse_share": kst["ms"] / msa}
     out["unit"] = "chain-steps/s (forward + reverse, checkpoints every sqrt(depth) levels)"
     out["energies"], out["groups"] = int(zc.shape[0]), len(specs)
     out["fp32_gradient_error"] = float(np.max(np.abs(grads["fp32"] - grads["fp64"])) / np.max(np.abs(grads["fp64"])))
@@ -512,6 +560,7 @@ def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
     if "adjoint" in want:
         out["adjoint"] = adjoint_leg(args, A, op, specs, groups, z_all, stream)
     out["fp64_peak_tflops"] = fp64_peak_tflops(torch)
+    out["fp32_peak_tflops"] = fp32_peak_tflops(torch)
     if "kpm" in want:
         out["kpm"] = kpm_leg(torch)
     if "plain" in want:
@@ -602,7 +651,8 @@ def main():
         dist.barrier()
     ms = e0.elapsed_time(e1)
     launches = ctx.launches() - launches0
-    ks = ctx.kernel_stats()
+    ks = ctx.kernel_stats("step")
+    kl = ctx.kernel_stats("lanczos")
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -640,23 +690,29 @@ def main():
     d2h = len(specs) * nzs * (16 + 4)
 
     if rank == 0:
-        peaks = {}
-        try:
-            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        except Exception:
-            pass
-        if "hbm_gbs" in peaks:
-            hbm_peak, peak_source = float(peaks["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
-        else:
-            hbm_peak, peak_source = 6650.0, "fallback 6650 GB/s (an earlier B200 copy measurement; no MEASURED_PEAKS.json)"
+        hbm_peak, peak_source = hbm_peak_of()
         per_launch_ms = ks["ms"] / max(ks["launches"], 1)
         achieved = (ks["bytes"] / max(ks["launches"], 1)) / (per_launch_ms / 1000.0) / 1e9
         tflops = (ks["flops"] / max(ks["launches"], 1)) / (per_launch_ms / 1000.0) / 1e12
         cpu = cpu_baseline(case, fl, groups, z_all) if args.cpu_sample else None
-        traffic = None
-        if args.precision in NCU_STEP_TRAFFIC:
-            meas, alg = NCU_STEP_TRAFFIC[args.precision]
+        traffic, traffic_source = None, None
+        if (args.precision, tune["link_gather"]) in NCU_STEP_TRAFFIC:
+            meas, alg, traffic_source = NCU_STEP_TRAFFIC[(args.precision, tune["link_gather"])]
             traffic = meas * (ks["bytes"] / max(ks["launches"], 1)) / alg
+            traffic_source += ", scaled to the mean launch"
+        # every timed kernel kind: the chain step and the Lanczos update of the timed region, the KPM Chebyshev step and
+        # the adjoint's reverse level of the legs
+        pipe = None
+        if legs:
+            pipe = legs["fp64_peak_tflops"] if args.precision == "fp64" else legs["fp32_peak_tflops"]
+        rooflines = {"step": roof(ks, hbm_peak, pipe), "lanczos": roof(kl, hbm_peak, pipe)}
+        if legs and "kpm" in legs:
+            for prec, st in legs["kpm"]["kernel_stats"].items():
+                rooflines["kpm_" + prec] = roof(st, hbm_peak, legs[prec + "_peak_tflops"])
+        if legs and "adjoint" in legs:
+            for prec in ("fp64", "fp32"):
+                rooflines["adjoint_level_" + prec] = roof(legs["adjoint"][prec]["reverse_level_stats"], hbm_peak,
+                                                          legs[prec + "_peak_tflops"])
         line = {
             "metric": "chain-steps/s (batched energy-dependent chains, fcc ternary, 54 groups, depths 16-28)",
             "value": value, "unit": "chain-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -674,14 +730,16 @@ def main():
                        "precision": args.precision},
             "e2e": {"value": e2e, "unit": "chain-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                         "traffic": traffic,
-                         "traffic_source": "ncu capture of the general-link k_smul<double,1,1> at 16 tiles, scaled to the "
-                                           "mean launch" if traffic is not None else None,
+                         "traffic": traffic, "traffic_source": traffic_source,
                          "kernel": "chain step operator (k_smul, fused S + diagonal + dot; %s link gathers)" % tune["link_gather"],
                          "per_launch_ms": per_launch_ms, "launches": ks["launches"], "fp64_tflops": tflops,
                          "share_of_step": ks["ms"] / ms, "peak_source": peak_source,
                          "fp64_frac": (tflops / legs["fp64_peak_tflops"]) if legs else None,
-                         "fp64_peak_source": "cuBLAS DGEMM 8192^3 measured in this run"},
+                         "fp64_peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                         "kernels": rooflines,
+                         "kernels_basis": "CUDA events around every launch of each kind in its timed region; achieved = "
+                                          "algorithmic bytes / time, hbm_frac against the HBM peak above, pipe_frac "
+                                          "against the cuBLAS GEMM of the kernel's precision measured in this run"},
             "cpu_baseline": cpu,
             "legs": legs,
             "gpu_launches": int(launches),

@@ -54,11 +54,19 @@ int asr_ctx_stats(const asr_ctx* ctx, int64_t* nchain, int64_t* nlev, int64_t* n
 /* run on the caller's CUDA stream (a cudaStream_t, e.g. the current stream of a PyTorch process); NULL: the context's own.
  * No counterpart in the reference (which has no device). */
 int asr_ctx_set_stream(asr_ctx* ctx, void* stream);
-/* per-launch CUDA-event timing of the chain step kernel (the timer buckets of src/asr_runstats.f90:1-96 on the device):
+/* per-launch CUDA-event timing of the hot kernels (the timer buckets of src/asr_runstats.f90:1-96 on the device):
  * on = 1 starts (and clears) it; asr_ctx_kernel_stats returns the summed device time, the launches and the algorithmic
- * bytes and flops of those launches */
+ * bytes and flops of the chain step operator's launches, asr_ctx_kernel_stats_kind the same for one kernel kind */
+enum {
+  ASR_KERNEL_STEP = 0,      /* chain step operator (S application, diagonal terms, a-dot) */
+  ASR_KERNEL_LANCZOS = 1,   /* Lanczos update w = y - a u - b u', projection, b-dot */
+  ASR_KERNEL_KPM = 2,       /* KPM Chebyshev step (block matvec, recurrence, moments) */
+  ASR_KERNEL_ADJOINT = 3,   /* one level of the adjoint's reverse sweep */
+  ASR_KERNEL_KINDS = 4
+};
 int asr_ctx_profile(asr_ctx* ctx, int on);
 int asr_ctx_kernel_stats(asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops);
+int asr_ctx_kernel_stats_kind(asr_ctx* ctx, int kind, double* ms, int64_t* launches, double* bytes, double* flops);
 /* number of kernels this context has launched (all kinds) */
 int asr_ctx_launches(asr_ctx* ctx, int64_t* launches);
 
