@@ -27,13 +27,14 @@ FP64, FP32 = 0, 1
 EXPORTS = ["asr_version", "asr_last_error", "asr_ctx_create", "asr_ctx_destroy", "asr_ctx_sync", "asr_ctx_stats",
            "asr_ctx_set_stream", "asr_ctx_profile", "asr_ctx_kernel_stats", "asr_ctx_kernel_stats_kind",
            "asr_ctx_launches", "asr_op_build", "asr_op_free", "asr_op_dims", "asr_op_export_tables",
-           "asr_op_set_params", "asr_op_freeze_site", "asr_op_unfreeze", "asr_op_set_start", "asr_op_set_chi",
-           "asr_op_set_class_conc", "asr_op_apply", "asr_op_rand_c", "asr_op_project_c", "asr_chains_run",
-           "asr_chains_run_dev", "asr_cf_eval", "asr_cf_adjoint", "asr_chains_adjoint", "asr_cf_eval_noalloc",
-           "asr_ed3_blocks", "asr_supercell_build", "asr_supercell_free", "asr_supercell_apply", "asr_kpm_moments",
-           "asr_kpm_dos", "asr_sro_layout", "asr_gauss_legendre", "asr_contour_nodes", "asr_contour_nodes_closed",
-           "asr_contour_nodes_fermi", "asr_contour_moment", "asr_op_build_targets", "asr_chains_proj",
-           "asr_epi_blocks", "asr_autotune", "asr_op_tuning", "asr_op_set_tuning"]
+           "asr_op_set_params", "asr_op_freeze_site", "asr_op_freeze_any", "asr_op_unfreeze", "asr_op_set_start",
+           "asr_op_set_chi", "asr_op_set_class_conc", "asr_op_apply", "asr_op_rand_c", "asr_op_project_c",
+           "asr_chains_run", "asr_chains_run_dev", "asr_cf_eval", "asr_cf_adjoint", "asr_chains_adjoint",
+           "asr_cf_eval_noalloc", "asr_ed3_blocks", "asr_supercell_build", "asr_supercell_free",
+           "asr_supercell_apply", "asr_kpm_moments", "asr_kpm_dos", "asr_sro_layout", "asr_gauss_legendre",
+           "asr_contour_nodes", "asr_contour_nodes_closed", "asr_contour_nodes_fermi", "asr_contour_moment",
+           "asr_op_build_targets", "asr_chains_proj", "asr_epi_blocks", "asr_autotune", "asr_op_tuning",
+           "asr_op_set_tuning", "asr_op_hp_c", "asr_dos_final"]
 
 
 class ChainGroup(C.Structure):
@@ -81,6 +82,10 @@ def lib():
     L.asr_op_export_tables.argtypes = [vp] + [i_p] * 8 + [d_p, d_p, i_p, i_p]
     L.asr_op_set_params.argtypes = [vp, d_p, d_p, d_p, d_p]
     L.asr_op_freeze_site.argtypes = [vp, C.c_int, C.c_int]
+    L.asr_op_freeze_any.argtypes = [vp, C.c_int, C.c_int, i_p]
+    L.asr_op_hp_c.argtypes = [vp, d_p, d_p, C.c_int]
+    L.asr_dos_final.argtypes = [vp, vp, C.POINTER(ChainGroup), C.c_int, i_p, i_p, i_p, d_p, C.c_int, C.c_int, C.c_double,
+                                C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, C.c_int, d_p, d_p]
     L.asr_op_unfreeze.argtypes = [vp]
     L.asr_op_set_start.argtypes = [vp, C.c_int]
     L.asr_op_set_chi.argtypes = [vp, d_p]

@@ -149,10 +149,26 @@ class AugclsOp:
         self.params = dict(c=args[0], d=args[1], o=args[2], e=args[3])
 
     def freeze_site(self, site: int, sp: int):
-        """``augcls_freeze_site`` / ``augcls_freeze_any``."""
+        """``augcls_freeze_site`` (src/asr_augcls.f90:129-142): freeze the (non-flippable) site to species sp of its
+        class; at the start site sp must belong to the start node's class."""
         check(lib().asr_op_freeze_site(self.h, site, sp))
 
-    freeze_any = freeze_site
+    def freeze_any(self, site: int, sp: int) -> int:
+        """``augcls_freeze_any`` (src/asr_augcls.f90:147-161): freeze the site to any species index 1..nsp (a path species,
+        the partner of a pair); returns the number of nodes on the site (0: outside the node set)."""
+        n = C.c_int(0)
+        check(lib().asr_op_freeze_any(self.h, site, sp, C.byref(n)))
+        return n.value
+
+    def hp_c(self, x):
+        """``augcls_hp_c`` (src/asr_augcls.f90:301-320): h x = (c + D S D) x for complex x (dim,) or (dim, nvec) in
+        normalised coordinates."""
+        x = np.asarray(x, np.complex128)
+        one = x.ndim == 1
+        xs = np.asfortranarray(x.reshape(self.dim, -1))
+        y = np.zeros_like(xs, order="F")
+        check(lib().asr_op_hp_c(self.h, _pd(xs), _pd(y), xs.shape[1]))
+        return y[:, 0] if one else y
 
     def unfreeze(self):
         check(lib().asr_op_unfreeze(self.h))

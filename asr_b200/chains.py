@@ -132,6 +132,25 @@ def ed3_blocks(op: AugclsOp, groups, z, depth_tol: float = 0.0, tail: str = "hul
     return out
 
 
+def dos_final(op: AugclsOp, specs, comp, spin, lorb, worb, ncomp: int, nspin: int, emin: float, emax: float, eta: float,
+              ndos: int, depth_tol: float = 0.0, tail: str = "hull", precision: str = "fp64"):
+    """``dos_final`` (src/asr_class_scf.f90:1912-1931): the l-resolved DOS at ndos uniform real energies on [emin, emax]
+    (Im z = eta) from the chains of every group.  comp, spin (1-based) and lorb (0 s, 1 p, 2 d) per group, worb the
+    orbital-group size of its start orbital.  Returns (e (ndos,), edos (ndos, 3, ncomp, nspin))."""
+    ng = len(specs)
+    arr, keep = _groups(specs)
+    comp, spin, lorb = (np.ascontiguousarray(x, np.int32) for x in (comp, spin, lorb))
+    worb = np.ascontiguousarray(worb, np.float64)
+    if not (comp.size == spin.size == lorb.size == worb.size == ng):
+        raise ValueError("dos_final: one component, spin, l and weight per group")
+    e = np.zeros(ndos)
+    edos = np.zeros((ndos, 3, ncomp, nspin), order="F")
+    check(lib().asr_dos_final(op.ctx.h, op.h, arr, ng, _pi(comp), _pi(spin), _pi(lorb), _pd(worb), int(ncomp), int(nspin),
+                              float(emin), float(emax), float(eta), int(ndos), float(depth_tol), _lib.TAILS[tail],
+                              PREC[precision], _pd(e), _pd(edos)))
+    return e, edos
+
+
 def chains_run_device(op: AugclsOp, specs, z_dev, g_dev, nz: int, mode: str = "edc", depth_tol: float = 0.0, tail: str = "hull",
                       precision: str = "fp64", project: bool = True):
     """Device-resident form: z_dev / g_dev are device pointers (ints, e.g. torch tensor data_ptr()) of complex128 arrays;

@@ -468,28 +468,65 @@ int asr_op_set_params(asr_op* op, const double* c, const double* d, const double
   return ASR_OK;
 }
 
-int asr_op_freeze_site(asr_op* op, int site, int sp) {
-  if (!op) { set_error("augcls_freeze_site: null operator"); return ASR_EINVAL; }
-  if (sp < 1 || sp > op->nsp) { set_error("augcls_freeze_any: species index out of range"); return ASR_EINVAL; }
-  ASR_ON_DEVICE(op->ctx->device);
+// the node tables of a freeze, copied to the host once per operator (they do not change after the build)
+static int freeze_tables(asr_op* op) {
+  if (!op->site_h.empty()) return ASR_OK;
   cudaStream_t s = op->ctx->stream;
   const size_t nn = op->nn, nsm = op->nsmax;
   std::vector<int> st(nn), fr(nsm * nn);
-  std::vector<int8_t> ls(nn);
+  std::vector<int8_t> ls(nn), nc(1);
   ASR_CUDA(cudaMemcpyAsync(st.data(), op->d_site, nn * sizeof(int), cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaMemcpyAsync(fr.data(), op->d_flipr, fr.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaMemcpyAsync(ls.data(), op->d_lst, nn, cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaMemcpyAsync(nc.data(), op->d_ncl, 1, cudaMemcpyDeviceToHost, s));   // device node 0 is the start node
   ASR_CUDA(cudaStreamSynchronize(s));
-  for (size_t i = 0; i < nn; ++i) {
-    if (st[i] != site) continue;
-    int nz = 0;
-    for (size_t k = 0; k < nsm; ++k) if (fr[k + nsm * i] >= 0) ++nz;
-    if (ls[i] != 0 || nz > 1) { set_error("augcls_freeze_site: the frozen site was flippable"); return ASR_EINVAL; }
-    op->frozen_h[i] = (int8_t)sp;
-  }
-  ASR_CUDA(cudaMemcpyAsync(op->d_frozen, op->frozen_h.data(), nn, cudaMemcpyHostToDevice, s));
-  ASR_CUDA(cudaStreamSynchronize(s));
+  std::vector<int8_t> nf(nn, 0);
+  for (size_t i = 0; i < nn; ++i)
+    for (size_t k = 0; k < nsm; ++k) if (fr[k + nsm * i] >= 0) ++nf[i];
+  op->site_h.swap(st);
+  op->lst_h.swap(ls);
+  op->nflip_h.swap(nf);
+  op->start_class = nc[0];
   return ASR_OK;
+}
+
+// sets the frozen species of every node on `site` (each must sit on a site that was not flippable: own state 0, at most
+// one flip link) and uploads the frozen array on the operator's stream (no synchronisation)
+static int freeze_nodes(asr_op* op, int site, int sp, const char* who, int* nfound) {
+  ASR_TRY(freeze_tables(op));
+  int n = 0;
+  for (int i = 0; i < op->nn; ++i) {
+    if (op->site_h[i] != site) continue;
+    if (op->lst_h[i] != 0 || op->nflip_h[i] > 1) { set_error("%s: the frozen site was flippable", who); return ASR_EINVAL; }
+    ++n;
+  }
+  for (int i = 0; i < op->nn; ++i)
+    if (op->site_h[i] == site) op->frozen_h[i] = (int8_t)sp;
+  if (nfound) *nfound = n;
+  // a pageable source: the call returns once the bytes are staged, so the host array may change afterwards
+  ASR_CUDA(cudaMemcpyAsync(op->d_frozen, op->frozen_h.data(), op->nn, cudaMemcpyHostToDevice, op->ctx->stream));
+  return ASR_OK;
+}
+
+int asr_op_freeze_site(asr_op* op, int site, int sp) {
+  if (!op) { set_error("augcls_freeze_site: null operator"); return ASR_EINVAL; }
+  if (sp < 1 || sp > op->nsp) { set_error("augcls_freeze_site: species index out of range"); return ASR_EINVAL; }
+  ASR_ON_DEVICE(op->ctx->device);
+  ASR_TRY(freeze_tables(op));
+  if (op->site_h[0] == site) {   // the start site: its species must belong to the start node's class (:133-134)
+    const int kap = op->start_class;
+    bool in = false;
+    for (int k = 0; k < op->nsc[kap]; ++k) if (op->spc[k + (size_t)op->ldspc * kap] == sp) in = true;
+    if (!in) { set_error("augcls_freeze_site: species not in the class of the frozen site"); return ASR_EINVAL; }
+  }
+  return freeze_nodes(op, site, sp, "augcls_freeze_site", nullptr);
+}
+
+int asr_op_freeze_any(asr_op* op, int site, int sp, int* nfound) {
+  if (!op) { set_error("augcls_freeze_any: null operator"); return ASR_EINVAL; }
+  if (sp < 1 || sp > op->nsp) { set_error("augcls_freeze_any: species index out of range"); return ASR_EINVAL; }
+  ASR_ON_DEVICE(op->ctx->device);
+  return freeze_nodes(op, site, sp, "augcls_freeze_any", nfound);
 }
 
 int asr_op_unfreeze(asr_op* op) {
@@ -497,7 +534,6 @@ int asr_op_unfreeze(asr_op* op) {
   ASR_ON_DEVICE(op->ctx->device);
   std::fill(op->frozen_h.begin(), op->frozen_h.end(), 0);
   ASR_CUDA(cudaMemsetAsync(op->d_frozen, 0, op->nn, op->ctx->stream));
-  ASR_CUDA(cudaStreamSynchronize(op->ctx->stream));
   return ASR_OK;
 }
 
@@ -554,6 +590,18 @@ int asr_op_apply(asr_op* op, const double* x, double* y, int nvec) {
   std::vector<GroupInfo> gi;
   ASR_TRY(op_group(op, GL, nullptr, nullptr, blob, gi));
   return apply_vectors(op->ctx, op, gi, blob, GL, nvec, x, false, y, APPLY_H);
+}
+
+int asr_op_hp_c(asr_op* op, const double* x, double* y, int nvec) {
+  if (!op || !x || !y || nvec < 1) { set_error("augcls_hp_c: bad argument"); return ASR_EINVAL; }
+  ASR_ON_DEVICE(op->ctx->device);
+  GroupLayout GL = layout(op);
+  // h = c + D S D: the operator's c and d with o = e = 0 (H = E_nu + h - h o h reduces to h)
+  std::vector<double> blob(GL.stride, 0.0), zero((size_t)9 * op->nsp, 0.0);
+  std::vector<GroupInfo> gi(1);
+  ASR_TRY(make_group(op, GL, op->c.data(), op->d.data(), zero.data(), zero.data(), nullptr, nullptr, 0, op->start_l, 1,
+                     op->chi.data(), blob.data(), gi[0]));
+  return apply_vectors(op->ctx, op, gi, blob, GL, nvec, x, true, y, APPLY_H);
 }
 
 int asr_op_rand_c(asr_op* op, const double* par, const double* x, double* w, int nvec) {
@@ -916,6 +964,40 @@ int asr_chains_run(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int 
   ASR_TRY(chains_common(ctx, op, groups, ngroup, d_z.p, nz, mode, depth_tol, tail, precision, project, d_g.p, a, b, mused));
   ASR_CUDA(cudaMemcpyAsync(g, d_g.p, ng * sizeof(double2), cudaMemcpyDeviceToHost, s));
   ASR_CUDA(cudaStreamSynchronize(s));
+  return ASR_OK;
+}
+
+// dos_final (src/asr_class_scf.f90:1912-1931): uniform real energies, the chains of every group there, and the l-resolved
+// sum -worb Im G / pi per (component, spin)
+int asr_dos_final(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const int* comp, const int* spin,
+                  const int* lorb, const double* worb, int ncomp, int nspin, double emin, double emax, double eta, int ndos,
+                  double depth_tol, int tail, int precision, double* edos_e, double* edos) {
+  if (!ctx || !op || !groups || ngroup < 1 || !comp || !spin || !lorb || !worb || ncomp < 1 || nspin < 1 || ndos < 1 ||
+      !edos_e || !edos) {
+    set_error("asr_dos_final: bad argument");
+    return ASR_EINVAL;
+  }
+  for (int q = 0; q < ngroup; ++q) {
+    if (comp[q] < 1 || comp[q] > ncomp || spin[q] < 1 || spin[q] > nspin || lorb[q] < 0 || lorb[q] > 2) {
+      set_error("asr_dos_final: group %d has component, spin or l out of range", q + 1);
+      return ASR_EINVAL;
+    }
+  }
+  std::vector<double> z(2 * (size_t)ndos);
+  for (int ie = 0; ie < ndos; ++ie) {
+    edos_e[ie] = emin + (emax - emin) * ie / (double)std::max(ndos - 1, 1);
+    z[2 * ie] = edos_e[ie];
+    z[2 * ie + 1] = eta;
+  }
+  std::vector<double> g(2 * (size_t)ndos * ngroup);
+  ASR_TRY(asr_chains_run(ctx, op, groups, ngroup, z.data(), ndos, ASR_MODE_EDC, depth_tol, tail, precision, 1, g.data(),
+                         nullptr, nullptr, nullptr));
+  std::fill(edos, edos + (size_t)ndos * 3 * ncomp * nspin, 0.0);
+  const double pi = 3.14159265358979323846;
+  for (int q = 0; q < ngroup; ++q) {
+    double* out = edos + (size_t)ndos * (lorb[q] + 3 * ((comp[q] - 1) + (size_t)ncomp * (spin[q] - 1)));
+    for (int ie = 0; ie < ndos; ++ie) out[ie] -= worb[q] * g[2 * ((size_t)ie + (size_t)ndos * q) + 1] / pi;
+  }
   return ASR_OK;
 }
 

@@ -96,6 +96,11 @@ struct asr_op {
   std::vector<double> block0;      // (9, 9, ntype)
   std::vector<double> c, d, o, e;  // (9, nsp) current operator parameters
   std::vector<int8_t> frozen_h;    // (nn) operator-level frozen species
+  // host copies of what a freeze reads (device node order), fetched from the device tables on the first freeze: the site,
+  // the own local state and the number of flip links of every node, and the class of the start node
+  std::vector<int> site_h;
+  std::vector<int8_t> lst_h, nflip_h;
+  int start_class = -1;
   // device node order: the tables live in a locality order (reverse Cuthill-McKee of the hop graph, start node first);
   // old_of_new[n] is the reference (build) index of device node n, new_of_old its inverse; empty: the build order
   std::vector<int> old_of_new, new_of_old;

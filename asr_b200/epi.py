@@ -319,7 +319,7 @@ def epi_blocks(op: AugclsOp, params, ed: dict, vec: np.ndarray, chi: np.ndarray,
                precision: str = "fp64", project: bool = True):
     """The central blocks of every start vector at every energy (epi_start + epi_blocks, src/asr_epi.f90:578-663) on the
     device: params (c, d, o, e) and ed from ``epi_setup``; vec (9, na) start vectors with characters chi (nop, na) and
-    orbital characters lo (na).  The operator carries the frozen path site and partner (``freeze_site``).  Returns
+    orbital characters lo (na).  The operator carries the frozen path site and partner (``freeze_any``).  Returns
     x (4, nz, na) complex (X0, X1, X2, X1 mismatch) and the depths m (2, nz, na)."""
     c, d, o, e = params
     z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)

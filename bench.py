@@ -410,8 +410,8 @@ def epi_leg(torch):
     params, ed = EP.epi_setup(par, pt)
     vec, chi, lo = EP.epi_adapted(dmat)
     op.set_params(*params)
-    op.freeze_site(1, 3)
-    op.freeze_site(jp, 2)
+    op.freeze_any(1, 3)
+    op.freeze_any(jp, 2)
     z, _ = CT.contour_nodes(-1.2, 0.3, 32)
     EP.epi_blocks(op, params, ed, vec[:, :1], chi[:, :1], lo[:1], z[:2], 24)
     torch.cuda.synchronize()

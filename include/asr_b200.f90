@@ -60,6 +60,26 @@ module asr_b200
     integer(c_int) function asr_op_freeze_site(op, site, sp) bind(c)
       import; type(c_ptr), value :: op; integer(c_int), value :: site, sp
     end function
+    integer(c_int) function asr_op_freeze_any(op, site, sp, nfound) bind(c)
+      import; type(c_ptr), value :: op; integer(c_int), value :: site, sp; integer(c_int) :: nfound
+    end function
+    integer(c_int) function asr_op_hp_c(op, x, y, nvec) bind(c)
+      import; type(c_ptr), value :: op; complex(c_double_complex) :: x(*), y(*); integer(c_int), value :: nvec
+    end function
+    integer(c_int) function asr_dos_final(ctx, op, groups, ngroup, comp, spin, lorb, worb, ncomp, nspin, emin, emax, eta, &
+                                          ndos, depth_tol, tail, precision, edos_e, edos) bind(c)
+      import
+      type(c_ptr), value :: ctx, op
+      type(asr_chain_group) :: groups(*)
+      integer(c_int), value :: ngroup, ncomp, nspin, ndos, tail, precision
+      integer(c_int) :: comp(*), spin(*), lorb(*)
+      real(c_double) :: worb(*), edos_e(*), edos(*)
+      real(c_double), value :: emin, emax, eta, depth_tol
+    end function
+    integer(c_int) function asr_ctx_kernel_stats_kind(ctx, kind, ms, launches, bytes, flops) bind(c)
+      import; type(c_ptr), value :: ctx; integer(c_int), value :: kind; real(c_double) :: ms, bytes, flops
+      integer(c_int64_t) :: launches
+    end function
     integer(c_int) function asr_op_unfreeze(op) bind(c)
       import; type(c_ptr), value :: op
     end function

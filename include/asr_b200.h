@@ -101,7 +101,14 @@ int asr_op_export_tables(const asr_op* op, int* flipr, int* flipg, int* hopr, in
 /* ---- per-operator state: augcls_set_params :121, augcls_freeze_site/_any :129/:147, augcls_set_start :107,
  *      augcls_set_chi :165, augcls_set_class_conc :178 --------------------------------------------------------------- */
 int asr_op_set_params(asr_op* op, const double* c, const double* d, const double* o, const double* e);
+/* augcls_freeze_site (src/asr_augcls.f90:129-142): every node on `site` takes the parameters of species sp (1..nsp);
+ * when the site is the start site, sp must belong to the start node's class.  The nodes must sit on a site that was not
+ * flippable when the node set was built.  The tables a freeze reads are copied to the host on the first freeze of the
+ * operator; later freezes only upload the frozen array (on the context's stream, no synchronisation). */
 int asr_op_freeze_site(asr_op* op, int site, int sp);
+/* augcls_freeze_any (src/asr_augcls.f90:147-161): the same for any species index 1..nsp (a path species, the partner of a
+ * pair); nfound (optional) receives the number of nodes on the site (0: the site lies outside the node set) */
+int asr_op_freeze_any(asr_op* op, int site, int sp, int* nfound);
 int asr_op_unfreeze(asr_op* op);
 int asr_op_set_start(asr_op* op, int l0);
 int asr_op_set_chi(asr_op* op, const double* chi);
@@ -110,6 +117,9 @@ int asr_op_set_class_conc(asr_op* op, int kap, const double* conc);
 /* ---- application: the linop interface (src/asr_operator.f90:10-28) -------------------------------------------------- */
 /* augcls_apply (src/asr_augcls.f90:275-297): y = H x for nvec real vectors x(9 nn, nvec), normalised coordinates */
 int asr_op_apply(asr_op* op, const double* x, double* y, int nvec);
+/* augcls_hp_c (src/asr_augcls.f90:301-320): y = h x = (c + D S D) x for nvec complex vectors x(9 nn, nvec) in normalised
+ * coordinates with the operator's c and d (o and e not applied; the route ed3's h') */
+int asr_op_hp_c(asr_op* op, const double* x, double* y, int nvec);
 /* augcls_rand_c (:419-446): w = X x, complex parameters par(9, nsp), complex x(9 nn, nvec) */
 int asr_op_rand_c(asr_op* op, const double* par, const double* x, double* w, int nvec);
 /* augcls_project_c (:329-348), in place on complex x(9 nn, nvec) */
@@ -142,6 +152,14 @@ int asr_chains_run(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int 
 int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const void* z_dev, int nz,
                        int mode, double depth_tol, int tail, int precision, int project, void* g_dev, double* a, double* b,
                        int* mused);
+
+/* dos_final (src/asr_class_scf.f90:1912-1931): the l-resolved DOS on the real axis.  edos_e(ndos) = emin + (emax - emin)
+ * (ie - 1) / max(ndos - 1, 1); the edc chains of every group at z = edos_e + i eta (as asr_chains_run); then
+ * edos(ie, l, comp, spin) = sum over the groups q with comp(q), spin(q) (1-based) and lorb(q) = l (0 s, 1 p, 2 d) of
+ * -worb(q) Im G_q / pi, worb the orbital-group sizes (lorbk, worbk of the reference).  edos (ndos, 3, ncomp, nspin). */
+int asr_dos_final(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const int* comp, const int* spin,
+                  const int* lorb, const double* worb, int ncomp, int nspin, double emin, double emax, double eta, int ndos,
+                  double depth_tol, int tail, int precision, double* edos_e, double* edos);
 
 /* edc_green_proj (src/asr_edc.f90:174-232) for every (group, energy): each chain runs its full depth (no depth test) and
  * every Lanczos vector is projected on the target states, cpr(k, l, t) = sum_ks tw(l, ks, t) psi_k(node ks of t, l) with

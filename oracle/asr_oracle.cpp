@@ -458,18 +458,39 @@ extern "C" void orc_set_params(void* h, const double* c, const double* d, const 
   size_t m = 9 * (size_t)op->nsp;
   op->c.assign(c, c + m); op->d.assign(d, d + m); op->o.assign(o, o + m); op->e.assign(e, e + m);
 }
-extern "C" int orc_freeze_site(void* h, int site, int sp) {  // augcls_freeze_site / augcls_freeze_any :129-161
-  Op* op = (Op*)h;
-  if (sp < 1 || sp > op->nsp) return fail("augcls_freeze_any: species index out of range");
-  int nfound = 0;
-  for (int i = 0; i < op->nn; ++i) {
+// the node loop shared by augcls_freeze_site and augcls_freeze_any: every node of the site must sit on a site that was not
+// flippable (own state 0, at most one flip link)
+static int freeze_nodes(Op* op, int site, int sp, const char* who, int* nfound) {
+  int n = 0;
+  for (int i = 0; i < op->nn; ++i) {   // the reference stops at the first flippable node; nothing is changed before it here
     if (op->site[i] != site) continue;
     int nz = 0;
     for (int k = 0; k < op->nsmax; ++k) if (op->flipr[k + (size_t)op->nsmax * i] != 0) ++nz;
-    if (op->lst[i] != 0 || nz > 1) return fail("augcls_freeze_site: the frozen site was flippable");
-    op->frozen[i] = sp; ++nfound;
+    if (op->lst[i] != 0 || nz > 1) return fail((std::string(who) + ": the frozen site was flippable").c_str());
+    ++n;
   }
+  for (int i = 0; i < op->nn; ++i)
+    if (op->site[i] == site) op->frozen[i] = sp;
+  if (nfound) *nfound = n;
   return 0;
+}
+// augcls_freeze_site :129-142: the species must belong to the class of the start node when the site is the start site
+extern "C" int orc_freeze_site(void* h, int site, int sp) {
+  Op* op = (Op*)h;
+  if (sp < 1 || sp > op->nsp) return fail("augcls_freeze_site: species index out of range");
+  if (op->site[0] == site) {
+    const int kap = op->ncl[0] - 1;
+    bool in = false;
+    for (int k = 0; k < op->nsc[kap]; ++k) if (op->spcv(k, kap) == sp) in = true;
+    if (!in) return fail("augcls_freeze_site: species not in the class of the frozen site");
+  }
+  return freeze_nodes(op, site, sp, "augcls_freeze_site", nullptr);
+}
+// augcls_freeze_any :147-161: any species index 1..nsp; nfound = nodes on the site
+extern "C" int orc_freeze_any(void* h, int site, int sp, int* nfound) {
+  Op* op = (Op*)h;
+  if (sp < 1 || sp > op->nsp) return fail("augcls_freeze_any: species index out of range");
+  return freeze_nodes(op, site, sp, "augcls_freeze_any", nfound);
 }
 extern "C" void orc_unfreeze(void* h) { Op* op = (Op*)h; std::fill(op->frozen.begin(), op->frozen.end(), 0); }
 extern "C" int orc_set_class_conc(void* h, int kap, const double* conc) {   // augcls_set_class_conc :178-185
@@ -1586,7 +1607,7 @@ extern "C" int orc_chain_greens(void* h, int ngroup, const double* params, const
       if (q != curq) {
         orc_set_params(&op, P, P + 9 * nsp, P + 18 * nsp, P + 27 * nsp);
         std::fill(op.frozen.begin(), op.frozen.end(), 0);
-        if (gcomp[q] > 0 && orc_freeze_site(&op, 1, gcomp[q])) { err = 1; }
+        if (gcomp[q] > 0 && orc_freeze_any(&op, 1, gcomp[q], nullptr)) { err = 1; }
         curq = q;
       }
       if (o != curo) { if (orc_set_start(&op, iorb[o])) err = 1; curo = o; }

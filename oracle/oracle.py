@@ -48,6 +48,7 @@ def lib():
         L.orc_set_chi.argtypes = [C.c_void_p, _d]
         L.orc_set_params.argtypes = [C.c_void_p, _d, _d, _d, _d]
         L.orc_freeze_site.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.orc_freeze_any.argtypes = [C.c_void_p, C.c_int, C.c_int, _i]
         L.orc_unfreeze.argtypes = [C.c_void_p]
         L.orc_set_class_conc.argtypes = [C.c_void_p, C.c_int, _d]
         L.orc_apply.argtypes = [C.c_void_p, _d, _d]
@@ -182,7 +183,15 @@ class OracleOp:
         _check(lib().orc_set_chi(self.h, _pd(_f64(chi))))
 
     def freeze_site(self, site, sp):
+        """``augcls_freeze_site`` (src/asr_augcls.f90:129-142): sp must belong to the start node's class when the site is the
+        start site."""
         _check(lib().orc_freeze_site(self.h, site, sp))
+
+    def freeze_any(self, site, sp):
+        """``augcls_freeze_any`` (src/asr_augcls.f90:147-161): any species index; returns the number of nodes on the site."""
+        n = C.c_int(0)
+        _check(lib().orc_freeze_any(self.h, site, sp, C.byref(n)))
+        return n.value
 
     def unfreeze(self):
         lib().orc_unfreeze(self.h)
@@ -325,6 +334,21 @@ class OracleOp:
             return gz.transpose(2, 1, 0), steps.value
         return gz.transpose(2, 1, 0), steps.value, dict(a=az.transpose(3, 2, 1, 0), b=bz.transpose(3, 2, 1, 0),
                                                         m=mz.transpose(2, 1, 0))
+
+
+def dos_final(oop, groups, gcomp, iorb, nlevq, lorb, worb, pcomp, spin, ncomp, nspin, emin, emax, eta, ndos, nthreads=0,
+              depth_tol=0.0, tail="hull"):
+    """``dos_final`` (src/asr_class_scf.f90:1912-1931) on the oracle: energies e_ie = emin + (emax - emin)(ie - 1) /
+    max(ndos - 1, 1), ``chain_greens`` at e + i eta for the groups (parameter sets) x start orbitals iorb, then
+    edos(ie, l, comp, spin) -= worb(o) Im G / pi for l = lorb(o); group q of the parameter sets belongs to component
+    pcomp[q] and spin spin[q] (1-based).  Returns (e, edos (ndos, 3, ncomp, nspin))."""
+    e = np.array([emin + (emax - emin) * ie / max(ndos - 1, 1) for ie in range(ndos)])
+    gz, _ = oop.chain_greens(groups, gcomp, iorb, nlevq, e + 1j * eta, 4, depth_tol=depth_tol, tail=tail, nthreads=nthreads)
+    edos = np.zeros((ndos, 3, ncomp, nspin))
+    for q in range(len(groups)):
+        for o in range(len(iorb)):
+            edos[:, lorb[o], pcomp[q] - 1, spin[q] - 1] -= worb[o] * gz[:, o, q].imag / np.pi
+    return e, edos
 
 
 # ---------------------------------------------------------------------------------------------- free functions

@@ -67,8 +67,8 @@ def dense_h(c, par, spsite, pt, sj):
         cc[:, s], dd[:, s], oo[:, s], ee[:, s] = p.c, p.d, p.o, p.e
     cc[:, 3], dd[:, 3], oo[:, 3], ee[:, 3] = pt.c, pt.d, pt.o, pt.e
     op.set_params(cc, dd, oo, ee)
-    op.freeze_site(1, 4)
-    op.freeze_site(c["jp"], sj)
+    op.freeze_any(1, 4)
+    op.freeze_any(c["jp"], sj)
     dim = 9 * n
     h = np.zeros((dim, dim))
     for k in range(dim):

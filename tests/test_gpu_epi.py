@@ -39,8 +39,8 @@ def test_device_blocks_match_the_oracle(group, tail, nlev):
     vec, chi, lo = EP.epi_adapted(d)
     for op in (dop, oop):
         op.set_params(*params)
-        op.freeze_site(1, 4)
-        op.freeze_site(c["jp"], 2)
+        op.freeze_any(1, 4)
+        op.freeze_any(c["jp"], 2)
     x, m = EP.epi_blocks(dop, params, ed, vec, chi, lo, ZS, nlev, tail)
     worst = 0.0
     for ia in range(9):
@@ -58,8 +58,8 @@ def test_device_trace_equals_the_exact_configuration_average(group):
     par = E.species()
     for sj in (2, 3):
         dop.unfreeze()
-        dop.freeze_site(1, 4)
-        dop.freeze_site(c["jp"], sj)
+        dop.freeze_any(1, 4)
+        dop.freeze_any(c["jp"], sj)
         tr, mism = EP.trace_at(dop, par, 1, 2, LAM, d, ZS[:1], 100, tail="none")
         ref = E.exact_trace(c, par, 1, 2, LAM, sj, ZS[0])
         assert abs(tr[0] - ref) / abs(ref) < 1e-8, (sj, tr[0], ref)
@@ -73,8 +73,8 @@ def test_fp32_blocks_close_to_fp64():
     params, ed = EP.epi_setup(par, pt)
     vec, chi, lo = EP.epi_adapted(d)
     dop.set_params(*params)
-    dop.freeze_site(1, 4)
-    dop.freeze_site(c["jp"], 3)
+    dop.freeze_any(1, 4)
+    dop.freeze_any(c["jp"], 3)
     x64, _ = EP.epi_blocks(dop, params, ed, vec, chi, lo, ZS, 16, "hull", "fp64")
     x32, _ = EP.epi_blocks(dop, params, ed, vec, chi, lo, ZS, 16, "hull", "fp32")
     assert np.max(np.abs(x32[:3] - x64[:3])) < 1e-4 * np.max(np.abs(x64[:3]))
@@ -89,8 +89,8 @@ def test_pair_table_against_the_exact_integral():
 
     def op_for(s):
         dop.unfreeze()
-        dop.freeze_site(1, 4)
-        dop.freeze_site(c["jp"], s)
+        dop.freeze_any(1, 4)
+        dop.freeze_any(c["jp"], s)
         return dop
     u = EP.pair_table(op_for, par, [1, 2, 3], [1, 2, 3], d, z, w, 2, 100, tail="none")
     xg, wg = np.polynomial.legendre.leggauss(2)
