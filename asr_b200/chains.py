@@ -151,6 +151,34 @@ def dos_final(op: AugclsOp, specs, comp, spin, lorb, worb, ncomp: int, nspin: in
     return e, edos
 
 
+def chains_run_lanes(op: AugclsOp, specs, lane_group, lane_z, depth_tol: float = 0.0, tail: str = "hull",
+                     precision: str = "fp64", project: bool = True):
+    """The tasks of ``chain_worker`` (src/asr_class_scf.f90:1071-1160) as explicit lanes of the edc route: lane L runs
+    group lane_group[L] (0-based) at energy lane_z[L].  Returns (g (nlane,), m (nlane,)), bitwise those of ``chains_run``
+    for the same (group, energy)."""
+    lg = np.ascontiguousarray(np.asarray(lane_group, np.int64) + 1, np.int32)
+    lz = np.ascontiguousarray(lane_z, np.complex128)
+    if lg.shape != lz.shape or lg.ndim != 1:
+        raise ValueError("chains_run_lanes: one group and one energy per lane")
+    arr, keep = _groups(specs)
+    g = np.zeros(lz.shape[0], np.complex128)
+    m = np.zeros(lz.shape[0], np.int32)
+    check(lib().asr_chains_run_lanes(op.ctx.h, op.h, arr, len(specs), _pi(lg), _pd(lz), lz.shape[0], float(depth_tol),
+                                     _lib.TAILS[tail], PREC[precision], int(bool(project)), _pd(g), _pi(m)))
+    return g, m
+
+
+def chains_run_lanes_device(op: AugclsOp, specs, lane_group, z_dev, g_dev, depth_tol: float = 0.0, tail: str = "hull",
+                            precision: str = "fp64", project: bool = True):
+    """Device-resident ``chains_run_lanes``: z_dev / g_dev device pointers (ints) of complex128 arrays of one entry per lane;
+    lane_group (0-based) on the host."""
+    lg = np.ascontiguousarray(np.asarray(lane_group, np.int64) + 1, np.int32)
+    arr, keep = _groups(specs)
+    check(lib().asr_chains_run_lanes_dev(op.ctx.h, op.h, arr, len(specs), _pi(lg), C.c_void_p(z_dev), lg.shape[0],
+                                         float(depth_tol), _lib.TAILS[tail], PREC[precision], int(bool(project)),
+                                         C.c_void_p(g_dev)))
+
+
 def chains_run_device(op: AugclsOp, specs, z_dev, g_dev, nz: int, mode: str = "edc", depth_tol: float = 0.0, tail: str = "hull",
                       precision: str = "fp64", project: bool = True):
     """Device-resident form: z_dev / g_dev are device pointers (ints, e.g. torch tensor data_ptr()) of complex128 arrays;

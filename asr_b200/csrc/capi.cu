@@ -944,6 +944,68 @@ int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
   return ASR_OK;
 }
 
+// chain_worker tasks as explicit lanes (edc route): lane L runs group lane_group[L] (1-based) at the energy lane_z[L]
+static int lanes_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const int* lane_group,
+                        const double2* d_lane_z, int nlane, double depth_tol, int tail, int precision, int project, double2* d_g,
+                        int* mused) {
+  if (!ctx || !op || !groups || ngroup < 1 || !lane_group || nlane < 1) { set_error("asr_chains_run_lanes: bad argument"); return ASR_EINVAL; }
+  if (tail < 0 || tail > 3) { set_error("asr_chains_run_lanes: unknown tail"); return ASR_EINVAL; }
+  std::vector<int> lg(nlane);
+  for (int L = 0; L < nlane; ++L) {
+    if (lane_group[L] < 1 || lane_group[L] > ngroup) { set_error("asr_chains_run_lanes: lane %d has group %d", L + 1, lane_group[L]); return ASR_EINVAL; }
+    lg[L] = lane_group[L] - 1;
+  }
+  ASR_ON_DEVICE(ctx->device);
+  GroupLayout GL = layout(op);
+  std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
+  std::vector<GroupInfo> gi(ngroup);
+  for (int q = 0; q < ngroup; ++q) {
+    const asr_chain_group& G = groups[q];
+    if (!G.c || !G.d) { set_error("asr_chains_run_lanes: group %d without c or d", q + 1); return ASR_EINVAL; }
+    if (G.nlev < 1 || G.nlev > NLMAX) { set_error("asr_chains_run_lanes: depth %d out of range 1..%d", G.nlev, NLMAX); return ASR_EINVAL; }
+    ASR_TRY(make_group(op, GL, G.c, G.d, G.o, G.e, G.pa, G.pb, G.frozen_sp, G.start_orb, G.nlev, nullptr,
+                       blob.data() + (size_t)GL.stride * q, gi[q]));
+  }
+  RunOptions opt;
+  opt.mode = ASR_MODE_EDC;
+  opt.depth_tol = depth_tol;
+  opt.tail = tail;
+  opt.precision = precision;
+  opt.project = project;
+  std::vector<int> hm;
+  int64_t nfall = 0, nsteps = 0;
+  ASR_TRY(run_lanes(ctx, op, gi, blob, GL, lg, d_lane_z, nlane, opt, d_g, nullptr, nullptr, &hm, &nfall, &nsteps));
+  if (mused) for (int L = 0; L < nlane; ++L) mused[L] = hm[L];
+  ctx->nchain += nlane;
+  ctx->nlev += nsteps;
+  ctx->nfall += nfall;
+  return ASR_OK;
+}
+
+int asr_chains_run_lanes(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const int* lane_group,
+                         const double* lane_z, int nlane, double depth_tol, int tail, int precision, int project, double* g,
+                         int* mused) {
+  if (!ctx || !lane_z || !g || nlane < 1) { set_error("asr_chains_run_lanes: bad argument"); return ASR_EINVAL; }
+  ASR_ON_DEVICE(ctx->device);
+  cudaStream_t s = ctx->stream;
+  Dev<double2> d_z, d_g;
+  ASR_TRY(d_z.alloc(nlane));
+  ASR_TRY(d_g.alloc(nlane));
+  ASR_CUDA(cudaMemcpyAsync(d_z.p, lane_z, nlane * sizeof(double2), cudaMemcpyHostToDevice, s));
+  ASR_TRY(lanes_common(ctx, op, groups, ngroup, lane_group, d_z.p, nlane, depth_tol, tail, precision, project, d_g.p, mused));
+  ASR_CUDA(cudaMemcpyAsync(g, d_g.p, nlane * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  ASR_CUDA(cudaStreamSynchronize(s));
+  return ASR_OK;
+}
+
+int asr_chains_run_lanes_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const int* lane_group,
+                             const void* lane_z_dev, int nlane, double depth_tol, int tail, int precision, int project,
+                             void* g_dev) {
+  if (!lane_z_dev || !g_dev) { set_error("asr_chains_run_lanes_dev: null device array"); return ASR_EINVAL; }
+  return lanes_common(ctx, op, groups, ngroup, lane_group, (const double2*)lane_z_dev, nlane, depth_tol, tail, precision,
+                      project, (double2*)g_dev, nullptr);
+}
+
 int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const void* z_dev, int nz, int mode,
                        double depth_tol, int tail, int precision, int project, void* g_dev, double* a, double* b, int* mused) {
   return chains_common(ctx, op, groups, ngroup, (const double2*)z_dev, nz, mode, depth_tol, tail, precision, project,

@@ -77,6 +77,8 @@ def parse():
     p.add_argument("--legs", default="1",
                    help="1: measure every leg (mixed precision with its DOS error, adjoint, KPM, plain, example, spectral, "
                         "EPI), 0: none, or a comma list of leg names")
+    p.add_argument("--lanes", type=int, default=0,
+                   help="1: run the multi-GPU step (task split, lane chains, all-reduce of the shares) also on one GPU")
     p.add_argument("--link", default="auto", choices=["auto", "general", "fixed"],
                    help="step-kernel link gathers: the autotuner's choice (auto; general without --autotune), or pinned")
     return p.parse_args()
@@ -588,9 +590,15 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
+    split = world > 1 or args.lanes == 1
+    if split:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        if world == 1:
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            os.environ.setdefault("MASTER_PORT", "29517")
+            dist.init_process_group("nccl", rank=0, world_size=1, timeout=timedelta(seconds=300))
+        else:
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     import asr_b200 as A
 
     case, fl, groups, z_all = workload()
@@ -619,16 +627,32 @@ def main():
         A.set_tuning(op, args.precision, tune["tiles_per_batch"], tune["nodes_per_warp"], tune["link_gather"])
 
     def slice_of(it):
-        # each rank walks its own slices (weak scaling); rank r starts r slices further
-        start = ((it * world + rank) * nzs) % (nall - nzs + 1)
-        return start
+        # one GPU: step it covers the it-th slice of nzs energies; N GPUs: step it covers N consecutive slices (weak
+        # scaling), split over the ranks by the reference's task rule below
+        return (it * world * nzs) % (nall - world * nzs + 1)
+
+    # N > 1: the step's tasks are (group, block of 32 energies) as chain_greens numbers them, dealt to the ranks by the
+    # cyclic rule with energy rotation (src/asr_class_scf.f90:1095-1097); each rank runs its lanes and one all-reduce of
+    # the disjoint shares (par_sum_z) leaves the step's whole G on every rank
+    from asr_b200 import distributed as D
+    nzw = world * nzs
+    lane_q, lane_j = D.rank_lanes(len(specs), nzw, 32, world, rank)
+    lane_q_dev = torch.from_numpy(lane_q).to("cuda")
+    lane_j_dev = torch.from_numpy(lane_j).to("cuda")
+    gl_dev = torch.zeros(max(lane_q.size, 1), dtype=torch.complex128, device="cuda")
+    zl_dev = torch.zeros_like(gl_dev)
+    gz_dev = torch.zeros((len(specs), nzw), dtype=torch.complex128, device="cuda")
 
     def step(it, precision=args.precision):
         s0 = slice_of(it)
-        A.chains_run_device(op, specs, z_dev[s0:s0 + nzs].data_ptr(), g_dev.data_ptr(), nzs, "edc", 0.0, "hull", precision)
-        if world > 1:
-            out = torch.empty(world * g_dev.numel(), dtype=g_dev.dtype, device="cuda")
-            dist.all_gather_into_tensor(out, g_dev)
+        if not split:
+            A.chains_run_device(op, specs, z_dev[s0:s0 + nzs].data_ptr(), g_dev.data_ptr(), nzs, "edc", 0.0, "hull", precision)
+            return
+        zl_dev[: lane_j.size] = z_dev[s0 + lane_j_dev]
+        A.chains_run_lanes_device(op, specs, lane_q, zl_dev.data_ptr(), gl_dev.data_ptr(), "edc" and 0.0, "hull", precision)
+        gz_dev.zero_()
+        gz_dev[lane_q_dev, lane_j_dev] = gl_dev[: lane_j.size]
+        dist.all_reduce(torch.view_as_real(gz_dev), op=dist.ReduceOp.SUM)
 
     for it in range(args.warmup):
         step(it)
@@ -661,10 +685,13 @@ def main():
     total_steps = chain_steps_per_step * args.steps * world
     value = total_steps / (ms / 1000.0)
     # e2e through the host C-ABI call (host z in pinned memory, host g; copies inside the timed region)
+    # (N > 1: each rank its lanes of the step, then the disjoint-share sum of the host results)
     z_pinned = []
     for it in range(args.steps):
-        zt = torch.empty(nzs, dtype=torch.complex128).pin_memory()
-        zt.numpy()[:] = z_all[slice_of(args.warmup + it): slice_of(args.warmup + it) + nzs]
+        s0 = slice_of(args.warmup + it)
+        zs = z_all[s0 + lane_j] if split else z_all[s0: s0 + nzs]
+        zt = torch.empty(zs.shape[0], dtype=torch.complex128).pin_memory()
+        zt.numpy()[:] = zs
         z_pinned.append(zt)
     z_host = [zt.numpy() for zt in z_pinned]
     torch.cuda.synchronize()
@@ -673,8 +700,14 @@ def main():
     e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2.record(stream)
     for it in range(args.steps if args.e2e else 0):
-        r = A.chains_run(op, specs, z_host[it], "edc", 0.0, "hull", args.precision)
-        _ = r["g"]
+        if not split:
+            r = A.chains_run(op, specs, z_host[it], "edc", 0.0, "hull", args.precision)
+            _ = r["g"]
+        else:
+            gl, _ = A.chains_run_lanes(op, specs, lane_q, z_host[it], 0.0, "hull", args.precision)
+            gz = np.zeros((len(specs), nzw), np.complex128)
+            gz[lane_q, lane_j] = gl
+            D.sum_disjoint(gz, dist, "cuda")
     e3.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3) if args.e2e else float("nan")
@@ -688,6 +721,9 @@ def main():
     nsp = 3
     h2d = nzs * 16 + len(specs) * 6 * 9 * nsp * 8
     d2h = len(specs) * nzs * (16 + 4)
+    if split:   # lane energies in, lane results and depths out, and the step's G array through the all-reduce
+        h2d = lane_j.size * 16 + len(specs) * 6 * 9 * nsp * 8 + len(specs) * nzw * 16
+        d2h = lane_j.size * (16 + 4) + len(specs) * nzw * 16
 
     if rank == 0:
         hbm_peak, peak_source = hbm_peak_of()
@@ -723,7 +759,9 @@ def main():
                                    "energies", "nodes": op.nn, "slots": op.nslot, "energies_per_step": nzs,
                        "chains_per_step": len(specs) * nzs, "chain_steps_per_step": chain_steps_per_step,
                        "l2": "inputs larger than L2 (one 32-lane vector is %.0f MB)" % (op.nn * 9 * 32 * 16 / 1e6),
-                       "parallelism": f"chain tasks over {world} GPU(s)", "operator_build_s": build_s,
+                       "parallelism": (f"chain tasks (group, 32-energy block) over {world} GPU(s) by the cyclic rule with "
+                                       f"energy rotation, all-reduce of the disjoint G shares" if split else "one GPU"),
+                       "energies_per_step_all_gpus": nzs * world, "operator_build_s": build_s,
                        "batch_shape": {"tiles_per_batch": tune["tiles_per_batch"], "nodes_per_warp": tune["nodes_per_warp"],
                                        "autotune_ms_tiles_4_8_16_32": tune["ms_tiles"], "autotune_ms_npw_1_2_4_8": tune["ms_npw"],
                                        "link_gather": tune["link_gather"], "autotune_ms_link_general_fixed": tune["ms_link"]},
@@ -746,7 +784,7 @@ def main():
             "clocks": clocks,
         }
         print(json.dumps(line))
-    if world > 1:
+    if split:
         dist.barrier()
         dist.destroy_process_group()
 

@@ -80,6 +80,25 @@ module asr_b200
       import; type(c_ptr), value :: ctx; integer(c_int), value :: kind; real(c_double) :: ms, bytes, flops
       integer(c_int64_t) :: launches
     end function
+    integer(c_int) function asr_chains_run_lanes(ctx, op, groups, ngroup, lane_group, lane_z, nlane, depth_tol, tail, &
+                                                 precision, project, g, mused) bind(c)
+      import
+      type(c_ptr), value :: ctx, op
+      type(asr_chain_group) :: groups(*)
+      integer(c_int), value :: ngroup, nlane, tail, precision, project
+      integer(c_int) :: lane_group(*), mused(*)
+      complex(c_double_complex) :: lane_z(*), g(*)
+      real(c_double), value :: depth_tol
+    end function
+    integer(c_int) function asr_chains_run_lanes_dev(ctx, op, groups, ngroup, lane_group, lane_z_dev, nlane, depth_tol, &
+                                                     tail, precision, project, g_dev) bind(c)
+      import
+      type(c_ptr), value :: ctx, op, lane_z_dev, g_dev
+      type(asr_chain_group) :: groups(*)
+      integer(c_int), value :: ngroup, nlane, tail, precision, project
+      integer(c_int) :: lane_group(*)
+      real(c_double), value :: depth_tol
+    end function
     integer(c_int) function asr_op_unfreeze(op) bind(c)
       import; type(c_ptr), value :: op
     end function

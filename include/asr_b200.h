@@ -153,6 +153,18 @@ int asr_chains_run_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
                        int mode, double depth_tol, int tail, int precision, int project, void* g_dev, double* a, double* b,
                        int* mused);
 
+/* The tasks of chain_worker (src/asr_class_scf.f90:1071-1160) as explicit lanes of the edc route: lane L runs group
+ * lane_group[L] (1-based) at the energy lane_z[L] (complex), so that a rank runs exactly its share of the cyclic task split
+ * (:1095-1097; energy blocks of a group need not be contiguous or the same for every group).  g(nlane) complex,
+ * mused(nlane) optional.  The _dev form takes device arrays of lane energies and results (lane_group stays on the host);
+ * results are bitwise those of asr_chains_run for the same (group, energy). */
+int asr_chains_run_lanes(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const int* lane_group,
+                         const double* lane_z, int nlane, double depth_tol, int tail, int precision, int project, double* g,
+                         int* mused);
+int asr_chains_run_lanes_dev(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const int* lane_group,
+                             const void* lane_z_dev, int nlane, double depth_tol, int tail, int precision, int project,
+                             void* g_dev);
+
 /* dos_final (src/asr_class_scf.f90:1912-1931): the l-resolved DOS on the real axis.  edos_e(ndos) = emin + (emax - emin)
  * (ie - 1) / max(ndos - 1, 1); the edc chains of every group at z = edos_e + i eta (as asr_chains_run); then
  * edos(ie, l, comp, spin) = sum over the groups q with comp(q), spin(q) (1-based) and lorb(q) = l (0 s, 1 p, 2 d) of
