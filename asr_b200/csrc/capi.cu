@@ -1282,8 +1282,8 @@ int asr_cf_eval(asr_ctx* ctx, const double* a, const double* b, const int* m, in
 // reverse mode of one terminated fraction (host): abar/bbar(m) complex receive w dG/da_k, w dG/db_k
 int asr_cf_adjoint(const double* a, const double* b, int m, double zr, double zi, int tail, double wr, double wi, double* abar,
                    double* bbar, double* g) {
-  if (!a || !b || !abar || !bbar || m < 1 || m > CF_NMAX || tail < 0 || tail > 3 || tail == ASR_TAIL_BP) {
-    set_error("asr_cf_adjoint: bad argument (tails none, hull, avg2; 1 <= m <= %d)", CF_NMAX);
+  if (!a || !b || !abar || !bbar || m < 1 || m > CF_NMAX || tail < 0 || tail > 3) {
+    set_error("asr_cf_adjoint: bad argument (tails none, hull, bp, avg2; 1 <= m <= %d)", CF_NMAX);
     return ASR_EINVAL;
   }
   std::vector<double2> gt(m), v(m), t(m), wd(m), we(m);

@@ -278,9 +278,10 @@ __host__ __device__ inline int tridiag_solve_shift(int m, const double2* a, cons
   return 0;
 }
 
-__host__ __device__ inline void eig_grad(int m, const double2* a, const double2* b, double2 lam, double2 w, double2* abar,
-                                         double2* bbar, double2* v, double2* t, double2* wd, double2* we) {
-  // eigenvector by two steps of inverse iteration at a shift next to lam, then dlam/da_j = v_j^2 / (v.v)
+// eigenvector t (scaled to max modulus 1) of the complex symmetric tridiagonal (a, b) at the simple eigenvalue lam: two
+// steps of inverse iteration at a shift next to lam; returns t.t (the bilinear, not the Hermitian, square)
+__host__ __device__ inline double2 eig_vec(int m, const double2* a, const double2* b, double2 lam, double2* v, double2* t,
+                                           double2* wd, double2* we) {
   double sc = 0.0;
   for (int j = 0; j < m; ++j) sc = fmax(sc, cmag(a[j]) + (j < m - 1 ? cmag(b[j]) : 0.0));
   double2 mu = cadd(lam, make_double2(1e-10 * (sc + 1.0), 1e-10 * (sc + 1.0)));
@@ -293,9 +294,23 @@ __host__ __device__ inline void eig_grad(int m, const double2* a, const double2*
   }
   double2 vv = make_double2(0.0, 0.0);
   for (int j = 0; j < m; ++j) vv = cadd(vv, cmul(t[j], t[j]));
+  return vv;
+}
+
+// abar_j += w dlam/da_j, bbar_j += w dlam/db_j with dlam = v^T dT v / (v^T v)
+__host__ __device__ inline void eig_grad(int m, const double2* a, const double2* b, double2 lam, double2 w, double2* abar,
+                                         double2* bbar, double2* v, double2* t, double2* wd, double2* we) {
+  double2 vv = eig_vec(m, a, b, lam, v, t, wd, we);
   double2 f = cdiv(w, vv);
   for (int j = 0; j < m; ++j) abar[j] = cadd(abar[j], cmul(f, cmul(t[j], t[j])));
   for (int j = 0; j < m - 1; ++j) bbar[j] = cadd(bbar[j], cmul(f, cscale(cmul(t[j], t[j + 1]), 2.0)));
+}
+
+// dlam / da_{m-1} = v_{m-1}^2 / (v^T v): the sensitivity of the eigenvalue to the last diagonal entry
+__host__ __device__ inline double2 eig_last_sens(int m, const double2* a, const double2* b, double2 lam, double2* v, double2* t,
+                                                 double2* wd, double2* we) {
+  double2 vv = eig_vec(m, a, b, lam, v, t, wd, we);
+  return cdiv(cmul(t[m - 1], t[m - 1]), vv);
 }
 
 // w: seed; work arrays of length >= m each: gt, v, t, wd, we.  Returns G.
@@ -303,9 +318,32 @@ __host__ __device__ inline double2 cf_species_adjoint(const double2* a, const do
                                                        double2* abar, double2* bbar, double2* gt, double2* v, double2* t, double2* wd,
                                                        double2* we) {
   // forward: tail parameters
-  double2 aa = make_double2(0, 0), bb = make_double2(0, 0), lo, hi;
-  int kind = 0;   // 0 none / finite, 1 hull, 3 avg2
-  if (tail == 3 && m >= 3) {
+  double2 aa = make_double2(0, 0), bb = make_double2(0, 0), lo, hi, ep = make_double2(0, 0), em = make_double2(0, 0);
+  int kind = 0;   // 0 none / finite, 1 hull, 2 last coefficients, 3 avg2, 4 Beer-Pettifor fixed point, 5 tail held fixed
+  if (tail == 2 && m >= 2 && chain_extremes(a, b, m, a[m - 1], wd, we, lo, hi) == 0) {
+    // the fixed point as cf_tail_dev iterates it (src/asr_chain.f90:126-156): converged -> differentiated implicitly;
+    // not converged -> the hull values (differentiated as the hull); an eigenvalue failure keeps the last iterate, whose
+    // dependence on (a, b) is not followed (kind 5)
+    aa = cscale(cadd(lo, hi), 0.5);
+    bb = cscale(csub(hi, lo), 0.25);
+    kind = 1;
+    for (int it = 0; it < 200; ++it) {
+      double2 l1, h1, l2, h2;
+      if (chain_extremes(a, b, m, cadd(a[m - 1], bb), wd, we, l1, h1) ||
+          chain_extremes(a, b, m, csub(a[m - 1], bb), wd, we, l2, h2)) { kind = 5; break; }
+      double2 an = cscale(cadd(h1, l2), 0.5), bn = cscale(csub(h1, l2), 0.25);
+      if (cmag(csub(an, aa)) + cmag(csub(bn, bb)) < 1.0e-12 * (1.0 + cmag(bn))) {
+        aa = an; bb = bn; ep = h1; em = l2; kind = 4;
+        break;
+      }
+      aa = an;
+      bb = bn;
+    }
+    if (kind == 1) {   // not converged within 200 iterations: the hull
+      aa = cscale(cadd(lo, hi), 0.5);
+      bb = cscale(csub(hi, lo), 0.25);
+    }
+  } else if (tail == 3 && m >= 3) {
     aa = cscale(cadd(a[m - 1], a[m - 2]), 0.5);
     bb = csqrt_p(cscale(cadd(cmul(b[m - 2], b[m - 2]), cmul(b[m - 3], b[m - 3])), 0.5));
     kind = 3;
@@ -331,6 +369,7 @@ __host__ __device__ inline double2 cf_species_adjoint(const double2* a, const do
   double2 one = make_double2(1.0, 0.0);
   gt[m - 1] = cdiv(one, csub(csub(z, a[m - 1]), tl));
   for (int j = m - 2; j >= 0; --j) gt[j] = cdiv(one, csub(csub(z, a[j]), cmul(cmul(b[j], b[j]), gt[j + 1])));
+  const double2 G = gt[0];
   // reverse: gbar_j is the adjoint of gt_j
   double2 gbar = w;
   double2 tbar = make_double2(0, 0);
@@ -357,6 +396,26 @@ __host__ __device__ inline double2 cf_species_adjoint(const double2* a, const do
     } else if (kind == 2) {
       abar[m - 1] = cadd(abar[m - 1], aabar);
       if (m > 1) bbar[m - 2] = cadd(bbar[m - 2], bbbar);
+    } else if (kind == 4) {
+      // bb = phi(bb) = (ep(a_m + bb) - em(a_m - bb)) / 4 and aa = (ep + em) / 2 at the fixed point.  With the
+      // sensitivities pv = d ep / d a_m, pu = d em / d a_m (eigenvectors of the two shifted chain matrices):
+      // d phi / d bb = (pv + pu) / 4, partial d aa / d bb = (pv - pu) / 2, and the adjoint of the fixed point
+      // lam = (bbbar + aabar (pv - pu) / 2) / (1 - (pv + pu) / 4); the eigenvalue seeds are aabar / 2 +- lam / 4.
+      double2* am = gt;   // gt is no longer needed: the shifted diagonal
+      for (int j = 0; j < m; ++j) am[j] = a[j];
+      am[m - 1] = cadd(a[m - 1], bb);
+      double2 pv = eig_last_sens(m, am, b, ep, v, t, wd, we);
+      am[m - 1] = csub(a[m - 1], bb);
+      double2 pu = eig_last_sens(m, am, b, em, v, t, wd, we);
+      double2 den = csub(one, cscale(cadd(pv, pu), 0.25));
+      double2 lam = cdiv(cadd(bbbar, cmul(aabar, cscale(csub(pv, pu), 0.5))), den);
+      double2 wp = cadd(cscale(aabar, 0.5), cscale(lam, 0.25)), wm = csub(cscale(aabar, 0.5), cscale(lam, 0.25));
+      am[m - 1] = cadd(a[m - 1], bb);
+      eig_grad(m, am, b, ep, wp, abar, bbar, v, t, wd, we);
+      am[m - 1] = csub(a[m - 1], bb);
+      eig_grad(m, am, b, em, wm, abar, bbar, v, t, wd, we);
+    } else if (kind == 5) {
+      // tail held fixed
     } else {
       // aa = (lo + hi)/2, bb = (hi - lo)/4
       double2 wlo = csub(cscale(aabar, 0.5), cscale(bbbar, 0.25)), whi = cadd(cscale(aabar, 0.5), cscale(bbbar, 0.25));
@@ -364,7 +423,7 @@ __host__ __device__ inline double2 cf_species_adjoint(const double2* a, const do
       eig_grad(m, a, b, hi, whi, abar, bbar, v, t, wd, we);
     }
   }
-  return gt[0];
+  return G;
 }
 
 // kernels of cf.cu

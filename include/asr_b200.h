@@ -260,7 +260,9 @@ int asr_cf_eval_noalloc(asr_ctx* ctx, const double* a, const double* b, const in
                         int nz, int tail, double* g, int64_t* nfall);
 
 /* reverse mode of cf_species for one chain (host): abar(m), bbar(m) complex receive w dG/da_k and w dG/db_k; g = G.
- * Tails none, hull, avg2 (the bp fixed point has no derivative here).  No counterpart in the reference. */
+ * Tails none, hull, bp, avg2; the Beer-Pettifor fixed point is differentiated implicitly (through the sensitivities of
+ * the two shifted extreme eigenvalues); a fixed point that did not converge falls back to the hull, as the forward does.
+ * No counterpart in the reference. */
 int asr_cf_adjoint(const double* a, const double* b, int m, double zr, double zi, int tail, double wr, double wi, double* abar,
                    double* bbar, double* g);
 
