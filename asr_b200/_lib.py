@@ -34,7 +34,8 @@ EXPORTS = ["asr_version", "asr_last_error", "asr_ctx_create", "asr_ctx_destroy",
            "asr_supercell_apply", "asr_kpm_moments", "asr_kpm_dos", "asr_sro_layout", "asr_gauss_legendre",
            "asr_contour_nodes", "asr_contour_nodes_closed", "asr_contour_nodes_fermi", "asr_contour_moment",
            "asr_op_build_targets", "asr_chains_proj", "asr_epi_blocks", "asr_autotune", "asr_op_tuning",
-           "asr_op_set_tuning", "asr_op_hp_c", "asr_dos_final", "asr_chains_run_lanes", "asr_chains_run_lanes_dev"]
+           "asr_op_set_tuning", "asr_op_hp_c", "asr_dos_final", "asr_chains_run_lanes", "asr_chains_run_lanes_dev",
+           "asr_chains_adjoint_ext"]
 
 
 class ChainGroup(C.Structure):
@@ -84,6 +85,8 @@ def lib():
     L.asr_op_freeze_site.argtypes = [vp, C.c_int, C.c_int]
     L.asr_op_freeze_any.argtypes = [vp, C.c_int, C.c_int, i_p]
     L.asr_op_hp_c.argtypes = [vp, d_p, d_p, C.c_int]
+    L.asr_chains_adjoint_ext.argtypes = [vp, vp, C.POINTER(ChainGroup), C.c_int, d_p, C.c_int, d_p, C.c_double, C.c_int,
+                                         C.c_int, C.c_int, C.c_int, d_p, i_p, d_p]
     L.asr_chains_run_lanes.argtypes = [vp, vp, C.POINTER(ChainGroup), C.c_int, i_p, d_p, C.c_int, C.c_double, C.c_int, C.c_int,
                                        C.c_int, d_p, i_p]
     L.asr_chains_run_lanes_dev.argtypes = [vp, vp, C.POINTER(ChainGroup), C.c_int, i_p, vp, C.c_int, C.c_double, C.c_int,

@@ -6,10 +6,11 @@ src/asr_edc.f90:41-71 and :237-316) and of the contour moments of ``ed_moments``
 differentiated with respect to the species parameters (c_l, d_l, Delta_l).
 
 * ``ChainGreens`` -- G(group, energy) of a batch of chain groups as a function of the groups' parameter arrays
-  (c, d, e, pa, pb per orbital and species).  Forward: ``asr_chains_run``; backward: ``asr_chains_adjoint``, the
+  (c, d, o, e, pa, pb per orbital and species).  Forward: ``asr_chains_run``; backward: ``asr_chains_adjoint_ext``, the
   device adjoint (Lanczos vectors kept every sqrt(depth) levels and recomputed, reverse sweep through the recurrence,
   reverse mode of the continued fraction).
-* ``edc_group_arrays`` -- the map of ``edc_setup`` from species parameters to a group's arrays, in torch.
+* ``edc_group_arrays``, ``edc_group_o`` -- the map of ``edc_setup`` from species parameters to a group's arrays, in
+  torch.
 * ``contour_moments`` -- M_k = -(1/pi) Im sum_j w_j (z_j - E_nu)^k G_j.
 """
 from __future__ import annotations
@@ -18,7 +19,7 @@ import numpy as np
 import torch
 
 from .augcls import AugclsOp
-from .chains import ChainSpec, chains_adjoint, chains_run
+from .chains import ChainSpec, chains_adjoint_ext, chains_run
 
 ORB_L = (0, 1, 1, 1, 2, 2, 2, 2, 2)   # l of the nine orbitals s | y z x | xy yz 3z2-r2 xz x2-y2
 
@@ -28,11 +29,11 @@ def _arr(t: torch.Tensor) -> np.ndarray:
     return np.asfortranarray(t.detach().cpu().numpy().astype(np.float64).T)
 
 
-def _specs(c, d, e, pa, pb, groups):
+def _specs(c, d, e, pa, pb, groups, o=None):
     out = []
     for q, (frozen_sp, start_orb, nlev) in enumerate(groups):
-        z9 = np.zeros((9, c.shape[1]), order="F")
-        out.append(ChainSpec(c=_arr(c[q]), d=_arr(d[q]), o=z9, e=_arr(e[q]), pa=_arr(pa[q]), pb=_arr(pb[q]),
+        oq = _arr(o[q]) if o is not None else np.zeros((9, c.shape[1]), order="F")
+        out.append(ChainSpec(c=_arr(c[q]), d=_arr(d[q]), o=oq, e=_arr(e[q]), pa=_arr(pa[q]), pb=_arr(pb[q]),
                              frozen_sp=int(frozen_sp), start_orb=int(start_orb), nlev=int(nlev)))
     return out
 
@@ -40,35 +41,42 @@ def _specs(c, d, e, pa, pb, groups):
 class ChainGreens(torch.autograd.Function):
     """G (ngroup, nz) complex128 of the edc chain groups.
 
-    Inputs: c, d, e, pa, pb -- (ngroup, nsp, 9) float64 tensors (each group's (9, nsp) arrays; o = 0); op -- the
-    operator; groups -- [(frozen_sp, start_orb, nlev)] per group; z (nz) complex energies; tail ('none' | 'hull' |
-    'avg2'); precision ('fp64' | 'fp32'); project; stride (checkpoint spacing, 0: sqrt(depth)).
+    Inputs: c, d, e, pa, pb -- (ngroup, nsp, 9) float64 tensors (each group's (9, nsp) arrays); o -- the same shape or
+    None (o = 0); op -- the operator; groups -- [(frozen_sp, start_orb, nlev)] per group; z (nz) complex energies; tail
+    ('none' | 'hull' | 'bp' | 'avg2'); precision ('fp64' | 'fp32'); project; stride (checkpoint spacing, 0: sqrt(depth));
+    depth_tol (> 0: the depth test of src/asr_edc.f90:121-127, the derivative taken at the depth each chain stopped at).
 
     The backward pass gives d(real loss)/dpar = Re(sum conj(dL/dG) dG/dpar): the seeds of the adjoint are the conjugated
-    output gradients.  c, e and pb enter the operator only as c + e + pb and share one derivative."""
+    output gradients.  e and pb enter the operator the same way and share one derivative (and c with them when o = 0)."""
 
     @staticmethod
-    def forward(ctx, c, d, e, pa, pb, op: AugclsOp, groups, z, tail="hull", precision="fp64", project=True, stride=0):
-        specs = _specs(c, d, e, pa, pb, groups)
+    def forward(ctx, c, d, e, pa, pb, o, op: AugclsOp, groups, z, tail="hull", precision="fp64", project=True, stride=0,
+                depth_tol=0.0):
+        specs = _specs(c, d, e, pa, pb, groups, o)
         z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
-        g = chains_run(op, specs, z, "edc", 0.0, tail, precision, project)["g"]
+        g = chains_run(op, specs, z, "edc", depth_tol, tail, precision, project)["g"]
         ctx.save_for_backward(c, d, e, pa, pb)
-        ctx.meta = (op, list(groups), z, tail, precision, project, stride)
+        ctx.o = o.detach() if o is not None else None
+        ctx.meta = (op, list(groups), z, tail, precision, project, stride, depth_tol)
         return torch.from_numpy(np.ascontiguousarray(g.T)).to(c.device)
 
     @staticmethod
     def backward(ctx, gout):
         c, d, e, pa, pb = ctx.saved_tensors
-        op, groups, z, tail, precision, project, stride = ctx.meta
+        op, groups, z, tail, precision, project, stride, depth_tol = ctx.meta
         w = np.conj(gout.detach().cpu().numpy()).T
-        _, gr = chains_adjoint(op, _specs(c, d, e, pa, pb, groups), z, w, tail, precision, project, stride)
+        _, _, gr = chains_adjoint_ext(op, _specs(c, d, e, pa, pb, groups, ctx.o), z, w, depth_tol, tail, precision, project,
+                                      stride)
         gr = torch.from_numpy(np.ascontiguousarray(gr.real)).to(device=c.device, dtype=c.dtype)
-        g0 = gr[:, 0]
-        return g0, gr[:, 1], g0.clone(), gr[:, 2], g0.clone(), None, None, None, None, None, None, None
+        ge = gr[:, 4]
+        go = gr[:, 3] if ctx.o is not None else None
+        return gr[:, 0], gr[:, 1], ge, gr[:, 2], ge.clone(), go, None, None, None, None, None, None, None, None
 
 
-def chain_greens(c, d, e, pa, pb, op, groups, z, tail="hull", precision="fp64", project=True, stride=0):
-    return ChainGreens.apply(c, d, e, pa, pb, op, groups, z, tail, precision, project, stride)
+def chain_greens(c, d, e, pa, pb, op, groups, z, tail="hull", precision="fp64", project=True, stride=0, o=None,
+                 depth_tol=0.0):
+    """G (ngroup, nz) of the edc chain groups, differentiable in c, d, e, pa, pb and (when given) o."""
+    return ChainGreens.apply(c, d, e, pa, pb, o, op, groups, z, tail, precision, project, stride, depth_tol)
 
 
 def orbital_orbits(dmat) -> list[list[int]]:
@@ -107,6 +115,14 @@ def edc_group_arrays(cl, dl, Dl, enu, central: int):
     dc = D[central - 1]
     r = dc[None, :] / D
     return r * c, d[central - 1][None, :].expand_as(d), torch.zeros_like(c), 1.0 - r, r * en
+
+
+def edc_group_o(ol, Dl, central: int):
+    """o of ``edc_setup`` (src/asr_edc.f90:66) in torch: o_s = o_l,s D_s / D_c per (species, orbital), from the per-l
+    o_l (nsp, 3) of every species (o of the alpha representation, ``o_alpha`` src/asr_lmto_ham.f90:131-139) and the
+    Delta_l (nsp, 3); central 1-based.  Returns (nsp, 9)."""
+    o, D = per_orbital(ol), per_orbital(Dl)
+    return o * D / D[central - 1][None, :]
 
 
 def contour_moments(g: torch.Tensor, z, w, enu, kmax: int = 1) -> torch.Tensor:

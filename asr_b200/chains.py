@@ -102,6 +102,29 @@ def chains_adjoint(op: AugclsOp, specs, z, w, tail: str = "hull", precision: str
     return g.T, grad
 
 
+KINDS_EXT = ("c", "d", "pa", "o", "e")
+
+
+def chains_adjoint_ext(op: AugclsOp, specs, z, w, depth_tol: float = 0.0, tail: str = "hull", precision: str = "fp64",
+                       project: bool = True, stride: int = 0):
+    """Reverse mode of the energy-dependent chains on the whole operator form H = E_nu + h - h o h + X(z) (o != 0 allowed),
+    with the depth test of src/asr_edc.f90:121-127 when depth_tol > 0 (the derivative at the depth each chain stopped at)
+    and every tail.  Returns (g (nz, ngroup), m (nz, ngroup), grad) with grad[q, kind, s, l] = sum_j w[j, q]
+    dG[j, q] / dpar_kind(l, s), kinds ``KINDS_EXT`` = c, d, pa, o, e (pb enters as e does)."""
+    z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
+    nz = z.shape[0]
+    ng = len(specs)
+    w = np.asarray(w, np.complex128).reshape(nz, ng)
+    wl = np.ascontiguousarray(w.T)
+    arr, keep = _groups(specs)
+    g = np.zeros((ng, nz), np.complex128)
+    m = np.zeros((ng, nz), np.int32)
+    grad = np.zeros((ng, 5, op.nsp, 9), np.complex128)
+    check(lib().asr_chains_adjoint_ext(op.ctx.h, op.h, arr, ng, _pd(z), nz, _pd(wl), float(depth_tol), _lib.TAILS[tail],
+                                       PREC[precision], int(bool(project)), int(stride), _pd(g), _pi(m), _pd(grad)))
+    return g.T, m.T, grad
+
+
 def ed3_blocks(op: AugclsOp, groups, z, depth_tol: float = 0.0, tail: str = "hull", precision: str = "fp64",
                project: bool = True, coefs: bool = False):
     """``ed3_blocks`` (src/asr_ed3.f90:242-265) for every group at every energy.  groups: dicts with g, d, o, p, dl, enu

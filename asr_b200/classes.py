@@ -23,10 +23,10 @@ class SublatticeChains:
     that sublattice (the same alloy with shifted site classes); nlev: chain depth."""
 
     def __init__(self, cases, nlev: int, ctx: Context | None = None, tail: str = "hull", precision: str = "fp64",
-                 project: bool = True):
+                 project: bool = True, depth_tol: float = 0.0):
         self.cases = cases
         self.nlev = nlev
-        self.tail, self.precision, self.project = tail, precision, project
+        self.tail, self.precision, self.project, self.depth_tol = tail, precision, project, depth_tol
         self.ops = [build_augcls_operator(c["graph"], c["model"], c["cls"], c["perm"], c["dmat"], 1, c["maxlevel"],
                                           maxrank=c["maxrank"], flippable=c["flippable"], ctx=ctx) for c in cases]
         self.nsp = cases[0]["model"].nsp
@@ -46,23 +46,28 @@ class SublatticeChains:
                 wts.append(len(orb))
         return out, wts
 
-    def greens(self, cl, dl, Dl, enu, z):
-        """G per sublattice: list of (ngroup, nz) complex tensors (component-major, then orbit)."""
+    def greens(self, cl, dl, Dl, enu, z, ol=None):
+        """G per sublattice: list of (ngroup, nz) complex tensors (component-major, then orbit).  ol (nsp, 3): o_l of every
+        species (edc_setup's o = o_l D_s / D_c, src/asr_edc.f90:66); None: o = 0."""
         out = []
         for kap, op in enumerate(self.ops):
             groups, _ = self.groups(kap)
             arrs = [[], [], [], [], []]
+            oarr = []
             for sp, _, _ in groups:
                 for a, v in zip(arrs, AG.edc_group_arrays(cl, dl, Dl, enu, sp)):
                     a.append(v)
+                if ol is not None:
+                    oarr.append(AG.edc_group_o(ol, Dl, sp))
             stk = [torch.stack(a) for a in arrs]
-            out.append(AG.chain_greens(*stk, op, groups, z, self.tail, self.precision, self.project))
+            out.append(AG.chain_greens(*stk, op, groups, z, self.tail, self.precision, self.project,
+                                       o=torch.stack(oarr) if ol is not None else None, depth_tol=self.depth_tol))
         return out
 
-    def energy_and_charges(self, cl, dl, Dl, enu, z, w):
+    def energy_and_charges(self, cl, dl, Dl, enu, z, w, ol=None):
         """Band energy sum_kap sum_s x_s sum_l (M_1 + E_nu M_0) and sublattice charges Q_kap = sum_s x_s sum_l M_0 from the
         contour (z, w); the moments are taken about E_nu of each (species, orbital)."""
-        gs = self.greens(cl, dl, Dl, enu, z)
+        gs = self.greens(cl, dl, Dl, enu, z, ol)
         e_band = torch.zeros((), dtype=torch.float64)
         q = []
         for kap, g in enumerate(gs):
@@ -74,3 +79,17 @@ class SublatticeChains:
             q.append(torch.sum(x * wt * mo[:, 0]))
             e_band = e_band + torch.sum(x * wt * (mo[:, 1] + en * mo[:, 0]))
         return e_band, torch.stack(q)
+
+    def dos(self, cl, dl, Dl, enu, e, eta: float, ol=None):
+        """DOS per sublattice on the real axis, -(1/pi) Im sum_s x_s sum_o w_o G_o(e + i eta) (the l-summed form of
+        ``dos_final``, src/asr_class_scf.f90:1912-1931), differentiable in the species parameters: a list of (ne,) tensors."""
+        import numpy as np
+        z = np.asarray(e, dtype=np.float64) + 1j * eta
+        gs = self.greens(cl, dl, Dl, enu, z, ol)
+        out = []
+        for kap, g in enumerate(gs):
+            groups, wts = self.groups(kap)
+            x = torch.tensor([dict(self.comps[kap])[sp] for sp, _, _ in groups], dtype=torch.float64)
+            wt = torch.tensor(wts, dtype=torch.float64)
+            out.append(-torch.sum((x * wt)[:, None] * torch.imag(g), dim=0) / np.pi)
+        return out

@@ -873,26 +873,31 @@ int asr_ed3_blocks(asr_ctx* ctx, asr_op* op, const asr_ed3_group* groups, int ng
   return ASR_OK;
 }
 
-int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz,
-                       const double* w, int tail, int precision, int project, int stride, double* g, double* grad) {
-  if (!ctx || !op || !groups || ngroup < 1 || nz < 1 || !z || !w || !grad) { set_error("asr_chains_adjoint: bad argument"); return ASR_EINVAL; }
-  if (tail != ASR_TAIL_NONE && tail != ASR_TAIL_HULL && tail != ASR_TAIL_AVG2) {
-    set_error("asr_chains_adjoint: tail must be none, hull or avg2");
-    return ASR_EINVAL;
-  }
+// the adjoint of the edc chains for every (group, energy) lane; grad receives nkind kinds (the first nkind of c, d, pa,
+// o, e), symmetrised over the orbits of the orbitals under the point group
+static int chains_adjoint_common(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz,
+                                 const double* w, double depth_tol, int tail, int precision, int project, int stride,
+                                 double* g, int* mused, double* grad, int nkind, const char* who) {
+  if (!ctx || !op || !groups || ngroup < 1 || nz < 1 || !z || !w || !grad) { set_error("%s: bad argument", who); return ASR_EINVAL; }
+  if (tail < ASR_TAIL_NONE || tail > ASR_TAIL_AVG2) { set_error("%s: unknown tail", who); return ASR_EINVAL; }
+  if (depth_tol < 0.0) { set_error("%s: depth_tol must be >= 0", who); return ASR_EINVAL; }
   ASR_ON_DEVICE(ctx->device);
   GroupLayout GL = layout(op);
   std::vector<double> blob((size_t)GL.stride * ngroup, 0.0);
   std::vector<GroupInfo> gi(ngroup);
   for (int q = 0; q < ngroup; ++q) {
     const asr_chain_group& G = groups[q];
-    if (!G.c || !G.d || !G.pa || !G.pb) { set_error("asr_chains_adjoint: group %d needs c, d, pa, pb", q + 1); return ASR_EINVAL; }
-    if (G.nlev < 1 || G.nlev > NLMAX) { set_error("asr_chains_adjoint: depth %d out of range 1..%d", G.nlev, NLMAX); return ASR_EINVAL; }
+    if (!G.c || !G.d || !G.pa || !G.pb) { set_error("%s: group %d needs c, d, pa, pb", who, q + 1); return ASR_EINVAL; }
+    if (G.nlev < 1 || G.nlev > NLMAX) { set_error("%s: depth %d out of range 1..%d", who, G.nlev, NLMAX); return ASR_EINVAL; }
     ASR_TRY(make_group(op, GL, G.c, G.d, G.o, G.e, G.pa, G.pb, G.frozen_sp, G.start_orb, G.nlev, nullptr,
                        blob.data() + (size_t)GL.stride * q, gi[q]));
+    if (nkind < 5 && !(gi[q].flags & GF_O_ZERO)) {
+      set_error("%s: group %d has o != 0; asr_chains_adjoint_ext differentiates that operator", who, q + 1);
+      return ASR_EINVAL;
+    }
   }
   const int nlane = ngroup * nz;
-  std::vector<int> lg(nlane);
+  std::vector<int> lg(nlane), hm;
   std::vector<double2> lz(nlane), lw(nlane), hg, hgrad;
   for (int q = 0; q < ngroup; ++q)
     for (int j = 0; j < nz; ++j) {
@@ -901,11 +906,12 @@ int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
       lz[L] = make_double2(z[2 * j], z[2 * j + 1]);
       lw[L] = make_double2(w[2 * L], w[2 * L + 1]);
     }
-  int rc = run_adjoint(ctx, op, gi, blob, GL, lg, lz, lw, tail, project, stride, precision, hg, hgrad);
+  int rc = run_adjoint(ctx, op, gi, blob, GL, lg, lz, lw, depth_tol, tail, project, stride, precision, hg, hm, hgrad);
   if (rc != ASR_OK) return rc;
   if (g)
     for (int L = 0; L < nlane; ++L) { g[2 * L] = hg[L].x; g[2 * L + 1] = hg[L].y; }
-  const int nsp = op->nsp;
+  if (mused) for (int L = 0; L < nlane; ++L) mused[L] = hm[L];
+  const int nsp = op->nsp, nk = 5;
   // orbits of the orbitals under the point group (pi of every operation): the group-reduced operator represents
   // only parameters that are constant on each orbit, so the gradient is reported symmetrised over the orbits -- exact
   // along every invariant direction (per l, per irreducible orbit), while the single orbitals of a degenerate orbit are
@@ -920,28 +926,34 @@ int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, 
         if (orbit[l] != r || orbit[m] != r) { orbit[l] = orbit[m] = r; changed = true; }
       }
   }
-  std::vector<double2> sym(hgrad.size(), make_double2(0, 0));
   for (int q = 0; q < ngroup; ++q)
-    for (int kind = 0; kind < 3; ++kind)
+    for (int kind = 0; kind < nkind; ++kind)
       for (int sp = 0; sp < nsp; ++sp)
         for (int l = 0; l < 9; ++l) {
           double2 acc = make_double2(0, 0);
           int cnt = 0;
           for (int l2 = 0; l2 < 9; ++l2)
-            if (orbit[l2] == orbit[l]) { acc = cadd(acc, hgrad[(((size_t)q * 3 + kind) * 9 + l2) * nsp + sp]); ++cnt; }
-          sym[(((size_t)q * 3 + kind) * 9 + l) * nsp + sp] = cscale(acc, 1.0 / cnt);
-        }
-  for (int q = 0; q < ngroup; ++q)
-    for (int kind = 0; kind < 3; ++kind)
-      for (int l = 0; l < 9; ++l)
-        for (int sp = 0; sp < nsp; ++sp) {
-          double2 v = sym[(((size_t)q * 3 + kind) * 9 + l) * nsp + sp];
-          size_t dst = 2 * (l + 9 * (sp + (size_t)nsp * (kind + 3 * (size_t)q)));
+            if (orbit[l2] == orbit[l]) { acc = cadd(acc, hgrad[(((size_t)q * nk + kind) * 9 + l2) * nsp + sp]); ++cnt; }
+          double2 v = cscale(acc, 1.0 / cnt);
+          size_t dst = 2 * (l + 9 * (sp + (size_t)nsp * (kind + (size_t)nkind * q)));
           grad[dst] = v.x;
           grad[dst + 1] = v.y;
         }
   ctx->nchain += nlane;
   return ASR_OK;
+}
+
+int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz,
+                       const double* w, int tail, int precision, int project, int stride, double* g, double* grad) {
+  return chains_adjoint_common(ctx, op, groups, ngroup, z, nz, w, 0.0, tail, precision, project, stride, g, nullptr, grad, 3,
+                               "asr_chains_adjoint");
+}
+
+int asr_chains_adjoint_ext(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz,
+                           const double* w, double depth_tol, int tail, int precision, int project, int stride, double* g,
+                           int* mused, double* grad) {
+  return chains_adjoint_common(ctx, op, groups, ngroup, z, nz, w, depth_tol, tail, precision, project, stride, g, mused, grad, 5,
+                               "asr_chains_adjoint_ext");
 }
 
 // chain_worker tasks as explicit lanes (edc route): lane L runs group lane_group[L] (1-based) at the energy lane_z[L]

@@ -1303,15 +1303,26 @@ __global__ void __launch_bounds__(WPB * TL) k_adj_u(OpView op, BatchView bv, con
   }
 }
 
-// gradient partials of one reverse step: thread (orbital l = warp, lane); per block and kind (c-like, d, pa) the sums
-// over its nodes and the 32 lanes: gpart[((tile * gbpt + blk) * 3 + kind) * 9 * nsp + l * nsp + species]
-template <typename ST>
+// gradient partials of one reverse step: thread (orbital l = warp, lane); per block and kind the sums over its nodes and
+// the 32 lanes: gpart[((tile * gbpt + blk) * NGK + kind) * 9 * nsp + l * nsp + species], kinds 0 c, 1 d, 2 pa, 3 o, 4 e
+// (e and pb enter the same way).  With G_p(x, v) = x . (dR_p / dpar) v (x at the node, v through the flip links with the
+// class weights mt, or the node itself on a frozen site) and A = h - h O h + E + X(z), h = C + D S D:
+//   c: G(yb, u) - G(yb, O h u) - G(O h yb, u)
+//   d: Gh(yb, u) - Gh(yb, O h u) - Gh(O h yb, u),  Gh(x, v) = G_d(x, S D v) + G_d(S D x, v)
+//   o: -G(h yb, h u);  e: G(yb, u);  pa: z G(yb, u)
+// GEN = false (O = 0): the last two terms of c and d and the o kind vanish, and the operator's intermediates are not read.
+constexpr int NGK = 5;
+struct AdjVecs {   // per level: node side (yb: ybar; tb = S D ybar; hb = h ybar; rb = O h ybar; qb = S D O h ybar) and link
+                   // side (unscaled X_k; tk = S D X_k; hk = h X_k; rk = O h X_k; qk = S D O h X_k)
+  const void *yb, *tb, *hb, *rb, *qb;
+  const void *xk, *tk, *hk, *rk, *qk;
+};
+template <typename ST, bool GEN>
 __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, const double* mt, const int* spc, int ldspc,
-                                                       const typename St2<ST>::T* __restrict__ yb,
-                                                       const typename St2<ST>::T* __restrict__ t2b,
-                                                       const typename St2<ST>::T* __restrict__ xk,
-                                                       const typename St2<ST>::T* __restrict__ t2k, const double2* sk, int nodes_per_block,
-                                                       double2* gpart) {
+                                                       AdjVecs V, const double2* sk, int nodes_per_block, double2* gpart) {
+  typedef typename St2<ST>::T T2;
+  const T2 *yb = (const T2*)V.yb, *tb = (const T2*)V.tb, *hb = (const T2*)V.hb, *rb = (const T2*)V.rb, *qb = (const T2*)V.qb;
+  const T2 *xk = (const T2*)V.xk, *tk = (const T2*)V.tk, *hk = (const T2*)V.hk, *rk = (const T2*)V.rk, *qk = (const T2*)V.qk;
   const int gbpt = (bv.nn + nodes_per_block - 1) / nodes_per_block;
   const int tile = blockIdx.x / gbpt, blk = blockIdx.x % gbpt;
   if (tile >= bv.ntile || !bv.tile_act[tile]) return;
@@ -1319,75 +1330,96 @@ __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, 
   const int L = tile * TL + lane;
   const int grp = bv.tile_group[tile];
   const int nsp = op.nsp, nsm = op.nsmax;
-  double2 g1[MAXSP], gd[MAXSP], gpa[MAXSP];
-  for (int q = 0; q < MAXSP; ++q) { g1[q] = make_double2(0, 0); gd[q] = g1[q]; gpa[q] = g1[q]; }
+  double2 gc[MAXSP], gd[MAXSP], ge[MAXSP], go[MAXSP];   // pa = z e-kind
+  for (int q = 0; q < MAXSP; ++q) { gc[q] = make_double2(0, 0); gd[q] = gc[q]; ge[q] = gc[q]; go[q] = gc[q]; }
   const bool live = bv.lane_group[L] >= 0 && grp >= 0;
+  double2 z = make_double2(0, 0);
   if (live) {
     const GroupInfo gi = bv.ginfo[grp];
-    const double2 s = sk[L], z = bv.lane_z[L];
+    const double2 s = sk[L];
+    z = bv.lane_z[L];
     const int i0 = blk * nodes_per_block, i1 = min(bv.nn, i0 + nodes_per_block);
     for (int i = i0; i < i1; ++i) {
       size_t q = vix(tile, bv.nn, i, l) + lane;
-      double2 ybv = ld(yb + q), tbv = ld(t2b + q);
-      double2 x = cmul(s, ld(xk + q)), t = cmul(s, ld(t2k + q));
-      double nb = op.sq[i] * op.sq[i];
-      int fs = frozen_of(op, gi, i);
-      if (fs > 0) {
-        double2 q1 = cscale(cmul(ybv, x), nb);
-        g1[fs - 1] = cadd(g1[fs - 1], q1);
-        gd[fs - 1] = cadd(gd[fs - 1], cscale(cadd(cmul(ybv, t), cmul(tbv, x)), nb));
-        gpa[fs - 1] = cadd(gpa[fs - 1], cmul(z, q1));
-        continue;
-      }
-      int kap = op.ncl[i], own = op.lst[i], nk = op.nsc[kap];
-      for (int kp = 0; kp < nk; ++kp) {
-        double2 lx, lt;
-        if (kp == own) { lx = x; lt = t; }
-        else {
+      const double2 y = ld(yb + q), ty = ld(tb + q);
+      double2 hy = make_double2(0, 0), ry = hy, qy = hy;
+      if (GEN) { hy = ld(hb + q); ry = ld(rb + q); qy = ld(qb + q); }
+      const double nb = op.sq[i] * op.sq[i];
+      const int fs = frozen_of(op, gi, i);
+      const int kap = op.ncl[i], own = op.lst[i], nk = op.nsc[kap];
+      const int nlink = fs > 0 ? 1 : nk;
+      for (int kp = 0; kp < nlink; ++kp) {
+        size_t qr = q;
+        double sgn = 1.0;
+        if (fs == 0 && kp != own) {
           int r = op.flipr[kp + nsm * i];
           if (r < 0) continue;
           int g = op.flipg[kp + nsm * i];
           bool neg = (gi.chimask >> g) & 1ull;
-          double sgn = ((((uint32_t)op.sgm[g] >> l) & 1u) ^ (neg ? 1u : 0u)) ? -1.0 : 1.0;
-          size_t qr = vix(tile, bv.nn, r, op.pi[g * 9 + l]) + lane;
-          lx = cscale(cmul(s, ld(xk + qr)), sgn);
-          lt = cscale(cmul(s, ld(t2k + qr)), sgn);
+          sgn = ((((uint32_t)op.sgm[g] >> l) & 1u) ^ (neg ? 1u : 0u)) ? -1.0 : 1.0;
+          qr = vix(tile, bv.nn, r, op.pi[g * 9 + l]) + lane;
         }
-        double2 q1 = cscale(cmul(ybv, lx), nb);
-        double2 qd = cscale(cadd(cmul(ybv, lt), cmul(tbv, lx)), nb);
+        const double2 x = cscale(cmul(s, ld(xk + qr)), sgn), t = cscale(cmul(s, ld(tk + qr)), sgn);
+        double2 qe = cmul(y, x);                                          // G(yb, u)
+        double2 qc = qe, qd = cadd(cmul(y, t), cmul(ty, x)), qo = make_double2(0, 0);
+        if (GEN) {
+          const double2 hx = cscale(cmul(s, ld(hk + qr)), sgn), rx = cscale(cmul(s, ld(rk + qr)), sgn);
+          const double2 qx = cscale(cmul(s, ld(qk + qr)), sgn);
+          qc = csub(csub(qe, cmul(y, rx)), cmul(ry, x));
+          qd = csub(csub(qd, cadd(cmul(y, qx), cmul(ty, rx))), cadd(cmul(ry, t), cmul(qy, x)));
+          qo = csub(make_double2(0, 0), cmul(hy, hx));
+        }
+        qe = cscale(qe, nb); qc = cscale(qc, nb); qd = cscale(qd, nb); qo = cscale(qo, nb);
+        if (fs > 0) {
+          ge[fs - 1] = cadd(ge[fs - 1], qe);
+          gd[fs - 1] = cadd(gd[fs - 1], qd);
+          if (GEN) { gc[fs - 1] = cadd(gc[fs - 1], qc); go[fs - 1] = cadd(go[fs - 1], qo); }
+          continue;
+        }
         for (int sidx = 0; sidx < nk; ++sidx) {
           double m = mt[own + nsm * (kp + nsm * (sidx + (size_t)nsm * kap))];
           if (m == 0.0) continue;
           int sp = spc[sidx + ldspc * kap] - 1;
-          g1[sp] = cadd(g1[sp], cscale(q1, m));
+          ge[sp] = cadd(ge[sp], cscale(qe, m));
           gd[sp] = cadd(gd[sp], cscale(qd, m));
-          gpa[sp] = cadd(gpa[sp], cmul(z, cscale(q1, m)));
+          if (GEN) { gc[sp] = cadd(gc[sp], cscale(qc, m)); go[sp] = cadd(go[sp], cscale(qo, m)); }
         }
       }
     }
   }
-  // sum over the 32 lanes (one warp = one orbital), fixed order
+  // sum over the 32 lanes (one warp = one orbital), fixed order; pa = z e per lane before the sum
+  double2 gpa[MAXSP];
+  for (int q = 0; q < nsp; ++q) {
+    gpa[q] = cmul(z, ge[q]);
+    if (!GEN) gc[q] = ge[q];   // o = 0: c enters as e does
+  }
   for (int q = 0; q < nsp; ++q) {
     for (int off = 16; off > 0; off >>= 1) {
-      g1[q].x += __shfl_xor_sync(0xffffffffu, g1[q].x, off);
-      g1[q].y += __shfl_xor_sync(0xffffffffu, g1[q].y, off);
+      gc[q].x += __shfl_xor_sync(0xffffffffu, gc[q].x, off);
+      gc[q].y += __shfl_xor_sync(0xffffffffu, gc[q].y, off);
       gd[q].x += __shfl_xor_sync(0xffffffffu, gd[q].x, off);
       gd[q].y += __shfl_xor_sync(0xffffffffu, gd[q].y, off);
       gpa[q].x += __shfl_xor_sync(0xffffffffu, gpa[q].x, off);
       gpa[q].y += __shfl_xor_sync(0xffffffffu, gpa[q].y, off);
+      go[q].x += __shfl_xor_sync(0xffffffffu, go[q].x, off);
+      go[q].y += __shfl_xor_sync(0xffffffffu, go[q].y, off);
+      ge[q].x += __shfl_xor_sync(0xffffffffu, ge[q].x, off);
+      ge[q].y += __shfl_xor_sync(0xffffffffu, ge[q].y, off);
     }
   }
   if (lane == 0) {
-    double2* out = gpart + ((size_t)(tile * gbpt + blk) * 3) * 9 * nsp;
+    double2* out = gpart + ((size_t)(tile * gbpt + blk) * NGK) * 9 * nsp;
     for (int q = 0; q < nsp; ++q) {
-      out[(0 * 9 + l) * nsp + q] = g1[q];
+      out[(0 * 9 + l) * nsp + q] = gc[q];
       out[(1 * 9 + l) * nsp + q] = gd[q];
       out[(2 * 9 + l) * nsp + q] = gpa[q];
+      out[(3 * 9 + l) * nsp + q] = go[q];
+      out[(4 * 9 + l) * nsp + q] = ge[q];
     }
   }
 }
 
-// gacc[tile][3][9][nsp] += sum over the blocks of the step's partials (fixed order)
+// gacc[tile][NGK][9][nsp] += sum over the blocks of the step's partials (fixed order)
 __global__ void k_adj_gsum(int ntile, int gbpt, int ng, const int* tile_act, const double2* gpart, double2* gacc) {
   int tile = blockIdx.x;
   if (tile >= ntile || !tile_act[tile]) return;
@@ -1494,19 +1526,33 @@ void apply_SD(asr_op* op, const BatchView& bv, bool dunif, const typename St2<ST
   }
 }
 
+// y = s (h x - h O h x + (E + X) x) on the general operator with its intermediates kept: TA = S D x, H = h x, R = O h x,
+// TB = S D O h x (unscaled), and the partial dots of the final combination
+template <typename ST>
+void apply_general_keep(asr_op* op, const BatchView& bv, bool dunif, const typename St2<ST>::T* x, typename St2<ST>::T* y,
+                        typename St2<ST>::T* TA, typename St2<ST>::T* H, typename St2<ST>::T* R, typename St2<ST>::T* TB,
+                        typename St2<ST>::T* TMP, double2* part, int npw, int grid, cudaStream_t s) {
+  OpView ov = op->view();
+  apply_SD<ST>(op, bv, dunif, x, TMP, TA, part, npw, grid, s);
+  k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TA, x, PC, false, x, false, nullptr, 1.0, false, H, part, npw);
+  k_rand<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, PO, H, R, npw);
+  apply_SD<ST>(op, bv, dunif, R, TMP, TB, part, npw, grid, s);
+  k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TB, R, PC, false, x, true, H, -1.0, true, y, part, npw);
+}
+
 template <typename ST>
 int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
                   const GroupLayout& GL, const std::vector<int>& lane_group, const std::vector<double2>& lane_z,
-                  const std::vector<double2>& lane_w, int tail, int project, int stride, std::vector<double2>& g_out,
-                  std::vector<double2>& grad_out /* [group][3][9][nsp] */) {
+                  const std::vector<double2>& lane_w, double depth_tol, int tail, int project, int stride,
+                  std::vector<double2>& g_out, std::vector<int>& m_out, std::vector<double2>& grad_out /* [group][NGK][9][nsp] */) {
   typedef typename St2<ST>::T T2;
   cudaStream_t s = ctx->stream;
   const int nn = op->nn, nsp = op->nsp, nlane = (int)lane_group.size();
   if (nsp > MAXSP) { set_error("adjoint: at most %d species", MAXSP); return ASR_EINVAL; }
-  bool dunif = true;
+  bool dunif = true, gen = false;
   int mmax = 0;
   for (auto& g : ginfo) {
-    if (!(g.flags & GF_O_ZERO)) { set_error("adjoint: o must be zero (H = E_nu + h)"); return ASR_EINVAL; }
+    if (!(g.flags & GF_O_ZERO)) gen = true;   // H = E_nu + h - h o h: the general operator and its intermediates
     if (!(g.flags & GF_D_UNIFORM)) dunif = false;
     mmax = std::max(mmax, g.nlev);
   }
@@ -1523,9 +1569,10 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         tiles.emplace_back(lst.begin() + q, lst.begin() + std::min(lst.size(), q + (size_t)TL));
   }
   const int ntile_all = (int)tiles.size();
-  // memory: forward 3 + checkpoints 2 nseg + segment (c + 2) X + c Y + c T2 + adjoint 7 (+1 temporary) vectors per tile
+  // memory: forward 3 + checkpoints 2 nseg + segment (c + 2) X + c Y + c T2 + adjoint 7 (+1 temporary) vectors per tile;
+  // the general operator keeps h X, O h X, S D O h X per segment level and h ybar, O h ybar, S D O h ybar (3 c + 3 more)
   const size_t vec_bytes = (size_t)nn * 9 * TL * sizeof(T2);
-  const int nvec = 3 + 2 * nseg + (c + 2) + 2 * c + 8;
+  const int nvec = 3 + 2 * nseg + (c + 2) + 2 * c + 8 + (gen ? 3 * c + 3 : 0);
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
   int tpb = 4;
@@ -1534,7 +1581,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   if ((size_t)nvec * vec_bytes > freeb) { set_error("adjoint: %d vectors of %zu bytes do not fit", nvec, vec_bytes); return ASR_ENOMEM; }
   tpb = std::min(tpb, ntile_all);
   const int npw = 4, npb = WPB * npw, bpt = (nn + npb - 1) / npb;
-  const int gnpb = 64, gbpt = (nn + gnpb - 1) / gnpb, ngd = 3 * 9 * nsp;
+  const int gnpb = 64, gbpt = (nn + gnpb - 1) / gnpb, ngd = NGK * 9 * nsp;
   const int nlp = tpb * TL;
   Dev<double> d_gblob, d_mt;
   Dev<GroupInfo> d_ginfo;
@@ -1574,7 +1621,15 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   T2* T2B = V[ab0 + 5].p;
   T2* AY = V[ab0 + 6].p;
   T2* TMP = V[ab0 + 7].p;
+  const int gs0 = ab0 + 8;   // general operator: per segment level q the intermediates of X, then those of ybar
+  auto HS = [&](int q) { return gen ? V[gs0 + q].p : nullptr; };
+  auto RS = [&](int q) { return gen ? V[gs0 + c + q].p : nullptr; };
+  auto QS = [&](int q) { return gen ? V[gs0 + 2 * c + q].p : nullptr; };
+  T2* HB = gen ? V[gs0 + 3 * c].p : nullptr;
+  T2* RB = gen ? V[gs0 + 3 * c + 1].p : nullptr;
+  T2* QB = gen ? V[gs0 + 3 * c + 2].p : nullptr;
   g_out.assign(nlane, make_double2(0, 0));
+  m_out.assign(nlane, 0);
   grad_out.assign(ginfo.size() * (size_t)ngd, make_double2(0, 0));
   std::vector<double2> ones(nlp, make_double2(1.0, 0.0));
   ASR_CUDA(cudaMemcpyAsync(d_one.p, ones.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
@@ -1608,9 +1663,11 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     ASR_CUDA(cudaMemsetAsync(d_sup.p, 0, nlp * sizeof(double2), s));
     ASR_CUDA(cudaMemsetAsync(d_nfall.p, 0, sizeof(int), s));
     ASR_CUDA(cudaMemsetAsync(d_gacc.p, 0, (size_t)tpb * ngd * sizeof(double2), s));
-    BatchView bv{nt, nn, op->nsmax, 0, ASR_MODE_EDC, project, tail, NLMAX, 0.0, d_gblob.p, GL, d_ginfo.p, d_lgroup.p, d_tgroup.p,
-                 d_z.p, d_act.p, d_wact.p, d_m.p, d_a.p, d_b.p, d_gprev.p, d_acur.p, d_bprev.p, d_su.p, d_sup.p, d_tact.p,
-                 d_nfall.p};
+    // the forward stops each lane by the depth test of src/asr_edc.f90:121-127 when depth_tol > 0; the reverse sweep then
+    // differentiates the chain at the depth it stopped at
+    BatchView bv{nt, nn, op->nsmax, 0, ASR_MODE_EDC, project, tail, NLMAX, depth_tol, d_gblob.p, GL, d_ginfo.p, d_lgroup.p,
+                 d_tgroup.p, d_z.p, d_act.p, d_wact.p, d_m.p, d_a.p, d_b.p, d_gprev.p, d_acur.p, d_bprev.p, d_su.p, d_sup.p,
+                 d_tact.p, d_nfall.p};
     const int grid = nt * bpt;
     int kmax = 0;
     for (int q = 0; q < nlp; ++q) if (hgroup[q] >= 0) kmax = std::max(kmax, ginfo[hgroup[q]].nlev);
@@ -1623,8 +1680,12 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
       T2* U = FW[k % 3];
       T2* UP = FW[(k + 2) % 3];
       T2* Y = FW[(k + 1) % 3];
-      apply_SD<ST>(op, bv, dunif, U, TMP, AY, d_part.p, npw, grid, s);
-      k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, AY, U, PCEB, true, U, false, nullptr, 1.0, true, Y, d_part.p, npw);
+      if (gen) {
+        apply_general_keep<ST>(op, bv, dunif, U, Y, AY, WB, YB, T2B, TMP, d_part.p, npw, grid, s);
+      } else {
+        apply_SD<ST>(op, bv, dunif, U, TMP, AY, d_part.p, npw, grid, s);
+        k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, AY, U, PCEB, true, U, false, nullptr, 1.0, true, Y, d_part.p, npw);
+      }
       k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
       k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, Y, U, UP, d_part.p, npw);
       k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
@@ -1648,6 +1709,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
       for (int q = 0; q < nlp; ++q) {
         int L = lmap[q];
         if (L < 0 || hm[q] < 1) continue;
+        m_out[L] = hm[q];
         g_out[L] = cf_species_adjoint(&ha[(size_t)q * NLMAX], &hb[(size_t)q * NLMAX], hm[q], lane_z[L], tail, lane_w[L],
                                       &habar[(size_t)q * NLMAX], &hbbar[(size_t)q * NLMAX], w1.data(), w2.data(), w3.data(),
                                       w4.data(), w5.data());
@@ -1670,9 +1732,13 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
       for (int k = k0; k <= k1; ++k) {
         int q = k - k0;
         k_set_fwd<<<(nlp + 127) / 128, 128, 0, s>>>(bv, S, nlp, k);
-        apply_SD<ST>(op, bv, dunif, XS(q + 1), TMP, TS(q), d_part.p, npw, grid, s);
-        k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TS(q), XS(q + 1), PCEB, true, XS(q + 1), false, nullptr, 1.0, true, YS(q),
-                                                d_part.p, npw);
+        if (gen) {
+          apply_general_keep<ST>(op, bv, dunif, XS(q + 1), YS(q), TS(q), HS(q), RS(q), QS(q), TMP, d_part.p, npw, grid, s);
+        } else {
+          apply_SD<ST>(op, bv, dunif, XS(q + 1), TMP, TS(q), d_part.p, npw, grid, s);
+          k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TS(q), XS(q + 1), PCEB, true, XS(q + 1), false, nullptr, 1.0, true,
+                                                  YS(q), d_part.p, npw);
+        }
         ASR_CUDA(cudaMemcpyAsync(XS(q + 2), YS(q), cpy, cudaMemcpyDeviceToDevice, s));
         k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, XS(q + 2), XS(q + 1), XS(q), d_part.p, npw);
       }
@@ -1692,12 +1758,19 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_d3.p);
         k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 1);
         k_adj_y<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, WB, XS(q + 1), d_c[2].p, d_c[3].p, YB, k > 1 ? ubp : nullptr, npw);
-        // A ybar (unit scale) and t2bar = S R_d ybar
-        apply_SD<ST>(op, bva, dunif, YB, TMP, T2B, d_part.p, npw, grid, s);
-        k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, T2B, YB, PCEB, true, YB, false, nullptr, 1.0, true, AY, d_part.p, npw);
+        // A ybar (unit scale) and t2bar = S R_d ybar (the general operator: also h ybar, O h ybar, S D O h ybar)
+        if (gen) {
+          apply_general_keep<ST>(op, bva, dunif, YB, AY, T2B, HB, RB, QB, TMP, d_part.p, npw, grid, s);
+        } else {
+          apply_SD<ST>(op, bva, dunif, YB, TMP, T2B, d_part.p, npw, grid, s);
+          k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, T2B, YB, PCEB, true, YB, false, nullptr, 1.0, true, AY, d_part.p, npw);
+        }
         k_adj_u<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, AY, YS(q), WB, d_c[4].p, d_c[5].p, ubk, npw);
-        k_adj_grad<ST><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, YB, T2B, XS(q + 1), TS(q), d_sk.p, gnpb,
-                                                      d_gpart.p);
+        AdjVecs av{YB, T2B, HB, RB, QB, XS(q + 1), TS(q), HS(q), RS(q), QS(q)};
+        if (gen)
+          k_adj_grad<ST, true><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb, d_gpart.p);
+        else
+          k_adj_grad<ST, false><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb, d_gpart.p);
         k_adj_gsum<<<nt, 128, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
         ASR_CUDA(cudaMemsetAsync(ubn, 0, cpy, s));   // becomes ubar_{k-2}
         // one reverse level: 26 vector streams per (node, lane) over its kernels (dot 2, w-bar 5, y-bar 4, S application
@@ -1715,8 +1788,9 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
       if (gq < 0) continue;
       for (int e = 0; e < ngd; ++e) grad_out[(size_t)gq * ngd + e] = cadd(grad_out[(size_t)gq * ngd + e], hgacc[(size_t)bt * ngd + e]);
     }
-    const int nsd = dunif ? 1 : 2;   // launches of one S application
-    ctx->launches += 1 + (int64_t)kmax * ((4 + nsd) + (3 + nsd) + (12 + nsd));
+    const int nsd = dunif ? 1 : 2;                       // launches of one S application
+    const int nap = gen ? 2 * nsd + 3 : nsd + 1;         // launches of one operator application
+    ctx->launches += 1 + (int64_t)kmax * ((nap + 3) + (nap + 2) + (nap + 11));
   }
   ASR_TRY(check_wait_error(ctx));
   return ASR_OK;
@@ -2370,13 +2444,15 @@ static void smem_attrs() {
 
 int run_adjoint(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
                 const GroupLayout& GL, const std::vector<int>& lane_group, const std::vector<double2>& lane_z,
-                const std::vector<double2>& lane_w, int tail, int project, int stride, int precision, std::vector<double2>& g_out,
-                std::vector<double2>& grad_out) {
+                const std::vector<double2>& lane_w, double depth_tol, int tail, int project, int stride, int precision,
+                std::vector<double2>& g_out, std::vector<int>& m_out, std::vector<double2>& grad_out) {
   smem_attrs();
   if (smul_smem(op, sizeof(double)) > 96 * 1024) { set_error("adjoint: bond tables above 96 KB of shared memory"); return ASR_EINVAL; }
   if (precision == ASR_FP32)
-    return run_adjoint_t<float>(ctx, op, ginfo, gblob, GL, lane_group, lane_z, lane_w, tail, project, stride, g_out, grad_out);
-  return run_adjoint_t<double>(ctx, op, ginfo, gblob, GL, lane_group, lane_z, lane_w, tail, project, stride, g_out, grad_out);
+    return run_adjoint_t<float>(ctx, op, ginfo, gblob, GL, lane_group, lane_z, lane_w, depth_tol, tail, project, stride, g_out,
+                                m_out, grad_out);
+  return run_adjoint_t<double>(ctx, op, ginfo, gblob, GL, lane_group, lane_z, lane_w, depth_tol, tail, project, stride, g_out,
+                               m_out, grad_out);
 }
 
 int run_ed3(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,

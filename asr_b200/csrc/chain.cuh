@@ -136,11 +136,12 @@ int run_ed3(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const
             std::vector<double>& nv_out, std::vector<int>& m_out, std::vector<double2>* a_out, std::vector<double2>* b_out,
             std::vector<double2>* c_out, int64_t* nfall_out);
 
-// reverse mode: G per lane and the gradients sum_lanes w_L dG_L/dpar per group, kinds (c | e | pb), d, pa, each (9, nsp)
+// reverse mode: G per lane, the depth each lane used (the depth test stops it when depth_tol > 0) and the gradients
+// sum_lanes w_L dG_L/dpar per group, kinds c, d, pa, o, e (e and pb share one derivative), each (9, nsp)
 int run_adjoint(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
                 const GroupLayout& GL, const std::vector<int>& lane_group, const std::vector<double2>& lane_z,
-                const std::vector<double2>& lane_w, int tail, int project, int stride, int precision, std::vector<double2>& g_out,
-                std::vector<double2>& grad_out);
+                const std::vector<double2>& lane_w, double depth_tol, int tail, int project, int stride, int precision,
+                std::vector<double2>& g_out, std::vector<int>& m_out, std::vector<double2>& grad_out);
 
 // y = H x style applications of the operator's own parameters on nvec vectors (normalised coordinates)
 int apply_vectors(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,

@@ -202,6 +202,22 @@ def draw_species(nsp: int, seed: int) -> SpeciesParams:
     return SpeciesParams(c=c, d=d, delta=delta, enu=np.zeros((nsp, 3)))
 
 
+def draw_o(nsp: int, seed: int, scale: float = 0.15) -> np.ndarray:
+    """o_l of every species and l (nsp, 3), U[-scale, scale] from the seed (the o of the alpha representation that
+    edc_setup scales to o_s = o_l D_s / D_c, src/asr_edc.f90:66)."""
+    rng = np.random.default_rng(1000 + seed)
+    return rng.uniform(-scale, scale, size=(nsp, 3))
+
+
+def edc_params_o(sp: SpeciesParams, ol: np.ndarray, central: int):
+    """``edc_params`` with the o of edc_setup: o(l, s) = o_l,s D_s / D_c (src/asr_edc.f90:66), (9, nsp) Fortran."""
+    ed = edc_params(sp, central)
+    o = sp.per_orbital(ol)
+    de = ed["dl"]
+    ed["o"] = np.asfortranarray(o * de / ed["dc"][:, None])
+    return ed
+
+
 def plain_params(sp: SpeciesParams):
     """(c, d, o, e) each (9, nsp) Fortran: H = c + d S d."""
     c = sp.per_orbital(sp.c)

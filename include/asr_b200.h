@@ -233,15 +233,24 @@ int asr_ed3_blocks(asr_ctx* ctx, asr_op* op, const asr_ed3_group* groups, int ng
 
 /* Reverse mode of the batched energy-dependent chains (edc route, o = 0, fixed depth nlev per group): g(nz, ngroup) as
  * asr_chains_run, and grad(9, nsp, 3, ngroup) complex = sum_j w(j, q) dG(j, q)/dpar for the parameter arrays of group q:
- * kind 0 the diagonal c (the same derivative applies to e and pb, which enter only as c + e + pb), kind 1 d, kind 2 pa.
- * w(nz, ngroup) complex seeds.  The entries are symmetrised over the orbits of the orbitals under the operator's point
- * group (the group-reduced operator represents only parameters constant on each orbit): derivatives along every
- * group-invariant direction (per l, per orbit) are exact.  The Lanczos vectors are kept every `stride` levels
- * (0: ceil(sqrt(depth))) and recomputed
- * in between.  Tails none, hull, avg2.  No counterpart in the reference (gradients of the chain with respect to the
- * species parameters of src/asr_edc.f90:41-71). */
+ * kind 0 the diagonal c (the same derivative applies to e and pb, which enter only as c + e + pb when o = 0), kind 1 d,
+ * kind 2 pa.  w(nz, ngroup) complex seeds.  The entries are symmetrised over the orbits of the orbitals under the
+ * operator's point group (the group-reduced operator represents only parameters constant on each orbit): derivatives
+ * along every group-invariant direction (per l, per orbit) are exact.  The Lanczos vectors are kept every `stride` levels
+ * (0: ceil(sqrt(depth))) and recomputed in between.  Every tail (none, hull, bp, avg2).  Groups with o != 0 are refused
+ * (asr_chains_adjoint_ext).  No counterpart in the reference (gradients of the chain with respect to the species
+ * parameters of src/asr_edc.f90:41-71). */
 int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz,
                        const double* w, int tail, int precision, int project, int stride, double* g, double* grad);
+
+/* asr_chains_adjoint for the reference's whole operator form: H = E_nu + h - h o h + X(z) with o != 0 (edc_setup's
+ * o = o_l D_s / D_c, src/asr_edc.f90:66), chains stopped by the depth test of src/asr_edc.f90:121-127 when
+ * depth_tol > 0 (the derivative of the chain at the depth it stopped at, mused(nz, ngroup) optional), and every tail
+ * (the Beer-Pettifor fixed point differentiated implicitly).  grad(9, nsp, 5, ngroup) complex, kinds 0 c, 1 d, 2 pa,
+ * 3 o, 4 e (pb enters as e does).  No counterpart in the reference. */
+int asr_chains_adjoint_ext(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz,
+                           const double* w, double depth_tol, int tail, int precision, int project, int stride, double* g,
+                           int* mused, double* grad);
 
 /* cf_species (src/asr_chain.f90:67-167) for nchain complex chains a, b (ld, nchain), depth m(nchain), at the energies
  * z(nz, nchain): g(nz, nchain).  edges (optional, (2, nz, nchain)) returns the tail (centre, quarter width). */
