@@ -1575,7 +1575,9 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   const int nvec = 3 + 2 * nseg + (c + 2) + 2 * c + 8 + (gen ? 3 * c + 3 : 0);
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
-  int tpb = 4;
+  // tiles per batch: as the forward's default (16), halved while the batch's vectors would take more than half the free
+  // device memory (a 16-tile batch of the fcc ternary workload holds about 70 GB)
+  int tpb = 16;
   if (const char* e = getenv("ASR_TILES_PER_BATCH")) tpb = std::max(1, atoi(e));
   while (tpb > 1 && (size_t)tpb * nvec * vec_bytes > freeb / 2) tpb /= 2;
   if ((size_t)nvec * vec_bytes > freeb) { set_error("adjoint: %d vectors of %zu bytes do not fit", nvec, vec_bytes); return ASR_ENOMEM; }

@@ -71,8 +71,9 @@ def parse():
     p.add_argument("--nz-slice", type=int, default=NZ_SLICE)
     p.add_argument("--cpu-sample", type=int, default=1, help="run the bounded CPU baseline sample (1) or skip it (0)")
     p.add_argument("--e2e", type=int, default=1, help="time the host-buffer C-ABI path too (1) or skip it (0)")
-    p.add_argument("--scf", type=int, default=0,
-                   help="SCF leg: 0 none, 1 two timed iterations at full size + convergence on a small cluster, 2 converge at full size")
+    p.add_argument("--scf", type=int, default=1,
+                   help="SCF leg: 0 none, 1 two timed iterations of each scheme at full size, 2 also the convergence on a "
+                        "small cluster, 3 converged at full size")
     p.add_argument("--autotune", type=int, default=1, help="choose the batch shape by timing first (1) or use the defaults (0)")
     p.add_argument("--legs", default="1",
                    help="1: measure every leg (mixed precision with its DOS error, adjoint, KPM, plain, example, spectral, "
@@ -263,7 +264,39 @@ def kpm_leg(torch):
     # algorithmic bytes per vector and Chebyshev step: 3 FP32 streams x 36 B + 1 B species per site
     out["fp32"]["hbm_gbs_algorithmic"] = (nmom // 2) * nvec * sc.n * (3 * 36 + 1) / (out["fp32"]["ms"] / 1000.0) / 1e9
     sc.free()
+    out["asr_comparison"] = kpm_vs_asr(egrid, r64, c, d, o, e)
     return out
+
+
+def kpm_vs_asr(egrid, dos_kpm, c, d, o, e, eta=0.02):
+    """The KPM DOS of the supercell against the configuration-averaged ASR DOS of the same alloy: the site-class operator
+    of the fcc ternary (0.66 / 0.14 / 0.20, the same NN + NNN blocks and species parameters, 5^3-cell cluster, levels 3,
+    rank 1, D2h), plain real chains of depth 40 from every orbital of the start site frozen to each species, Beer-Pettifor
+    tail, DOS per state sum_s x_s sum_l -Im G / (9 pi) at E + i eta; the Jackson-kernel KPM DOS convolved with the same
+    Lorentzian of width eta.  The supercell carries short-range order (alpha_1 = -0.10), the single-site ASR configuration
+    average does not, so the difference is the physics of the two models plus both methods' truncations."""
+    import asr_b200 as A
+    from asr_b200 import synthetic as S
+    conc = [0.66, 0.14, 0.20]
+    case = S.cubic_case("fcc", 5, 3, conc, seed=4, group="d2h")
+    fl = np.ones(case["graph"].n, np.int32)
+    fl[0] = 0
+    op = A.build_augcls_operator(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, 3, maxrank=1,
+                                 flippable=fl)
+    specs = [A.ChainSpec(c=c, d=d, o=o, e=e, frozen_sp=s, start_orb=l0, nlev=40) for s in (1, 2, 3) for l0 in range(1, 10)]
+    sel = np.arange(0, egrid.shape[0], 5)
+    eg = egrid[sel]
+    g = A.chains_run(op, specs, eg + 1j * eta, mode="plain", tail="bp")["g"].reshape(eg.shape[0], 3, 9)
+    dos_asr = np.einsum("s,jsl->j", np.asarray(conc), -g.imag / np.pi) / 9.0
+    de = egrid[1] - egrid[0]
+    lor = eta / np.pi / ((eg[:, None] - egrid[None, :]) ** 2 + eta ** 2)
+    dos_k = lor @ dos_kpm * de
+    diff = np.abs(dos_k - dos_asr)
+    return {"asr_nodes": int(op.nn), "energies": int(eg.shape[0]), "eta": eta,
+            "max_abs_difference_over_max_dos": float(np.max(diff) / np.max(dos_asr)),
+            "l1_difference_over_l1_dos": float(np.sum(diff) / np.sum(dos_asr)),
+            "kpm_weight_in_window": float(np.sum(dos_k) * (eg[1] - eg[0])),
+            "asr_weight_in_window": float(np.sum(dos_asr) * (eg[1] - eg[0]))}
 
 
 def plain_leg(torch):
@@ -443,21 +476,23 @@ def scf_model(l, maxlevel, precision):
                        u=np.full(5, 0.08), stoner=np.full(5, 0.06), depths=depths, ebot=-2.0, ncont=64, precision=precision)
 
 
-def scf_leg(torch, full: bool):
-    """Time per SCF iteration at full size (5^3-cell cluster, levels 3): the reference's scheme (FP64 forward, E_F search,
-    Anderson) against the mixed one (FP32 forward, E_F search, adjoint Jacobian, quasi-Newton step); iterations to a
-    1e-6 charge residual on the same alloy (a 3^3-cell cluster at levels 2 unless full)."""
+def scf_leg(torch, mode: int):
+    """The large batched SCF configuration at full size (5^3-cell cluster, levels 3): time per SCF iteration of the
+    reference's scheme (FP64 forward, E_F search, Anderson) against the mixed one (FP32 forward, E_F search, adjoint
+    Jacobian, quasi-Newton step).  mode 1: two iterations of each; 2: also the iterations to a 1e-6 charge residual on a
+    3^3-cell cluster at levels 2; 3: converged at full size."""
     from asr_b200 import scf as SC
     out = {}
     for prec, mixer in (("fp64", "anderson"), ("fp32", "broyden")):
         m = scf_model(5, 3, prec)
         q0 = np.vstack([m.z / 2 + 0.3, m.z / 2 - 0.3])
         torch.cuda.synchronize()
-        r = SC.scf_run(m, q0, 0.0, mixer=mixer, tol=1e-6, maxit=40 if full else 2)
+        r = SC.scf_run(m, q0, 0.0, mixer=mixer, tol=1e-6, maxit=40 if mode == 3 else 2)
         out[f"{prec}_{mixer}"] = {"seconds_per_iteration": r["seconds"] / r["iterations"], "iterations_run": r["iterations"],
                                  "converged": r["converged"], "forward_runs": r["stats"]["forward"],
-                                 "adjoint_runs": r["stats"]["adjoint"], "nodes": int(m.op.nn)}
-    if not full:
+                                 "adjoint_runs": r["stats"]["adjoint"], "nodes": int(m.op.nn),
+                                 "residuals": [h["residual"] for h in r["history"]]}
+    if mode == 2:
         for prec, mixer in (("fp64", "anderson"), ("fp32", "broyden")):
             m = scf_model(3, 2, prec)
             q0 = np.vstack([m.z / 2 + 0.3, m.z / 2 - 0.3])
@@ -467,7 +502,43 @@ def scf_leg(torch, full: bool):
     return out
 
 
-LEGS = ("mixed", "adjoint", "kpm", "plain", "example", "spectral", "epi")
+def heusler_leg(torch):
+    """The adjoint configuration itself: L2_1 four-sublattice bcc cell (one sublattice Cr0.6Fe0.4-like), depth 20, 32-point
+    contour, edc_setup's o (o_l D_s / D_c), the Jacobian of the band energy and the four sublattice charges with respect to
+    the 45 species parameters through torch.autograd and the device adjoint: time of the forward and of the Jacobian."""
+    from asr_b200 import classes as CL
+    from asr_b200 import contour as CT
+    from asr_b200 import synthetic as S
+    cases = [S.heusler_case(4, 3, k) for k in (1, 2, 3, 4)]
+    sc = CL.SublatticeChains(cases, 20)
+    sp = S.draw_species(5, 3)
+    ol = torch.tensor(S.draw_o(5, 3), dtype=torch.float64)
+    enu = torch.zeros(5, 3, dtype=torch.float64)
+    z, w = CT.contour_nodes(-1.2, 0.2, 32)
+    params = [torch.tensor(x, dtype=torch.float64, requires_grad=True) for x in (sp.c, sp.d, sp.delta)]
+    sc.energy_and_charges(*params, enu, z, w, ol)   # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.no_grad():
+        sc.energy_and_charges(*params, enu, z, w, ol)
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    e_band, q = sc.energy_and_charges(*params, enu, z, w, ol)
+    jac = []
+    for o in [e_band] + [q[k] for k in range(4)]:
+        gr = torch.autograd.grad(o, params, retain_graph=True)
+        jac.append(np.concatenate([g.numpy().ravel() for g in gr]))
+    torch.cuda.synchronize()
+    t_jac = time.perf_counter() - t0
+    nodes = [int(op.nn) for op in sc.ops]
+    chains = sum(len(sc.groups(k)[0]) for k in range(4)) * len(z)
+    return {"nodes": nodes, "chains": chains, "depth": 20, "energies": len(z), "parameters": 45, "outputs": 5,
+            "forward_s": t_fwd, "jacobian_s": t_jac, "jacobian_over_forward": t_jac / t_fwd,
+            "forward_chain_steps_per_s": chains * 20 / t_fwd, "jacobian_norm": float(np.linalg.norm(np.array(jac)))}
+
+
+LEGS = ("mixed", "adjoint", "heusler", "kpm", "plain", "example", "spectral", "epi")
 
 
 def contour_weights(z_all):
@@ -573,8 +644,10 @@ def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
         out["spectral"] = spectral_leg(torch)
     if "epi" in want:
         out["epi"] = epi_leg(torch)
-    if args.scf:
-        out["scf"] = scf_leg(torch, args.scf == 2)
+    if "heusler" in want:
+        out["heusler"] = heusler_leg(torch)
+    if args.scf and (args.legs == "1" or "scf" in want):
+        out["scf"] = scf_leg(torch, args.scf)
     return out
 
 

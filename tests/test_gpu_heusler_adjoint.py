@@ -1,7 +1,8 @@
 """Adjoint on the L2_1 four-sublattice bcc alloy (one sublattice Cr0.6Fe0.4-like, the others ordered): the Jacobian of
 the band energy and the four sublattice charges with respect to all 45 species parameters (c_l, d_l, Delta_l for
-l = s, p, d and 5 species), through torch.autograd and the device adjoint, against central finite differences
-(h = 1e-5, Richardson-extrapolated) of the CUDA forward and of the oracle's chain_greens."""
+l = s, p, d and 5 species), through torch.autograd and the device adjoint: with o = 0 against central differences
+(h = 1e-5, Richardson-extrapolated) of the CUDA forward, and with edc_setup's o against the oracle's central differences
+(all 45 x 5 entries, the committed fixture of tests/golden/make_c3_jacobian.py)."""
 import numpy as np
 import pytest
 import torch
@@ -67,45 +68,35 @@ def test_jacobian_of_band_energy_and_charges(system):
     assert worst < 1e-6, (worst, where)
 
 
-def test_charge_gradient_against_oracle_differences(system):
-    """Three parameters of the disordered sublattice's species through the oracle's chain_greens (CPU restatement)."""
-    from oracle.oracle import OracleOp
-    cases, sc, sp, z, w = system
+def test_jacobian_with_o_against_oracle_central_differences():
+    """All 45 parameters x 5 outputs with edc_setup's o (o_l D_s / D_c) against the oracle's central differences with
+    h = 1e-5 (tests/golden/c3_oracle_jacobian.json, made by tests/golden/make_c3_jacobian.py).  Tolerance per entry:
+    1e-6 of the entry itself plus the rounding floor of a central difference, 4 eps |f_r| / h for output r (2.2e-10 for
+    the band energy, 2.0e-10 for a charge); the floor is at most 1e-6 of every entry whose magnitude is above 2.2e-4.
+    The Richardson column (h and h / 2) agrees with the h column within the same floor."""
+    import json
+    import os
+
+    from tests import heusler_oracle as HO
+    fx = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c3_oracle_jacobian.json")))
+    fd = np.array(fx["central_h"])
+    rich = np.array(fx["richardson"])
+    vals = np.array(fx["values"])
+    floor = 4 * np.finfo(float).eps * np.abs(vals) / fx["h"]
+    assert np.all(np.abs(rich - fd) <= 1e-6 * np.abs(fd) + floor[:, None])
+    cases, sp, ol, z, w = HO.configuration()
+    sc = CL.SublatticeChains(cases, HO.NLEV)
     enu = torch.zeros(5, 3, dtype=torch.float64)
     params = _params(sp)
-    _, q = sc.energy_and_charges(*params, enu, z, w)
-    gr = torch.autograd.grad(q[3], params)
-    case = cases[3]
-    oop = OracleOp(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, case["maxlevel"], case["maxrank"],
-                   case["flippable"])
-    groups, wts = sc.groups(3)
-    conc = dict(sc.comps[3])
-    orbs = sorted({orb for _, orb, _ in groups})
-    comps = [spc for spc, _ in sc.comps[3]]
-
-    def q4(c, d, delta):
-        spp = S.SpeciesParams(c=c, d=d, delta=delta, enu=np.zeros((5, 3)))
-        eds = [S.edc_params(spp, spc) for spc in comps]
-        gz, _ = oop.chain_greens(eds, comps, orbs, np.full((len(comps), len(orbs)), NLEV), z, 4)
-        tot = 0.0
-        for (spc, orb, nlev), wt in zip(groups, wts):
-            g = gz[:, orbs.index(orb), comps.index(spc)]
-            tot += conc[spc] * wt * (-np.imag(np.sum(w * g)) / np.pi)
-        return tot
-
-    gmax = max(g.abs().max().item() for g in gr)
-    for a, s, l in ((0, 3, 2), (1, 4, 1), (2, 3, 0)):   # c_d of species 4, d_p of species 5, Delta_s of species 4
-        vals = [sp.c.copy(), sp.d.copy(), sp.delta.copy()]
-        vp = [v.copy() for v in vals]
-        vm = [v.copy() for v in vals]
-        vp[a][s, l] += H
-        vm[a][s, l] -= H
-        vp2 = [v.copy() for v in vals]
-        vm2 = [v.copy() for v in vals]
-        vp2[a][s, l] += H / 2
-        vm2[a][s, l] -= H / 2
-        d1 = (q4(*vp) - q4(*vm)) / (2 * H)
-        d2 = (q4(*vp2) - q4(*vm2)) / H
-        fd = (4 * d2 - d1) / 3   # Richardson-extrapolated central difference
-        adj = gr[a][s, l].item()
-        assert abs(adj - fd) <= 1e-6 * max(abs(fd), 1e-2 * gmax), (a, s, l, adj, fd)
+    olt = torch.tensor(ol, dtype=torch.float64)
+    e_band, q = sc.energy_and_charges(*params, enu, z, w, olt)
+    assert abs(e_band.item() - vals[0]) <= 1e-9 * abs(vals[0])
+    assert np.max(np.abs(q.detach().numpy() - vals[1:])) <= 1e-9 * np.max(np.abs(vals[1:]))
+    outs = [e_band] + [q[k] for k in range(4)]
+    jac = np.zeros((5, 45))
+    for r, o in enumerate(outs):
+        gr = torch.autograd.grad(o, params, retain_graph=True)
+        jac[r] = np.concatenate([g.numpy().ravel() for g in gr])
+    err = np.abs(jac - fd) - (1e-6 * np.abs(fd) + floor[:, None])
+    r, k = np.unravel_index(np.argmax(err), err.shape)
+    assert np.all(err <= 0), (r, k, jac[r, k], fd[r, k])
