@@ -163,5 +163,145 @@ module asr_b200
     integer(c_int) function asr_last_error(buf, n) bind(c)
       import; character(kind=c_char) :: buf(*); integer(c_size_t), value :: n
     end function
+    integer(c_int) function asr_version() bind(c)
+      import
+    end function
+    integer(c_int) function asr_ctx_sync(ctx) bind(c)
+      import; type(c_ptr), value :: ctx
+    end function
+    integer(c_int) function asr_ctx_stats(ctx, nchain, nlev, nfall) bind(c)
+      import; type(c_ptr), value :: ctx; integer(c_int64_t) :: nchain, nlev, nfall
+    end function
+    integer(c_int) function asr_ctx_set_stream(ctx, stream) bind(c)
+      import; type(c_ptr), value :: ctx, stream
+    end function
+    integer(c_int) function asr_ctx_profile(ctx, on) bind(c)
+      import; type(c_ptr), value :: ctx; integer(c_int), value :: on
+    end function
+    integer(c_int) function asr_ctx_kernel_stats(ctx, ms, launches, bytes, flops) bind(c)
+      import; type(c_ptr), value :: ctx; real(c_double) :: ms, bytes, flops; integer(c_int64_t) :: launches
+    end function
+    integer(c_int) function asr_ctx_launches(ctx, launches) bind(c)
+      import; type(c_ptr), value :: ctx; integer(c_int64_t) :: launches
+    end function
+    integer(c_int) function asr_op_dims(op, dims) bind(c)
+      import; type(c_ptr), value :: op; integer(c_int) :: dims(*)
+    end function
+    integer(c_int) function asr_op_export_tables(op, flipr, flipg, hopr, hopg, lst, site, ncl, level, norb, sq, stab_ptr, &
+                                                 stab) bind(c)
+      import; type(c_ptr), value :: op
+      integer(c_int) :: flipr(*), flipg(*), hopr(*), hopg(*), lst(*), site(*), ncl(*), level(*), stab_ptr(*), stab(*)
+      real(c_double) :: norb(*), sq(*)
+    end function
+    integer(c_int) function asr_op_rand_c(op, par, x, w, nvec) bind(c)
+      import; type(c_ptr), value :: op; complex(c_double_complex) :: par(*), x(*), w(*); integer(c_int), value :: nvec
+    end function
+    integer(c_int) function asr_op_project_c(op, x, nvec) bind(c)
+      import; type(c_ptr), value :: op; complex(c_double_complex) :: x(*); integer(c_int), value :: nvec
+    end function
+    integer(c_int) function asr_chains_run_dev(ctx, op, groups, ngroup, z_dev, nz, mode, depth_tol, tail, precision, project, &
+                                               g_dev, a, b, mused) bind(c)
+      import
+      type(c_ptr), value :: ctx, op, z_dev, g_dev
+      type(asr_chain_group) :: groups(*)
+      integer(c_int), value :: ngroup, nz, mode, tail, precision, project
+      real(c_double), value :: depth_tol
+      complex(c_double_complex) :: a(*), b(*)
+      integer(c_int) :: mused(*)
+    end function
+    integer(c_int) function asr_autotune(ctx, op, groups, ngroup, z, nz, precision, levels, tpb, npw, times) bind(c)
+      import
+      type(c_ptr), value :: ctx, op
+      type(asr_chain_group) :: groups(*)
+      integer(c_int), value :: ngroup, nz, precision, levels
+      complex(c_double_complex) :: z(*)
+      integer(c_int) :: tpb, npw
+      real(c_double) :: times(*)
+    end function
+    integer(c_int) function asr_op_tuning(op, precision, tpb, npw, link, ms) bind(c)
+      import; type(c_ptr), value :: op; integer(c_int), value :: precision; integer(c_int) :: tpb, npw, link
+      real(c_double) :: ms(*)
+    end function
+    integer(c_int) function asr_op_set_tuning(op, precision, tpb, npw, link) bind(c)
+      import; type(c_ptr), value :: op; integer(c_int), value :: precision, tpb, npw, link
+    end function
+    integer(c_int) function asr_chains_adjoint(ctx, op, groups, ngroup, z, nz, w, tail, precision, project, stride, g, grad) &
+                                               bind(c)
+      import
+      type(c_ptr), value :: ctx, op
+      type(asr_chain_group) :: groups(*)
+      integer(c_int), value :: ngroup, nz, tail, precision, project, stride
+      complex(c_double_complex) :: z(*), w(*), g(*), grad(*)
+    end function
+    integer(c_int) function asr_chains_adjoint_ext(ctx, op, groups, ngroup, z, nz, w, depth_tol, tail, precision, project, &
+                                                   stride, g, mused, grad) bind(c)
+      import
+      type(c_ptr), value :: ctx, op
+      type(asr_chain_group) :: groups(*)
+      integer(c_int), value :: ngroup, nz, tail, precision, project, stride
+      real(c_double), value :: depth_tol
+      complex(c_double_complex) :: z(*), w(*), g(*), grad(*)
+      integer(c_int) :: mused(*)
+    end function
+    integer(c_int) function asr_cf_eval_noalloc(ctx, a, b, m, ld, nchain, z, nz, tail, g, nfall) bind(c)
+      import
+      type(c_ptr), value :: ctx
+      complex(c_double_complex) :: a(*), b(*), z(*), g(*)
+      integer(c_int) :: m(*)
+      integer(c_int), value :: ld, nchain, nz, tail
+      integer(c_int64_t) :: nfall
+    end function
+    integer(c_int) function asr_cf_adjoint(a, b, m, zr, zi, tail, wr, wi, abar, bbar, g) bind(c)
+      import
+      complex(c_double_complex) :: a(*), b(*), abar(*), bbar(*), g
+      integer(c_int), value :: m, tail
+      real(c_double), value :: zr, zi, wr, wi
+    end function
+    integer(c_int) function asr_supercell_build(ctx, nsite, nslot, nbr, spc, nsp, c, d, o, e, block, block0, sc) bind(c)
+      import
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: nsite, nslot, nsp
+      integer(c_int) :: nbr(*), spc(*)
+      real(c_double) :: c(*), d(*), o(*), e(*), block(*), block0(*)
+      type(c_ptr) :: sc
+    end function
+    integer(c_int) function asr_supercell_free(sc) bind(c)
+      import; type(c_ptr), value :: sc
+    end function
+    integer(c_int) function asr_supercell_apply(sc, x, y, nvec) bind(c)
+      import; type(c_ptr), value :: sc; real(c_double) :: x(*), y(*); integer(c_int), value :: nvec
+    end function
+    integer(c_int) function asr_kpm_moments(ctx, sc, cen, scl, nmom, v0, nvec, seed, precision, doubling, mu) bind(c)
+      import
+      type(c_ptr), value :: ctx, sc
+      real(c_double), value :: cen, scl
+      integer(c_int), value :: nmom, v0, nvec, precision, doubling
+      integer(c_int64_t), value :: seed
+      real(c_double) :: mu(*)
+    end function
+    integer(c_int) function asr_kpm_dos(mu, nmom, cen, scl, e, ne, rho) bind(c)
+      import
+      real(c_double) :: mu(*), e(*), rho(*)
+      integer(c_int), value :: nmom, ne
+      real(c_double), value :: cen, scl
+    end function
+    integer(c_int) function asr_sro_layout(nsite, z, nbr, ldnbr, nsp, conc, alpha, seed, sweeps, spc, alpha_out) bind(c)
+      import
+      integer(c_int), value :: nsite, z, ldnbr, nsp, sweeps
+      integer(c_int) :: nbr(*), spc(*)
+      real(c_double) :: conc(*), alpha(*), alpha_out(*)
+      integer(c_int64_t), value :: seed
+    end function
+    integer(c_int) function asr_gauss_legendre(n, x, w) bind(c)
+      import; integer(c_int), value :: n; real(c_double) :: x(*), w(*)
+    end function
+    integer(c_int) function asr_contour_nodes_closed(ebot, ef, eta, n_arc, n_vert, z, w) bind(c)
+      import; real(c_double), value :: ebot, ef, eta; integer(c_int), value :: n_arc, n_vert
+      complex(c_double_complex) :: z(*), w(*)
+    end function
+    integer(c_int) function asr_contour_nodes_fermi(ebot, mu, kt, npole, n_main, n_step, z, w) bind(c)
+      import; real(c_double), value :: ebot, mu, kt; integer(c_int), value :: npole, n_main, n_step
+      complex(c_double_complex) :: z(*), w(*)
+    end function
   end interface
 end module asr_b200
