@@ -232,6 +232,42 @@ template <> struct Pair<double> { typedef double2 T; };
 template <> struct Pair<float> { typedef float2 T; };
 
 constexpr int RW = 12;   // padded row of a shared-memory block (16-byte aligned pairs for FP64 and FP32)
+
+// acc += row . v for one output orbital: the nine products in the order lp = 0 .. 8 into acc.x and acc.y.  FP64 reads the
+// row as four 16-byte pairs and one double; FP32 as two 16-byte quads and one float (fewer shared-memory instructions
+// for the issue-bound FP32 step, the same products in the same order).
+template <typename ST, typename T2>
+__device__ __forceinline__ void row_fma(const ST* __restrict__ row, const T2* v, T2& acc);
+template <>
+__device__ __forceinline__ void row_fma<double, double2>(const double* __restrict__ row, const double2* v, double2& acc) {
+#pragma unroll
+  for (int lp = 0; lp < 8; lp += 2) {
+    double2 bb = *(const double2*)(row + lp);
+    acc.x = fma(bb.x, v[lp].x, acc.x);
+    acc.y = fma(bb.x, v[lp].y, acc.y);
+    acc.x = fma(bb.y, v[lp + 1].x, acc.x);
+    acc.y = fma(bb.y, v[lp + 1].y, acc.y);
+  }
+  acc.x = fma(row[8], v[8].x, acc.x);
+  acc.y = fma(row[8], v[8].y, acc.y);
+}
+template <>
+__device__ __forceinline__ void row_fma<float, float2>(const float* __restrict__ row, const float2* v, float2& acc) {
+#pragma unroll
+  for (int lp = 0; lp < 8; lp += 4) {
+    float4 bb = *(const float4*)(row + lp);
+    acc.x = fmaf(bb.x, v[lp].x, acc.x);
+    acc.y = fmaf(bb.x, v[lp].y, acc.y);
+    acc.x = fmaf(bb.y, v[lp + 1].x, acc.x);
+    acc.y = fmaf(bb.y, v[lp + 1].y, acc.y);
+    acc.x = fmaf(bb.z, v[lp + 2].x, acc.x);
+    acc.y = fmaf(bb.z, v[lp + 2].y, acc.y);
+    acc.x = fmaf(bb.w, v[lp + 3].x, acc.x);
+    acc.y = fmaf(bb.w, v[lp + 3].y, acc.y);
+  }
+  acc.x = fmaf(row[8], v[8].x, acc.x);
+  acc.y = fmaf(row[8], v[8].y, acc.y);
+}
 // packed orbital operation of the identity: permutation pi(l) = l in bits 4l..4l+3, no signs (bits 40..48)
 constexpr unsigned long long PW_IDENTITY = 0x876543210ull;
 constexpr unsigned long long PW_PERM_MASK = 0xFFFFFFFFFull;   // the nine 4-bit orbital indices
@@ -340,18 +376,8 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
       const T2* src = in + vix(it.tile, bv.nn, i, 0) + lane;
       T2 v[9];
       for (int l2 = 0; l2 < 9; ++l2) v[l2] = src[l2 * TL];
-      for (int l = 0; l < 9; ++l) {
-        const ST* row = B + l * RW;
-        for (int lp = 0; lp < 8; lp += 2) {
-          P2 bb = *(const P2*)(row + lp);
-          acc[l].x = fma_(bb.x, v[lp].x, acc[l].x);
-          acc[l].y = fma_(bb.x, v[lp].y, acc[l].y);
-          acc[l].x = fma_(bb.y, v[lp + 1].x, acc[l].x);
-          acc[l].y = fma_(bb.y, v[lp + 1].y, acc[l].y);
-        }
-        acc[l].x = fma_(row[8], v[8].x, acc[l].x);
-        acc[l].y = fma_(row[8], v[8].y, acc[l].y);
-      }
+#pragma unroll
+      for (int l = 0; l < 9; ++l) row_fma<ST, T2>(B + l * RW, v, acc[l]);
     }
     // the node's links, one slot per lane, read once with a coalesced load and broadcast by shuffles: the row gathers
     // then wait on one global latency per slot instead of two dependent ones (link, then row)
@@ -383,18 +409,8 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
         }
       }
       const ST* Bk = B + (size_t)(k + 1) * 9 * RW;
-      for (int l = 0; l < 9; ++l) {
-        const ST* row = Bk + l * RW;
-        for (int lp = 0; lp < 8; lp += 2) {
-          P2 bb = *(const P2*)(row + lp);
-          acc[l].x = fma_(bb.x, v[lp].x, acc[l].x);
-          acc[l].y = fma_(bb.x, v[lp].y, acc[l].y);
-          acc[l].x = fma_(bb.y, v[lp + 1].x, acc[l].x);
-          acc[l].y = fma_(bb.y, v[lp + 1].y, acc[l].y);
-        }
-        acc[l].x = fma_(row[8], v[8].x, acc[l].x);
-        acc[l].y = fma_(row[8], v[8].y, acc[l].y);
-      }
+#pragma unroll
+      for (int l = 0; l < 9; ++l) row_fma<ST, T2>(Bk + l * RW, v, acc[l]);
     }
     smul_node_out<ST, FINAL>(op, bv, it.tile, i, lane, L, grp, gflags, gfrozen, piw, in, out, acc, dot);
   }
