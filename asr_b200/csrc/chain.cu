@@ -233,48 +233,13 @@ template <> struct Pair<float> { typedef float2 T; };
 
 constexpr int RW = 12;   // padded row of a shared-memory block (16-byte aligned pairs for FP64 and FP32)
 
-// acc += row . v for one output orbital: the nine products in the order lp = 0 .. 8 into acc.x and acc.y.  FP64 reads the
-// row as four 16-byte pairs and one double; FP32 as two 16-byte quads and one float (fewer shared-memory instructions
-// for the issue-bound FP32 step, the same products in the same order).
-template <typename ST, typename T2>
-__device__ __forceinline__ void row_fma(const ST* __restrict__ row, const T2* v, T2& acc);
-template <>
-__device__ __forceinline__ void row_fma<double, double2>(const double* __restrict__ row, const double2* v, double2& acc) {
-#pragma unroll
-  for (int lp = 0; lp < 8; lp += 2) {
-    double2 bb = *(const double2*)(row + lp);
-    acc.x = fma(bb.x, v[lp].x, acc.x);
-    acc.y = fma(bb.x, v[lp].y, acc.y);
-    acc.x = fma(bb.y, v[lp + 1].x, acc.x);
-    acc.y = fma(bb.y, v[lp + 1].y, acc.y);
-  }
-  acc.x = fma(row[8], v[8].x, acc.x);
-  acc.y = fma(row[8], v[8].y, acc.y);
-}
-template <>
-__device__ __forceinline__ void row_fma<float, float2>(const float* __restrict__ row, const float2* v, float2& acc) {
-#pragma unroll
-  for (int lp = 0; lp < 8; lp += 4) {
-    float4 bb = *(const float4*)(row + lp);
-    acc.x = fmaf(bb.x, v[lp].x, acc.x);
-    acc.y = fmaf(bb.x, v[lp].y, acc.y);
-    acc.x = fmaf(bb.y, v[lp + 1].x, acc.x);
-    acc.y = fmaf(bb.y, v[lp + 1].y, acc.y);
-    acc.x = fmaf(bb.z, v[lp + 2].x, acc.x);
-    acc.y = fmaf(bb.z, v[lp + 2].y, acc.y);
-    acc.x = fmaf(bb.w, v[lp + 3].x, acc.x);
-    acc.y = fmaf(bb.w, v[lp + 3].y, acc.y);
-  }
-  acc.x = fmaf(row[8], v[8].x, acc.x);
-  acc.y = fmaf(row[8], v[8].y, acc.y);
-}
 // packed orbital operation of the identity: permutation pi(l) = l in bits 4l..4l+3, no signs (bits 40..48)
 constexpr unsigned long long PW_IDENTITY = 0x876543210ull;
 constexpr unsigned long long PW_PERM_MASK = 0xFFFFFFFFFull;   // the nine 4-bit orbital indices
 
 // the output of one node of the S application: t2 (unscaled), or with FINAL y = s (d t2 + (c + e + X(z)) U) and the
 // node's share of the dot sum norb (s U) . y
-template <typename ST, bool FINAL, typename T2, typename A2>
+template <typename ST, bool FINAL, bool T2OUT = false, typename T2, typename A2>
 __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView& bv, int tile, int i, int lane, int L, int grp,
                                               int gflags, int gfrozen, const unsigned long long* piw, const T2* __restrict__ in,
                                               T2* __restrict__ out, const A2* acc, double2& dot) {
@@ -310,6 +275,10 @@ __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView&
       }
       double2 y = cmul(s, cadd(make_double2(acc[l].x, acc[l].y), pt));
       stv_cs(out + vix(tile, bv.nn, i, l) + lane, y);
+      if (T2OUT) {   // the blocks carry d on both sides: t2 = S (d o U) = acc / d_l
+        const double il = 1.0 / bv.ginfo[grp >= 0 ? grp : 0].dd[l];
+        stv((T2*)bv.t2out + vix(tile, bv.nn, i, l) + lane, make_double2(acc[l].x * il, acc[l].y * il));
+      }
       dot = cadd(dot, cscale(cmul(cmul(s, ui), y), norb));
     }
   }
@@ -323,7 +292,7 @@ __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView&
 // LINK_ID: links whose orbital operation keeps the orbital order (the identity, and the pure sign changes of diagonal
 // groups such as D2h) gather their nine rows at fixed offsets, without the per-orbital index and sign decoding; the
 // products and their order are those of the general path, so both instantiations give the same bits.
-template <typename ST, bool FUSE_D, bool FINAL, bool LINK_ID>
+template <typename ST, bool FUSE_D, bool FINAL, bool LINK_ID, bool T2OUT = false>
 __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, const ST* __restrict__ blocks,
                                                    const typename St2<ST>::T* __restrict__ in,
                                                    typename St2<ST>::T* __restrict__ out, double2* part, int npw) {
@@ -376,8 +345,18 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
       const T2* src = in + vix(it.tile, bv.nn, i, 0) + lane;
       T2 v[9];
       for (int l2 = 0; l2 < 9; ++l2) v[l2] = src[l2 * TL];
-#pragma unroll
-      for (int l = 0; l < 9; ++l) row_fma<ST, T2>(B + l * RW, v, acc[l]);
+      for (int l = 0; l < 9; ++l) {
+        const ST* row = B + l * RW;
+        for (int lp = 0; lp < 8; lp += 2) {
+          P2 bb = *(const P2*)(row + lp);
+          acc[l].x = fma_(bb.x, v[lp].x, acc[l].x);
+          acc[l].y = fma_(bb.x, v[lp].y, acc[l].y);
+          acc[l].x = fma_(bb.y, v[lp + 1].x, acc[l].x);
+          acc[l].y = fma_(bb.y, v[lp + 1].y, acc[l].y);
+        }
+        acc[l].x = fma_(row[8], v[8].x, acc[l].x);
+        acc[l].y = fma_(row[8], v[8].y, acc[l].y);
+      }
     }
     // the node's links, one slot per lane, read once with a coalesced load and broadcast by shuffles: the row gathers
     // then wait on one global latency per slot instead of two dependent ones (link, then row)
@@ -409,10 +388,20 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
         }
       }
       const ST* Bk = B + (size_t)(k + 1) * 9 * RW;
-#pragma unroll
-      for (int l = 0; l < 9; ++l) row_fma<ST, T2>(Bk + l * RW, v, acc[l]);
+      for (int l = 0; l < 9; ++l) {
+        const ST* row = Bk + l * RW;
+        for (int lp = 0; lp < 8; lp += 2) {
+          P2 bb = *(const P2*)(row + lp);
+          acc[l].x = fma_(bb.x, v[lp].x, acc[l].x);
+          acc[l].y = fma_(bb.x, v[lp].y, acc[l].y);
+          acc[l].x = fma_(bb.y, v[lp + 1].x, acc[l].x);
+          acc[l].y = fma_(bb.y, v[lp + 1].y, acc[l].y);
+        }
+        acc[l].x = fma_(row[8], v[8].x, acc[l].x);
+        acc[l].y = fma_(row[8], v[8].y, acc[l].y);
+      }
     }
-    smul_node_out<ST, FINAL>(op, bv, it.tile, i, lane, L, grp, gflags, gfrozen, piw, in, out, acc, dot);
+    smul_node_out<ST, FINAL, T2OUT>(op, bv, it.tile, i, lane, L, grp, gflags, gfrozen, piw, in, out, acc, dot);
   }
   if (FINAL) {
     block_reduce_store(dot, part, it.tile, bpt);
@@ -925,11 +914,18 @@ bool smul_bulk_enabled() {
   return on == 1;
 }
 
-template <typename ST, bool FUSE_D, bool FINAL>
+template <typename ST, bool FUSE_D, bool FINAL, bool T2OUT = false>
 void launch_smul(asr_op* op, const BatchView& bv, const ST* blk, const typename St2<ST>::T* in, typename St2<ST>::T* out,
                  double2* part, int npw, int grid, cudaStream_t s) {
   OpView ov = op->view();
   const int pix = std::is_same<ST, double>::value ? 0 : 1;
+  if (T2OUT) {   // the adjoint's fused step that also stores t2 (bv.t2out)
+    if (op->tuned_link[pix] == 1)
+      k_smul<ST, FUSE_D, FINAL, true, T2OUT><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
+    else
+      k_smul<ST, FUSE_D, FINAL, false, T2OUT><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
+    return;
+  }
   if (smul_bulk_enabled())
     k_smul_bulk<ST, FUSE_D, FINAL><<<grid, WPB * TL, smul_bulk_smem<ST>(op), s>>>(ov, bv, blk, in, out, part, npw, op->ctx->d_err);
   else if (op->tuned_link[pix] == 1)
@@ -1655,6 +1651,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   std::vector<double2> hz(nlp), ha((size_t)nlp * NLMAX), hb((size_t)nlp * NLMAX), habar((size_t)nlp * NLMAX), hbbar((size_t)nlp * NLMAX);
   std::vector<double2> hgacc((size_t)tpb * ngd);
   OpView ov = op->view();
+  const ST* blk = std::is_same<ST, double>::value ? (const ST*)op->d_blocks : (const ST*)op->d_blocks_f;
   for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
     const int nt = std::min(tpb, ntile_all - t0);
     std::vector<int> tact(tpb, 0), act(nlp, 0), tgroup(tpb, -1);
@@ -1700,6 +1697,8 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
       T2* Y = FW[(k + 1) % 3];
       if (gen) {
         apply_general_keep<ST>(op, bv, dunif, U, Y, AY, WB, YB, T2B, TMP, d_part.p, npw, grid, s);
+      } else if (dunif) {   // the fused step of the forward chains (d folded into the blocks)
+        launch_smul<ST, true, true>(op, bv, blk, U, Y, d_part.p, npw, grid, s);
       } else {
         apply_SD<ST>(op, bv, dunif, U, TMP, AY, d_part.p, npw, grid, s);
         k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, AY, U, PCEB, true, U, false, nullptr, 1.0, true, Y, d_part.p, npw);
@@ -1752,6 +1751,10 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         k_set_fwd<<<(nlp + 127) / 128, 128, 0, s>>>(bv, S, nlp, k);
         if (gen) {
           apply_general_keep<ST>(op, bv, dunif, XS(q + 1), YS(q), TS(q), HS(q), RS(q), QS(q), TMP, d_part.p, npw, grid, s);
+        } else if (dunif) {   // the forward's fused step, bit for bit, with t2 = S d X stored for the gradient
+          BatchView bvt = bv;
+          bvt.t2out = TS(q);
+          launch_smul<ST, true, true, true>(op, bvt, blk, XS(q + 1), YS(q), d_part.p, npw, grid, s);
         } else {
           apply_SD<ST>(op, bv, dunif, XS(q + 1), TMP, TS(q), d_part.p, npw, grid, s);
           k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TS(q), XS(q + 1), PCEB, true, XS(q + 1), false, nullptr, 1.0, true,
@@ -1779,6 +1782,10 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         // A ybar (unit scale) and t2bar = S R_d ybar (the general operator: also h ybar, O h ybar, S D O h ybar)
         if (gen) {
           apply_general_keep<ST>(op, bva, dunif, YB, AY, T2B, HB, RB, QB, TMP, d_part.p, npw, grid, s);
+        } else if (dunif) {
+          BatchView bvt = bva;
+          bvt.t2out = T2B;
+          launch_smul<ST, true, true, true>(op, bvt, blk, YB, AY, d_part.p, npw, grid, s);
         } else {
           apply_SD<ST>(op, bva, dunif, YB, TMP, T2B, d_part.p, npw, grid, s);
           k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, T2B, YB, PCEB, true, YB, false, nullptr, 1.0, true, AY, d_part.p, npw);
@@ -2451,6 +2458,10 @@ static void smem_attrs() {
   cudaFuncSetAttribute(k_smul<float, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   cudaFuncSetAttribute(k_smul<float, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   cudaFuncSetAttribute(k_smul<float, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, true, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, true, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   cudaFuncSetAttribute(k_smul_bulk<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_smul_bulk<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_smul_bulk<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);

@@ -55,6 +55,8 @@ struct BatchView {
   int* lane_closed;        // optional: 1 where |b| < 1e-12 ended the chain
   int* tick;               // optional (ntile): per-tile tickets; set, the step and Lanczos kernels reduce a and b in the
                            // epilogue of the tile's last block instead of separate reduction launches
+  void* t2out;             // optional: the fused step kernel also stores t2 = S (d o U) (unscaled, the vector type of the
+                           // batch) for the adjoint's parameter gradient
 };
 
 struct RunOptions {
