@@ -69,11 +69,15 @@ def test_jacobian_of_band_energy_and_charges(system):
 
 
 def test_jacobian_with_o_against_oracle_central_differences():
-    """All 45 parameters x 5 outputs with edc_setup's o (o_l D_s / D_c) against the oracle's central differences with
-    h = 1e-5 (tests/golden/c3_oracle_jacobian.json, made by tests/golden/make_c3_jacobian.py).  Tolerance per entry:
-    1e-6 of the entry itself plus the rounding floor of a central difference, 4 eps |f_r| / h for output r (2.2e-10 for
-    the band energy, 2.0e-10 for a charge); the floor is at most 1e-6 of every entry whose magnitude is above 2.2e-4.
-    The Richardson column (h and h / 2) agrees with the h column within the same floor."""
+    """All 45 parameters x 5 outputs with edc_setup's o (o_l D_s / D_c) against the oracle's central differences
+    (tests/golden/c3_oracle_jacobian.json, made by tests/golden/make_c3_jacobian.py), h = 1e-5 and h / 2.
+
+    The plain central difference at h = 1e-5 carries a truncation error of up to 4.3e-6 of the entry (its distance from
+    the Richardson combination of h and h / 2), so the 1e-6 comparison is made against the Richardson column:
+    |J - R| <= 1e-6 |R| + F_r, where F_r = 8 eps |f_r| / h (1.4e-9 to 1.6e-9 per output) bounds the rounding of R; F_r is
+    at most 1e-6 of every entry above 1.6e-3 in magnitude, and the entries below it (the charges of the two ordered
+    sublattices whose derivatives vanish or nearly so, and small couplings) are held to F_r itself.  Against the h column
+    itself: |J - D_h| <= |D_h - R| + 1e-6 |R| + F_r."""
     import json
     import os
 
@@ -82,8 +86,7 @@ def test_jacobian_with_o_against_oracle_central_differences():
     fd = np.array(fx["central_h"])
     rich = np.array(fx["richardson"])
     vals = np.array(fx["values"])
-    floor = 4 * np.finfo(float).eps * np.abs(vals) / fx["h"]
-    assert np.all(np.abs(rich - fd) <= 1e-6 * np.abs(fd) + floor[:, None])
+    floor = (8 * np.finfo(float).eps * np.abs(vals) / fx["h"])[:, None]
     cases, sp, ol, z, w = HO.configuration()
     sc = CL.SublatticeChains(cases, HO.NLEV)
     enu = torch.zeros(5, 3, dtype=torch.float64)
@@ -97,6 +100,8 @@ def test_jacobian_with_o_against_oracle_central_differences():
     for r, o in enumerate(outs):
         gr = torch.autograd.grad(o, params, retain_graph=True)
         jac[r] = np.concatenate([g.numpy().ravel() for g in gr])
-    err = np.abs(jac - fd) - (1e-6 * np.abs(fd) + floor[:, None])
+    err = np.abs(jac - rich) - (1e-6 * np.abs(rich) + floor)
     r, k = np.unravel_index(np.argmax(err), err.shape)
-    assert np.all(err <= 0), (r, k, jac[r, k], fd[r, k])
+    assert np.all(err <= 0), (r, k, jac[r, k], rich[r, k])
+    err_h = np.abs(jac - fd) - (np.abs(fd - rich) + 1e-6 * np.abs(rich) + floor)
+    assert np.all(err_h <= 0)
