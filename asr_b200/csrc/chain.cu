@@ -1569,7 +1569,14 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     mmax = std::max(mmax, g.nlev);
   }
   if (mmax > NLMAX) { set_error("adjoint: depth above %d", NLMAX); return ASR_EINVAL; }
-  const int c = std::max(1, stride > 0 ? stride : (int)std::ceil(std::sqrt((double)mmax)));
+  // Vectors kept for the reverse sweep: every level's (keep = true, no recomputation) when the caller leaves the stride
+  // to the library and a batch of at least 4 tiles fits in half the free device memory; else checkpoints every c
+  // levels (c = stride, or ceil(sqrt(depth))) with the segments recomputed.  Both give the same bits.
+  size_t freeb0 = 0, totb0 = 0;
+  cudaMemGetInfo(&freeb0, &totb0);
+  const size_t vbytes = (size_t)nn * 9 * TL * sizeof(T2);
+  const bool keep = stride <= 0 && (size_t)4 * (3 * mmax + 15 + (gen ? 3 * mmax + 3 : 0)) * vbytes <= freeb0 / 2;
+  const int c = keep ? std::max(1, mmax) : std::max(1, stride > 0 ? stride : (int)std::ceil(std::sqrt((double)mmax)));
   const int nseg = (mmax + c - 1) / c;
   // tiles: one group each
   std::vector<std::vector<int>> tiles;
@@ -1686,12 +1693,34 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     const int grid = nt * bpt;
     int kmax = 0;
     for (int q = 0; q < nlp; ++q) if (hgroup[q] >= 0) kmax = std::max(kmax, ginfo[hgroup[q]].nlev);
-    // ---- forward with checkpoints (X_{k0-1}, X_{k0}) at k0 = 1 + j c
-    k_init<ST><<<std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256), 256, 0, s>>>(bv, FW[1], FW[0]);
+    // ---- forward with checkpoints (X_{k0-1}, X_{k0}) at k0 = 1 + j c, or keeping every level in the segment buffers
     const size_t cpy = (size_t)nt * nn * 9 * TL * sizeof(T2);
-    ASR_CUDA(cudaMemcpyAsync(CK(0, 0), FW[0], cpy, cudaMemcpyDeviceToDevice, s));
-    ASR_CUDA(cudaMemcpyAsync(CK(0, 1), FW[1], cpy, cudaMemcpyDeviceToDevice, s));
-    for (int k = 1; k <= kmax; ++k) {
+    if (keep) {
+      k_init<ST><<<std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256), 256, 0, s>>>(bv, XS(1), XS(0));
+      for (int k = 1; k <= kmax; ++k) {   // the recomputation's step, with the reductions of the forward
+        const int q = k - 1;
+        if (gen) {
+          apply_general_keep<ST>(op, bv, dunif, XS(q + 1), YS(q), TS(q), HS(q), RS(q), QS(q), TMP, d_part.p, npw, grid, s);
+        } else if (dunif) {
+          BatchView bvt = bv;
+          bvt.t2out = TS(q);
+          launch_smul<ST, true, true, true>(op, bvt, blk, XS(q + 1), YS(q), d_part.p, npw, grid, s);
+        } else {
+          apply_SD<ST>(op, bv, dunif, XS(q + 1), TMP, TS(q), d_part.p, npw, grid, s);
+          k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TS(q), XS(q + 1), PCEB, true, XS(q + 1), false, nullptr, 1.0, true,
+                                                  YS(q), d_part.p, npw);
+        }
+        k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+        ASR_CUDA(cudaMemcpyAsync(XS(q + 2), YS(q), cpy, cudaMemcpyDeviceToDevice, s));
+        k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, XS(q + 2), XS(q + 1), XS(q), d_part.p, npw);
+        k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
+      }
+    } else {
+      k_init<ST><<<std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256), 256, 0, s>>>(bv, FW[1], FW[0]);
+      ASR_CUDA(cudaMemcpyAsync(CK(0, 0), FW[0], cpy, cudaMemcpyDeviceToDevice, s));
+      ASR_CUDA(cudaMemcpyAsync(CK(0, 1), FW[1], cpy, cudaMemcpyDeviceToDevice, s));
+    }
+    for (int k = 1; k <= (keep ? 0 : kmax); ++k) {
       T2* U = FW[k % 3];
       T2* UP = FW[(k + 2) % 3];
       T2* Y = FW[(k + 1) % 3];
@@ -1743,10 +1772,12 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     for (int j = nseg - 1; j >= 0; --j) {
       const int k0 = 1 + j * c, k1 = std::min(kmax, k0 + c - 1);
       if (k0 > kmax) continue;
-      // recompute X_{k0-1} .. X_{k1+1}, Y_k, T2_k
-      ASR_CUDA(cudaMemcpyAsync(XS(0), CK(j, 0), cpy, cudaMemcpyDeviceToDevice, s));
-      ASR_CUDA(cudaMemcpyAsync(XS(1), CK(j, 1), cpy, cudaMemcpyDeviceToDevice, s));
-      for (int k = k0; k <= k1; ++k) {
+      // recompute X_{k0-1} .. X_{k1+1}, Y_k, T2_k (kept from the forward in the keep mode)
+      if (!keep) {
+        ASR_CUDA(cudaMemcpyAsync(XS(0), CK(j, 0), cpy, cudaMemcpyDeviceToDevice, s));
+        ASR_CUDA(cudaMemcpyAsync(XS(1), CK(j, 1), cpy, cudaMemcpyDeviceToDevice, s));
+      }
+      for (int k = k0; k <= (keep ? k0 - 1 : k1); ++k) {
         int q = k - k0;
         k_set_fwd<<<(nlp + 127) / 128, 128, 0, s>>>(bv, S, nlp, k);
         if (gen) {
@@ -1815,7 +1846,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     }
     const int nsd = dunif ? 1 : 2;                       // launches of one S application
     const int nap = gen ? 2 * nsd + 3 : nsd + 1;         // launches of one operator application
-    ctx->launches += 1 + (int64_t)kmax * ((nap + 3) + (nap + 2) + (nap + 11));
+    ctx->launches += 1 + (int64_t)kmax * ((nap + 3) + (keep ? 0 : nap + 2) + (nap + 11));
   }
   ASR_TRY(check_wait_error(ctx));
   return ASR_OK;

@@ -149,3 +149,15 @@ def test_dos_gradient_through_autograd():
             return f(v)
         fd = _central(shifted)
         assert abs(grads[a][s, l].item() - fd) <= 1e-6 * max(abs(fd), 1e-2 * gmax), (a, s, l, grads[a][s, l].item(), fd)
+
+
+def test_kept_vectors_and_checkpoints_give_the_same_bits():
+    """stride 0 keeps every level's vectors when the device has room (no recomputation); explicit strides checkpoint and
+    recompute: the general operator's gradient is the same bit for bit."""
+    op, specs, _ = _setup(seed=2)
+    z = np.linspace(-0.4, 0.2, 5) + 0.06j
+    w = np.ones((5, 3), complex)
+    ref = CH.chains_adjoint_ext(op, specs, z, w, 0.0, "hull", "fp64", True, stride=0)[2]
+    for stride in (1, 3, 40):
+        gr = CH.chains_adjoint_ext(op, specs, z, w, 0.0, "hull", "fp64", True, stride=stride)[2]
+        assert np.array_equal(gr, ref), stride
