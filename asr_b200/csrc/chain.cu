@@ -713,10 +713,12 @@ __device__ __forceinline__ void project_node(const OpView& op, int i, unsigned l
   for (int l = 0; l < 9; ++l) x[l] = cscale(acc[l], 1.0 / (double)ns);
 }
 
+// w = y - a u - b u' (projected) and the partials of w . w; w replaces y, or goes to wout when given (y kept)
 template <typename ST>
 __global__ void __launch_bounds__(WPB * TL) k_lanczos_w(OpView op, BatchView bv, typename St2<ST>::T* __restrict__ y,
                                                         const typename St2<ST>::T* __restrict__ u,
-                                                        const typename St2<ST>::T* __restrict__ up, double2* part, int npw) {
+                                                        const typename St2<ST>::T* __restrict__ up, double2* part, int npw,
+                                                        typename St2<ST>::T* __restrict__ wout = nullptr) {
   NodeIter it;
   int bpt;
   if (!node_iter(bv, npw, it, bpt)) return;
@@ -744,7 +746,8 @@ __global__ void __launch_bounds__(WPB * TL) k_lanczos_w(OpView op, BatchView bv,
     } else {
       for (int l = 0; l < 9; ++l) x[l] = make_double2(0, 0);
     }
-    for (int l = 0; l < 9; ++l) stv(y + vix(it.tile, bv.nn, i, l) + lane, x[l]);
+    typename St2<ST>::T* dst = wout ? wout : y;
+    for (int l = 0; l < 9; ++l) stv(dst + vix(it.tile, bv.nn, i, l) + lane, x[l]);
   }
   block_reduce_store(dot, part, it.tile, bpt);
   if (bv.tick && last_block_of_tile(bv.tick, it.tile, bpt) && threadIdx.x < TL)
@@ -1711,8 +1714,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
                                                   YS(q), d_part.p, npw);
         }
         k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
-        ASR_CUDA(cudaMemcpyAsync(XS(q + 2), YS(q), cpy, cudaMemcpyDeviceToDevice, s));
-        k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, XS(q + 2), XS(q + 1), XS(q), d_part.p, npw);
+        k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, YS(q), XS(q + 1), XS(q), d_part.p, npw, XS(q + 2));
         k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
       }
     } else {
@@ -1791,8 +1793,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
           k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TS(q), XS(q + 1), PCEB, true, XS(q + 1), false, nullptr, 1.0, true,
                                                   YS(q), d_part.p, npw);
         }
-        ASR_CUDA(cudaMemcpyAsync(XS(q + 2), YS(q), cpy, cudaMemcpyDeviceToDevice, s));
-        k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, XS(q + 2), XS(q + 1), XS(q), d_part.p, npw);
+        k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, YS(q), XS(q + 1), XS(q), d_part.p, npw, XS(q + 2));
       }
       // reverse k = k1 .. k0
       for (int k = k1; k >= k0; --k) {
