@@ -25,7 +25,7 @@ FP64, FP32 = 0, 1
 
 # names of every exported entry point declared in include/asr_b200.h
 EXPORTS = ["asr_version", "asr_last_error", "asr_ctx_create", "asr_ctx_destroy", "asr_ctx_sync", "asr_ctx_stats",
-           "asr_ctx_set_stream", "asr_ctx_profile", "asr_ctx_kernel_stats", "asr_ctx_kernel_stats_kind",
+           "asr_ctx_set_stream", "asr_ctx_profile", "asr_ctx_hold_workspace", "asr_ctx_kernel_stats", "asr_ctx_kernel_stats_kind",
            "asr_ctx_launches", "asr_op_build", "asr_op_free", "asr_op_dims", "asr_op_export_tables",
            "asr_op_set_params", "asr_op_freeze_site", "asr_op_freeze_any", "asr_op_unfreeze", "asr_op_set_start",
            "asr_op_set_chi", "asr_op_set_class_conc", "asr_op_apply", "asr_op_rand_c", "asr_op_project_c",
@@ -72,6 +72,7 @@ def lib():
     L.asr_ctx_stats.argtypes = [vp, i64_p, i64_p, i64_p]
     L.asr_ctx_set_stream.argtypes = [vp, vp]
     L.asr_ctx_profile.argtypes = [vp, C.c_int]
+    L.asr_ctx_hold_workspace.argtypes = [vp, C.c_int]
     L.asr_ctx_kernel_stats.argtypes = [vp, d_p, i64_p, d_p, d_p]
     L.asr_ctx_kernel_stats_kind.argtypes = [vp, C.c_int, d_p, i64_p, d_p, d_p]
     L.asr_ctx_launches.argtypes = [vp, i64_p]

@@ -61,7 +61,12 @@ class Context:
         """Run on the caller's CUDA stream (e.g. ``torch.cuda.current_stream().cuda_stream``); None: the own stream."""
         check(lib().asr_ctx_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
-    KERNEL_KINDS = {"step": 0, "lanczos": 1, "kpm": 2, "adjoint": 3}
+    KERNEL_KINDS = {"step": 0, "lanczos": 1, "kpm": 2, "adjoint": 3, "adj_step": 4, "adj_vec": 5, "adj_grad": 6,
+                    "adj_scal": 7}
+
+    def hold_workspace(self, on: bool):
+        """Keep the adjoint's device vector memory in this context between calls (on) or free it (off, the default)."""
+        check(lib().asr_ctx_hold_workspace(self.h, int(bool(on))))
 
     def profile(self, on: bool):
         """Start (and clear) or stop the per-launch event timing of the hot kernels."""
@@ -69,7 +74,9 @@ class Context:
 
     def kernel_stats(self, kind: str = "step") -> dict:
         """Summed device time, launches and algorithmic bytes and flops of one kernel kind since ``profile(True)``:
-        'step' (chain step operator), 'lanczos' (Lanczos update), 'kpm' (Chebyshev step), 'adjoint' (reverse level)."""
+        'step' (chain step operator), 'lanczos' (Lanczos update), 'kpm' (Chebyshev step), 'adjoint' (reverse level), and
+        the reverse level's parts 'adj_step' (operator on wbar), 'adj_vec' (vector updates), 'adj_grad' (parameter
+        gradient) and 'adj_scal' (dot sums and scalars)."""
         ms, n, by, fl = C.c_double(), C.c_int64(), C.c_double(), C.c_double()
         check(lib().asr_ctx_kernel_stats_kind(self.h, self.KERNEL_KINDS[kind], C.byref(ms), C.byref(n), C.byref(by),
                                               C.byref(fl)))

@@ -249,6 +249,7 @@ int asr_ctx_destroy(asr_ctx* ctx) {
   dg.set(ctx->device);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   if (ctx->d_err) cudaFree(ctx->d_err);
+  ctx->ws_release();
   for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
   delete ctx;
   return ASR_OK;
@@ -264,6 +265,7 @@ static int drain_events(asr_ctx* ctx) {
   if (ctx->ev_used == 0) return ASR_OK;
   ASR_CUDA(cudaStreamSynchronize(ctx->stream));
   for (int q = 0; q < ctx->ev_used; ++q) {
+    if (ctx->ev_kind[q] < 0) continue;   // started and never stopped (an error path)
     float ms = 0.f;
     ASR_CUDA(cudaEventElapsedTime(&ms, ctx->ev_pool[2 * q], ctx->ev_pool[2 * q + 1]));
     ctx->prof[ctx->ev_kind[q]].ms += ms;
@@ -278,6 +280,17 @@ int asr_ctx_profile(asr_ctx* ctx, int on) {
   ctx->profile = on;
   if (on)
     for (auto& p : ctx->prof) p = asr_ctx::ProfStat();
+  return ASR_OK;
+}
+
+int asr_ctx_hold_workspace(asr_ctx* ctx, int on) {
+  if (!ctx) { set_error("asr_ctx_hold_workspace: null context"); return ASR_EINVAL; }
+  ASR_ON_DEVICE(ctx->device);
+  if (!on && ctx->ws) {
+    ASR_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->ws_release();
+  }
+  ctx->ws_hold = on != 0;
   return ASR_OK;
 }
 

@@ -141,6 +141,22 @@ __device__ __forceinline__ void block_reduce_store(double2 v, double2* part, int
 // Ticket of a finished block: true in every thread of the block of `tile` that stored its partials last, once all bpt
 // blocks of the tile have stored theirs (no block waits on another).  The last block resets the ticket for the next
 // launch.  Every thread of the block calls it, after block_reduce_store.
+// sum_{q < n} p[q * stride] added in the order q = 0, 1, ... (the bits of the plain loop), with the loads issued sixteen
+// at a time so that one L2 latency covers sixteen partials instead of one (the per-tile partial arrays hold nn / 32 rows)
+__device__ __forceinline__ double2 sum_ordered(const double2* __restrict__ p, int n, size_t stride) {
+  double2 s = make_double2(0, 0);
+  int q = 0;
+  for (; q + 16 <= n; q += 16) {
+    double2 v[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __ldcg(p + (size_t)(q + j) * stride);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) s = cadd(s, v[j]);
+  }
+  for (; q < n; ++q) s = cadd(s, __ldcg(p + (size_t)q * stride));
+  return s;
+}
+
 __device__ __forceinline__ bool last_block_of_tile(int* tick, int tile, int bpt) {
   __shared__ int s_last;
   __threadfence();   // the partials this block stored, before its ticket
@@ -164,7 +180,7 @@ __device__ __forceinline__ void reduce_a_lane(const BatchView& bv, const double2
   bv.lane_wact[L] = 0;
   if (grp < 0 || !bv.lane_act[L]) return;
   double2 a = make_double2(0, 0);
-  for (int q = 0; q < bpt; ++q) a = cadd(a, __ldcg(part + ((size_t)tile * bpt + q) * TL + lane));
+  a = cadd(a, sum_ordered(part + (size_t)tile * bpt * TL + lane, bpt, TL));
   bv.acur[L] = a;
   bv.acoef[(size_t)L * NLMAX + k - 1] = a;
   bv.lane_m[L] = k;
@@ -194,7 +210,7 @@ __device__ __forceinline__ void reduce_b_lane(const BatchView& bv, const double2
   bool act = false;
   if (tile_live && grp >= 0 && bv.lane_wact[L]) {
     double2 ww = make_double2(0, 0);
-    for (int q = 0; q < bpt; ++q) ww = cadd(ww, __ldcg(part + ((size_t)tile * bpt + q) * TL + lane));
+    ww = cadd(ww, sum_ordered(part + (size_t)tile * bpt * TL + lane, bpt, TL));
     double2 b = bv.mode == ASR_MODE_PLAIN ? make_double2(sqrt(ww.x), 0.0) : csqrt_p(ww);
     bv.bcoef[(size_t)L * NLMAX + k - 1] = b;
     bool ok = bv.mode == ASR_MODE_PLAIN ? (b.x >= btol) : (cmag(b) >= btol);   // |b| < 1e-12 ends the chain
@@ -238,8 +254,10 @@ constexpr unsigned long long PW_IDENTITY = 0x876543210ull;
 constexpr unsigned long long PW_PERM_MASK = 0xFFFFFFFFFull;   // the nine 4-bit orbital indices
 
 // the output of one node of the S application: t2 (unscaled), or with FINAL y = s (d t2 + (c + e + X(z)) U) and the
-// node's share of the dot sum norb (s U) . y
-template <typename ST, bool FINAL, bool T2OUT = false, typename T2, typename A2>
+// node's share of the dot sum norb (s U) . y.  EPI 1: also t2 = S (d o U) into bv.t2out.  EPI 2 (the adjoint, U = wbar_k,
+// unit scales): t2 into bv.t2out and, in place of y, ubar_k = y + ca Y_k - cb U - cc wbar_{k+1} into bv.adj.ubk, the dot
+// being sum norb ubar_k . X_k (raw)
+template <typename ST, bool FINAL, int EPI = 0, typename T2, typename A2>
 __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView& bv, int tile, int i, int lane, int L, int grp,
                                               int gflags, int gfrozen, const unsigned long long* piw, const T2* __restrict__ in,
                                               T2* __restrict__ out, const A2* acc, double2& dot) {
@@ -255,6 +273,8 @@ __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView&
     const double norb = op.sq[i] * op.sq[i];
     const int fs = (op.start[i] && gfrozen > 0) ? gfrozen : (int)op.frozen[i];
     const int nsm = op.nsmax, kap = op.ncl[i], l0 = op.lst[i], nk = op.nsc[kap];
+    double2 ea = make_double2(0, 0), eb = ea, ec = ea;
+    if (EPI == 2) { ea = bv.adj.ca[L]; eb = bv.adj.cb[L]; ec = bv.adj.cc[L]; }
 #pragma unroll
     for (int l = 0; l < 9; ++l) {
       double2 ui = ld(in + vix(tile, bv.nn, i, l) + lane);
@@ -274,12 +294,21 @@ __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView&
         }
       }
       double2 y = cmul(s, cadd(make_double2(acc[l].x, acc[l].y), pt));
-      stv_cs(out + vix(tile, bv.nn, i, l) + lane, y);
-      if (T2OUT) {   // the blocks carry d on both sides: t2 = S (d o U) = acc / d_l
+      const size_t q = vix(tile, bv.nn, i, l) + lane;
+      if (EPI != 2) stv_cs(out + q, y);
+      if (EPI >= 1) {   // the blocks carry d on both sides: t2 = S (d o U) = acc / d_l
         const double il = 1.0 / bv.ginfo[grp >= 0 ? grp : 0].dd[l];
-        stv((T2*)bv.t2out + vix(tile, bv.nn, i, l) + lane, make_double2(acc[l].x * il, acc[l].y * il));
+        stv((T2*)bv.t2out + q, make_double2(acc[l].x * il, acc[l].y * il));
       }
-      dot = cadd(dot, cscale(cmul(cmul(s, ui), y), norb));
+      if (EPI == 2) {
+        double2 ub = cadd(y, cmul(ea, ld((const T2*)bv.adj.yk + q)));
+        ub = csub(ub, cmul(eb, ui));
+        ub = csub(ub, cmul(ec, ld((const T2*)bv.adj.wbn + q)));
+        stv((T2*)bv.adj.ubk + q, ub);
+        dot = cadd(dot, cscale(cmul(ub, ld((const T2*)bv.adj.xk + q)), norb));
+      } else {
+        dot = cadd(dot, cscale(cmul(cmul(s, ui), y), norb));
+      }
     }
   }
 }
@@ -292,7 +321,7 @@ __device__ __forceinline__ void smul_node_out(const OpView& op, const BatchView&
 // LINK_ID: links whose orbital operation keeps the orbital order (the identity, and the pure sign changes of diagonal
 // groups such as D2h) gather their nine rows at fixed offsets, without the per-orbital index and sign decoding; the
 // products and their order are those of the general path, so both instantiations give the same bits.
-template <typename ST, bool FUSE_D, bool FINAL, bool LINK_ID, bool T2OUT = false>
+template <typename ST, bool FUSE_D, bool FINAL, bool LINK_ID, int EPI = 0>
 __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, const ST* __restrict__ blocks,
                                                    const typename St2<ST>::T* __restrict__ in,
                                                    typename St2<ST>::T* __restrict__ out, double2* part, int npw) {
@@ -401,7 +430,7 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
         acc[l].y = fma_(row[8], v[8].y, acc[l].y);
       }
     }
-    smul_node_out<ST, FINAL, T2OUT>(op, bv, it.tile, i, lane, L, grp, gflags, gfrozen, piw, in, out, acc, dot);
+    smul_node_out<ST, FINAL, EPI>(op, bv, it.tile, i, lane, L, grp, gflags, gfrozen, piw, in, out, acc, dot);
   }
   if (FINAL) {
     block_reduce_store(dot, part, it.tile, bpt);
@@ -917,16 +946,16 @@ bool smul_bulk_enabled() {
   return on == 1;
 }
 
-template <typename ST, bool FUSE_D, bool FINAL, bool T2OUT = false>
+template <typename ST, bool FUSE_D, bool FINAL, int EPI = 0>
 void launch_smul(asr_op* op, const BatchView& bv, const ST* blk, const typename St2<ST>::T* in, typename St2<ST>::T* out,
                  double2* part, int npw, int grid, cudaStream_t s) {
   OpView ov = op->view();
   const int pix = std::is_same<ST, double>::value ? 0 : 1;
-  if (T2OUT) {   // the adjoint's fused step that also stores t2 (bv.t2out)
+  if (EPI) {   // the adjoint's fused steps: also t2 (bv.t2out); EPI 2, the reverse epilogue (bv.adj)
     if (op->tuned_link[pix] == 1)
-      k_smul<ST, FUSE_D, FINAL, true, T2OUT><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
+      k_smul<ST, FUSE_D, FINAL, true, EPI><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
     else
-      k_smul<ST, FUSE_D, FINAL, false, T2OUT><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
+      k_smul<ST, FUSE_D, FINAL, false, EPI><<<grid, WPB * TL, smul_smem(op, sizeof(ST)), s>>>(ov, bv, blk, in, out, part, npw);
     return;
   }
   if (smul_bulk_enabled())
@@ -1233,7 +1262,7 @@ __global__ void __launch_bounds__(WPB * TL) k_dot(OpView op, BatchView bv, const
 
 // wbar = P (c1 ubar_next + c2 X_next); partial dots wbar . X_k and wbar . X_{k-1}
 template <typename ST>
-__global__ void __launch_bounds__(WPB * TL) k_adj_w(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ ubn,
+__global__ void __launch_bounds__(WPB * TL, 2) k_adj_w(OpView op, BatchView bv, const typename St2<ST>::T* __restrict__ ubn,
                                                     const typename St2<ST>::T* __restrict__ xn, const typename St2<ST>::T* __restrict__ xk,
                                                     const typename St2<ST>::T* __restrict__ xkm, const double2* c1, const double2* c2,
                                                     typename St2<ST>::T* __restrict__ wb, double2* part1, double2* part2, int npw) {
@@ -1332,9 +1361,10 @@ struct AdjVecs {   // per level: node side (yb: ybar; tb = S D ybar; hb = h ybar
   const void *yb, *tb, *hb, *rb, *qb;
   const void *xk, *tk, *hk, *rk, *qk;
 };
-template <typename ST, bool GEN>
+template <typename ST, bool GEN, bool WY = false>
 __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, const double* mt, const int* spc, int ldspc,
-                                                       AdjVecs V, const double2* sk, int nodes_per_block, double2* gpart) {
+                                                       AdjVecs V, const double2* sk, int nodes_per_block, double2* gpart,
+                                                       const double2* cy = nullptr) {
   typedef typename St2<ST>::T T2;
   const T2 *yb = (const T2*)V.yb, *tb = (const T2*)V.tb, *hb = (const T2*)V.hb, *rb = (const T2*)V.rb, *qb = (const T2*)V.qb;
   const T2 *xk = (const T2*)V.xk, *tk = (const T2*)V.tk, *hk = (const T2*)V.hk, *rk = (const T2*)V.rk, *qk = (const T2*)V.qk;
@@ -1352,11 +1382,16 @@ __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, 
   if (live) {
     const GroupInfo gi = bv.ginfo[grp];
     const double2 s = sk[L];
+    const double2 c3 = WY ? cy[L] : make_double2(0, 0);
     z = bv.lane_z[L];
     const int i0 = blk * nodes_per_block, i1 = min(bv.nn, i0 + nodes_per_block);
     for (int i = i0; i < i1; ++i) {
       size_t q = vix(tile, bv.nn, i, l) + lane;
-      const double2 y = ld(yb + q), ty = ld(tb + q);
+      double2 y = ld(yb + q), ty = ld(tb + q);
+      if (WY) {   // the fused reverse step passes wbar and S D wbar: ybar = wbar + c3 X_k, S D ybar = S D wbar + c3 S D X_k
+        y = cadd(y, cmul(c3, ld(xk + q)));
+        ty = cadd(ty, cmul(c3, ld(tk + q)));
+      }
       double2 hy = make_double2(0, 0), ry = hy, qy = hy;
       if (GEN) { hy = ld(hb + q); ry = ld(rb + q); qy = ld(qb + q); }
       const double nb = op.sq[i] * op.sq[i];
@@ -1440,7 +1475,7 @@ __global__ void k_adj_gsum(int ntile, int gbpt, int ng, const int* tile_act, con
   if (tile >= ntile || !tile_act[tile]) return;
   for (int e = threadIdx.x; e < ng; e += blockDim.x) {
     double2 sum = make_double2(0, 0);
-    for (int b = 0; b < gbpt; ++b) sum = cadd(sum, gpart[(size_t)(tile * gbpt + b) * ng + e]);
+    sum = cadd(sum, sum_ordered(gpart + (size_t)tile * gbpt * ng + e, gbpt, ng));
     gacc[(size_t)tile * ng + e] = cadd(gacc[(size_t)tile * ng + e], sum);
   }
 }
@@ -1451,13 +1486,18 @@ __global__ void k_lane_sum(int ntile, int bpt, const int* tile_act, const double
   if (tile >= ntile) return;
   double2 sum = make_double2(0, 0);
   if (tile_act[tile])
-    for (int q = 0; q < bpt; ++q) sum = cadd(sum, part[((size_t)tile * bpt + q) * TL + lane]);
+    sum = cadd(sum, sum_ordered(part + (size_t)tile * bpt * TL + lane, bpt, TL));
   out[tile * TL + lane] = sum;
 }
 
 // scalars of reverse step k for every lane (state arrays indexed [lane][NLMAX], k 1-based):
-//   phase 0: coefficients of wbar from d1 = ubar_{k+1} . X_{k+1} (raw)
-//   phase 1: abar', bbar_{k-1} update from d2 = wbar . X_k, d3 = wbar . X_{k-1} (raw)
+//   phase 0: coefficients of wbar from d1 = ubar_{k+1} . X_{k+1} (raw); with tile_act, a tile takes part in step k
+//            when one of its lanes is at least k deep (a warp of the launch is a tile)
+//   phase 1: abar', bbar_{k-1} update from d2 = wbar . X_k, d3 = wbar . X_{k-1} (raw), the coefficients of ybar and of
+//            ubar_k += A ybar + abar y_k - a_k wbar, ubar_{k-1} -= b_{k-1} wbar
+//   phase 2: phase 1 for the fused reverse step, where A ybar = A wbar + abar y_k and ubar_k is written whole:
+//            ubar_k = A wbar + 2 abar y_k - a_k wbar - b_k wbar_{k+1} (c5 = 2 abar, c6 = a_k, c4 = b_k below the lane's
+//            last level, else 0)
 struct AdjScal {
   const double2* a;       // forward a_k
   const double2* b;       // forward b_k
@@ -1474,9 +1514,13 @@ __device__ __forceinline__ double2 scale_of(const AdjScal& S, int L, int k) {   
   if (cmag(b) == 0.0 || k > S.m[L]) return make_double2(0, 0);
   return cdiv(make_double2(1.0, 0.0), b);
 }
-__global__ void k_adj_scal(AdjScal S, int nlane, const int* lane_group, int k, int phase) {
+__global__ void k_adj_scal(AdjScal S, int nlane, const int* lane_group, int k, int phase, int* tile_act = nullptr) {
   int L = blockIdx.x * blockDim.x + threadIdx.x;
-  if (L >= nlane) return;
+  if (L >= nlane) return;   // nlane is a multiple of TL: whole warps leave
+  if (tile_act) {
+    const unsigned any = __ballot_sync(0xffffffffu, lane_group[L] >= 0 && k <= S.m[L]);
+    if (L % TL == 0) tile_act[L / TL] = any != 0;
+  }
   const double2 zero = make_double2(0, 0);
   if (lane_group[L] < 0 || k > S.m[L]) {
     if (phase == 0) { S.c1[L] = zero; S.c2[L] = zero; S.s_next[L] = zero; S.s_k[L] = zero; S.s_prev[L] = zero; }
@@ -1507,8 +1551,13 @@ __global__ void k_adj_scal(AdjScal S, int nlane, const int* lane_group, int k, i
     S.abar[o + k - 1] = ab;
     if (k > 1) S.bbar[o + k - 2] = csub(S.bbar[o + k - 2], cmul(sp, S.d3[L]));   // bbar_{k-1} -= wbar . u_{k-1}
     S.c3[L] = cmul(ab, sk);                                      // ybar = wbar + abar u_k
-    S.c4[L] = k > 1 ? S.b[o + k - 2] : zero;                     // ubar_{k-1} -= b_{k-1} wbar
-    S.c5[L] = ab;                                                // ubar_k += A ybar + abar y_k - a_k wbar
+    if (phase == 2) {
+      S.c4[L] = k < S.m[L] ? S.b[o + k - 1] : zero;
+      S.c5[L] = cscale(ab, 2.0);
+    } else {
+      S.c4[L] = k > 1 ? S.b[o + k - 2] : zero;                   // ubar_{k-1} -= b_{k-1} wbar
+      S.c5[L] = ab;                                              // ubar_k += A ybar + abar y_k - a_k wbar
+    }
     S.c6[L] = S.a[o + k - 1];
   }
 }
@@ -1577,6 +1626,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   // levels (c = stride, or ceil(sqrt(depth))) with the segments recomputed.  Both give the same bits.
   size_t freeb0 = 0, totb0 = 0;
   cudaMemGetInfo(&freeb0, &totb0);
+  freeb0 += ctx->ws_bytes;   // a held slab is this call's to reuse
   const size_t vbytes = (size_t)nn * 9 * TL * sizeof(T2);
   const bool keep = stride <= 0 && (size_t)4 * (3 * mmax + 15 + (gen ? 3 * mmax + 3 : 0)) * vbytes <= freeb0 / 2;
   const int c = keep ? std::max(1, mmax) : std::max(1, stride > 0 ? stride : (int)std::ceil(std::sqrt((double)mmax)));
@@ -1589,14 +1639,25 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     for (auto& lst : per_group)
       for (size_t q = 0; q < lst.size(); q += TL)
         tiles.emplace_back(lst.begin() + q, lst.begin() + std::min(lst.size(), q + (size_t)TL));
+    // deepest tiles first, so that the tiles of a batch have about one depth: the forward retires a tile at its depth
+    // and the reverse sweep skips a tile above it
+    std::vector<int> ord(tiles.size()), dep(tiles.size());
+    for (size_t t = 0; t < tiles.size(); ++t) { ord[t] = (int)t; dep[t] = ginfo[lane_group[tiles[t][0]]].nlev; }
+    std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return dep[x] > dep[y]; });
+    std::vector<std::vector<int>> sorted(tiles.size());
+    for (size_t t = 0; t < tiles.size(); ++t) sorted[t] = std::move(tiles[ord[t]]);
+    tiles.swap(sorted);
   }
   const int ntile_all = (int)tiles.size();
+  // the fused reverse step (o = 0, d uniform): the step kernel applies A to wbar and writes ubar_k in its epilogue
+  const bool fusedrev = !gen && dunif;
   // memory: forward 3 + checkpoints 2 nseg + segment (c + 2) X + c Y + c T2 + adjoint 7 (+1 temporary) vectors per tile;
   // the general operator keeps h X, O h X, S D O h X per segment level and h ybar, O h ybar, S D O h ybar (3 c + 3 more)
   const size_t vec_bytes = (size_t)nn * 9 * TL * sizeof(T2);
   const int nvec = 3 + 2 * nseg + (c + 2) + 2 * c + 8 + (gen ? 3 * c + 3 : 0);
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
+  freeb += ctx->ws_bytes;
   // tiles per batch: as the forward's default (16), halved while the batch's vectors would take more than half the free
   // device memory (a 16-tile batch of the fcc ternary workload holds about 70 GB)
   int tpb = 16;
@@ -1605,7 +1666,9 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   if ((size_t)nvec * vec_bytes > freeb) { set_error("adjoint: %d vectors of %zu bytes do not fit", nvec, vec_bytes); return ASR_ENOMEM; }
   tpb = std::min(tpb, ntile_all);
   const int npw = 4, npb = WPB * npw, bpt = (nn + npb - 1) / npb;
-  const int gnpb = 64, gbpt = (nn + gnpb - 1) / gnpb, ngd = NGK * 9 * nsp;
+  int gnpb = 64;   // nodes per block of the gradient kernel
+  if (const char* e = getenv("ASR_ADJ_GRAD_NODES")) gnpb = std::max(1, atoi(e));
+  const int gbpt = (nn + gnpb - 1) / gnpb, ngd = NGK * 9 * nsp;
   const int nlp = tpb * TL;
   Dev<double> d_gblob, d_mt;
   Dev<GroupInfo> d_ginfo;
@@ -1616,11 +1679,12 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   ASR_CUDA(cudaMemcpyAsync(d_ginfo.p, ginfo.data(), ginfo.size() * sizeof(GroupInfo), cudaMemcpyHostToDevice, s));
   ASR_CUDA(cudaMemcpyAsync(d_mt.p, op->mt.data(), op->mt.size() * sizeof(double), cudaMemcpyHostToDevice, s));
   ASR_CUDA(cudaMemcpyAsync(d_spc.p, op->spc.data(), op->spc.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-  Dev<int> d_lgroup, d_act, d_wact, d_m, d_tact, d_nfall, d_tgroup;
+  Dev<int> d_lgroup, d_act, d_wact, d_m, d_tact, d_tact0, d_nfall, d_tgroup, d_tick;
   Dev<double2> d_a, d_b, d_abar, d_bbar, d_gprev, d_acur, d_bprev, d_su, d_sup, d_part, d_part2, d_z, d_gpart, d_gacc;
   Dev<double2> d_sn, d_sk, d_sp, d_c[6], d_d1, d_d2, d_d3, d_one;
   ASR_TRY(d_lgroup.alloc(nlp)); ASR_TRY(d_act.alloc(nlp)); ASR_TRY(d_wact.alloc(nlp)); ASR_TRY(d_m.alloc(nlp));
-  ASR_TRY(d_tact.alloc(tpb)); ASR_TRY(d_nfall.alloc(1)); ASR_TRY(d_tgroup.alloc(tpb));
+  ASR_TRY(d_tact.alloc(tpb)); ASR_TRY(d_tact0.alloc(tpb)); ASR_TRY(d_nfall.alloc(1)); ASR_TRY(d_tgroup.alloc(tpb));
+  ASR_TRY(d_tick.alloc(tpb));
   ASR_TRY(d_a.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_b.alloc((size_t)nlp * NLMAX));
   ASR_TRY(d_abar.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_bbar.alloc((size_t)nlp * NLMAX));
   ASR_TRY(d_gprev.alloc(nlp)); ASR_TRY(d_acur.alloc(nlp)); ASR_TRY(d_bprev.alloc(nlp)); ASR_TRY(d_su.alloc(nlp));
@@ -1629,9 +1693,30 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   ASR_TRY(d_sn.alloc(nlp)); ASR_TRY(d_sk.alloc(nlp)); ASR_TRY(d_sp.alloc(nlp));
   for (int q = 0; q < 6; ++q) ASR_TRY(d_c[q].alloc(nlp));
   ASR_TRY(d_d1.alloc(nlp)); ASR_TRY(d_d2.alloc(nlp)); ASR_TRY(d_d3.alloc(nlp)); ASR_TRY(d_one.alloc(nlp));
+  // the vectors: one slab, from the context when it holds one large enough (asr_ctx_hold_workspace), else allocated
+  // here and freed on return
   const size_t vlen = (size_t)tpb * nn * 9 * TL;
-  std::vector<Dev<T2>> V(nvec);
-  for (int q = 0; q < nvec; ++q) ASR_TRY(V[q].alloc(vlen));
+  const size_t slab = (size_t)nvec * vlen * sizeof(T2);
+  Dev<unsigned char> own;
+  T2* vbase = nullptr;
+  if (ctx->ws_hold) {
+    if (ctx->ws_bytes < slab) {
+      ctx->ws_release();
+      if (cudaMalloc(&ctx->ws, slab) != cudaSuccess) {
+        ctx->ws = nullptr;
+        set_error("adjoint: device allocation of %zu bytes failed", slab);
+        return ASR_ENOMEM;
+      }
+      ctx->ws_bytes = slab;
+    }
+    vbase = (T2*)ctx->ws;
+  } else {
+    ASR_TRY(own.alloc(slab));
+    vbase = (T2*)own.p;
+  }
+  struct VecRef { T2* p; };
+  std::vector<VecRef> V(nvec);
+  for (int q = 0; q < nvec; ++q) V[q].p = vbase + (size_t)q * vlen;
   T2* FW[3] = {V[0].p, V[1].p, V[2].p};
   auto CK = [&](int j, int which) { return V[3 + 2 * j + which].p; };          // checkpoint j: X_{k0-1}, X_{k0}
   const int xs0 = 3 + 2 * nseg;
@@ -1677,6 +1762,8 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     ASR_CUDA(cudaMemcpyAsync(d_tgroup.p, tgroup.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemcpyAsync(d_act.p, act.data(), nlp * sizeof(int), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemcpyAsync(d_tact.p, tact.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
+    ASR_CUDA(cudaMemcpyAsync(d_tact0.p, d_tact.p, tpb * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    ASR_CUDA(cudaMemsetAsync(d_tick.p, 0, tpb * sizeof(int), s));
     ASR_CUDA(cudaMemcpyAsync(d_z.p, hz.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemcpyAsync(d_su.p, ones.data(), nlp * sizeof(double2), cudaMemcpyHostToDevice, s));
     ASR_CUDA(cudaMemsetAsync(d_wact.p, 0, nlp * sizeof(int), s));
@@ -1696,26 +1783,46 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     const int grid = nt * bpt;
     int kmax = 0;
     for (int q = 0; q < nlp; ++q) if (hgroup[q] >= 0) kmax = std::max(kmax, ginfo[hgroup[q]].nlev);
-    // ---- forward with checkpoints (X_{k0-1}, X_{k0}) at k0 = 1 + j c, or keeping every level in the segment buffers
+    // ---- forward with checkpoints (X_{k0-1}, X_{k0}) at k0 = 1 + j c, or keeping every level in the segment buffers.
+    // The Lanczos update reduces b_k in its epilogue (the tile's last block), the fused step a_k except at the levels of
+    // the depth test, whose fraction evaluation runs in the separate reduction kernel: the sums are those of the separate
+    // kernels, in the same order.
+    auto depth_due = [&](int k) { return depth_tol > 0.0 && k >= 8 && k % 4 == 0; };
+    // algorithmic work of the forward's kernels (the step's vector streams: read U, write Y, and t2 where kept; the node
+    // tables per tile), as the forward chains count them
+    const double tab = (double)op->nslot * 5 + (double)op->nsmax * 5 + 8 + 8 + 4;
+    auto step_bytes = [&](int streams) { return (double)nt * nn * (streams * 9.0 * TL * sizeof(T2) + tab); };
+    const double step_flops = (double)nt * nn * TL * (op->nslot + 1) * 81.0 * 4.0;
+    const double lanczos_bytes = (double)nt * nn * 4.0 * 9 * TL * sizeof(T2), lanczos_flops = (double)nt * nn * TL * 9 * 30.0;
+    const double vstream = (double)nt * nn * 9 * TL * sizeof(T2), sflops = step_flops;   // one vector stream; one S application
     const size_t cpy = (size_t)nt * nn * 9 * TL * sizeof(T2);
     if (keep) {
       k_init<ST><<<std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256), 256, 0, s>>>(bv, XS(1), XS(0));
       for (int k = 1; k <= kmax; ++k) {   // the recomputation's step, with the reductions of the forward
         const int q = k - 1;
+        const bool a_in_step = fusedrev && !depth_due(k);
+        int ps = ctx->prof_start(s);
         if (gen) {
           apply_general_keep<ST>(op, bv, dunif, XS(q + 1), YS(q), TS(q), HS(q), RS(q), QS(q), TMP, d_part.p, npw, grid, s);
         } else if (dunif) {
           BatchView bvt = bv;
+          bvt.kstep = k;
           bvt.t2out = TS(q);
-          launch_smul<ST, true, true, true>(op, bvt, blk, XS(q + 1), YS(q), d_part.p, npw, grid, s);
+          bvt.tick = a_in_step ? d_tick.p : nullptr;
+          launch_smul<ST, true, true, 1>(op, bvt, blk, XS(q + 1), YS(q), d_part.p, npw, grid, s);
         } else {
           apply_SD<ST>(op, bv, dunif, XS(q + 1), TMP, TS(q), d_part.p, npw, grid, s);
           k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TS(q), XS(q + 1), PCEB, true, XS(q + 1), false, nullptr, 1.0, true,
                                                   YS(q), d_part.p, npw);
         }
-        k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
-        k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, YS(q), XS(q + 1), XS(q), d_part.p, npw, XS(q + 2));
-        k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
+        ctx->prof_stop(s, ps, ASR_KERNEL_STEP, step_bytes(3), step_flops);
+        if (!a_in_step) k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+        BatchView bvw = bv;
+        bvw.kstep = k;
+        bvw.tick = d_tick.p;
+        ps = ctx->prof_start(s);
+        k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bvw, YS(q), XS(q + 1), XS(q), d_part.p, npw, XS(q + 2));
+        ctx->prof_stop(s, ps, ASR_KERNEL_LANCZOS, lanczos_bytes, lanczos_flops);
       }
     } else {
       k_init<ST><<<std::min<size_t>(65535, ((size_t)nt * nn * 9 * TL + 255) / 256), 256, 0, s>>>(bv, FW[1], FW[0]);
@@ -1726,25 +1833,36 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
       T2* U = FW[k % 3];
       T2* UP = FW[(k + 2) % 3];
       T2* Y = FW[(k + 1) % 3];
+      const bool a_in_step = fusedrev && !depth_due(k);
+      int ps = ctx->prof_start(s);
       if (gen) {
         apply_general_keep<ST>(op, bv, dunif, U, Y, AY, WB, YB, T2B, TMP, d_part.p, npw, grid, s);
       } else if (dunif) {   // the fused step of the forward chains (d folded into the blocks)
-        launch_smul<ST, true, true>(op, bv, blk, U, Y, d_part.p, npw, grid, s);
+        BatchView bvt = bv;
+        bvt.kstep = k;
+        bvt.tick = a_in_step ? d_tick.p : nullptr;
+        launch_smul<ST, true, true>(op, bvt, blk, U, Y, d_part.p, npw, grid, s);
       } else {
         apply_SD<ST>(op, bv, dunif, U, TMP, AY, d_part.p, npw, grid, s);
         k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, AY, U, PCEB, true, U, false, nullptr, 1.0, true, Y, d_part.p, npw);
       }
-      k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
-      k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, Y, U, UP, d_part.p, npw);
-      k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
+      ctx->prof_stop(s, ps, ASR_KERNEL_STEP, step_bytes(2), step_flops);
+      if (!a_in_step) k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+      BatchView bvw = bv;
+      bvw.kstep = k;
+      bvw.tick = d_tick.p;
+      ps = ctx->prof_start(s);
+      k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bvw, Y, U, UP, d_part.p, npw);
+      ctx->prof_stop(s, ps, ASR_KERNEL_LANCZOS, lanczos_bytes, lanczos_flops);
       if (k % c == 0 && k / c < nseg) {   // X_k and X_{k+1} start segment k / c
         ASR_CUDA(cudaMemcpyAsync(CK(k / c, 0), U, cpy, cudaMemcpyDeviceToDevice, s));
         ASR_CUDA(cudaMemcpyAsync(CK(k / c, 1), Y, cpy, cudaMemcpyDeviceToDevice, s));
       }
     }
     ASR_CUDA(cudaGetLastError());
-    // the forward retired finished tiles; the recomputation and the reverse sweep visit every tile of the batch
-    ASR_CUDA(cudaMemcpyAsync(d_tact.p, tact.data(), tpb * sizeof(int), cudaMemcpyHostToDevice, s));
+    // the forward retired finished tiles; the recomputation visits every tile of the batch, the reverse step k the tiles
+    // with a lane at least k deep (k_adj_scal)
+    ASR_CUDA(cudaMemcpyAsync(d_tact.p, d_tact0.p, tpb * sizeof(int), cudaMemcpyDeviceToDevice, s));
     // ---- fraction adjoint on the host: G and the seeds abar, bbar
     ASR_CUDA(cudaMemcpyAsync(hm.data(), d_m.p, nlp * sizeof(int), cudaMemcpyDeviceToHost, s));
     ASR_CUDA(cudaMemcpyAsync(ha.data(), d_a.p, ha.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
@@ -1770,12 +1888,21 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     // adjoint BatchView: unit scales for applying A to ybar
     BatchView bva = bv;
     bva.su = d_one.p;
+    // ubar (three rotating buffers; two in the fused step, which writes ubar_k whole) and, in the fused step, wbar of
+    // this and the previous level (WB, YB alternating) start at zero; d1 = ubar_{k+1} . X_{k+1} is zero above the top
     for (int q = 0; q < 3; ++q) ASR_CUDA(cudaMemsetAsync(UB[q], 0, cpy, s));
+    if (fusedrev) {
+      ASR_CUDA(cudaMemsetAsync(WB, 0, cpy, s));
+      ASR_CUDA(cudaMemsetAsync(YB, 0, cpy, s));
+      ASR_CUDA(cudaMemsetAsync(d_d1.p, 0, nlp * sizeof(double2), s));
+    }
+    T2* WBF[2] = {WB, YB};
     for (int j = nseg - 1; j >= 0; --j) {
       const int k0 = 1 + j * c, k1 = std::min(kmax, k0 + c - 1);
       if (k0 > kmax) continue;
-      // recompute X_{k0-1} .. X_{k1+1}, Y_k, T2_k (kept from the forward in the keep mode)
+      // recompute X_{k0-1} .. X_{k1+1}, Y_k, T2_k (kept from the forward in the keep mode) on every tile of the batch
       if (!keep) {
+        ASR_CUDA(cudaMemcpyAsync(d_tact.p, d_tact0.p, tpb * sizeof(int), cudaMemcpyDeviceToDevice, s));
         ASR_CUDA(cudaMemcpyAsync(XS(0), CK(j, 0), cpy, cudaMemcpyDeviceToDevice, s));
         ASR_CUDA(cudaMemcpyAsync(XS(1), CK(j, 1), cpy, cudaMemcpyDeviceToDevice, s));
       }
@@ -1787,7 +1914,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         } else if (dunif) {   // the forward's fused step, bit for bit, with t2 = S d X stored for the gradient
           BatchView bvt = bv;
           bvt.t2out = TS(q);
-          launch_smul<ST, true, true, true>(op, bvt, blk, XS(q + 1), YS(q), d_part.p, npw, grid, s);
+          launch_smul<ST, true, true, 1>(op, bvt, blk, XS(q + 1), YS(q), d_part.p, npw, grid, s);
         } else {
           apply_SD<ST>(op, bv, dunif, XS(q + 1), TMP, TS(q), d_part.p, npw, grid, s);
           k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TS(q), XS(q + 1), PCEB, true, XS(q + 1), false, nullptr, 1.0, true,
@@ -1796,7 +1923,49 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, YS(q), XS(q + 1), XS(q), d_part.p, npw, XS(q + 2));
       }
       // reverse k = k1 .. k0
-      for (int k = k1; k >= k0; --k) {
+      for (int k = k1; k >= k0 && fusedrev; --k) {
+        // wbar_k = P (ubar_{k+1} / b_k + bbar_k u_{k+1}); then one step kernel on wbar_k (unit scales) gives S D wbar_k
+        // and, by linearity (A ybar = A wbar + abar y_k), ubar_k = A wbar_k + 2 abar y_k - a_k wbar_k - b_k wbar_{k+1}
+        // with the dots ubar_k . X_k of the next step; the gradient kernel forms ybar = wbar + abar u_k and
+        // S D ybar = S D wbar + abar S D u_k itself
+        const int q = k - k0;
+        T2* wk = WBF[k % 2];
+        T2* wn = WBF[(k + 1) % 2];
+        T2* ubk = UB[k % 2];
+        T2* ubn = UB[(k + 1) % 2];
+        const int ps = ctx->prof_start(s);
+        int pp = ctx->prof_start(s);
+        k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 0, d_tact.p);
+        ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_SCAL, 0.0, 0.0);
+        pp = ctx->prof_start(s);
+        k_adj_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, ubn, XS(q + 2), XS(q + 1), XS(q), d_c[0].p, d_c[1].p, wk, d_part.p, d_part2.p,
+                                              npw);
+        ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_VEC, vstream * 5.0, 0.0);
+        pp = ctx->prof_start(s);
+        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d2.p);
+        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_d3.p);
+        k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 2);
+        ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_SCAL, 0.0, 0.0);
+        BatchView bvt = bva;
+        bvt.t2out = T2B;
+        bvt.adj = AdjEpi{YS(q), wn, XS(q + 1), ubk, d_c[4].p, d_c[5].p, d_c[3].p};
+        pp = ctx->prof_start(s);
+        launch_smul<ST, true, true, 2>(op, bvt, blk, wk, nullptr, d_part.p, npw, grid, s);
+        ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_STEP, vstream * 6.0, sflops);
+        pp = ctx->prof_start(s);
+        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d1.p);
+        ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_SCAL, 0.0, 0.0);
+        AdjVecs av{wk, T2B, nullptr, nullptr, nullptr, XS(q + 1), TS(q), nullptr, nullptr, nullptr};
+        pp = ctx->prof_start(s);
+        k_adj_grad<ST, false, true><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb,
+                                                                   d_gpart.p, d_c[2].p);
+        k_adj_gsum<<<nt, 128, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
+        ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_GRAD, vstream * 4.0, 0.0);
+        // one fused reverse level: 15 vector streams per (node, lane) (w-bar 5, step 6, parameter gradient 4); flops of its
+        // one S application
+        ctx->prof_stop(s, ps, ASR_KERNEL_ADJOINT, vstream * 15.0, sflops);
+      }
+      for (int k = k1; k >= k0 && !fusedrev; --k) {
         int q = k - k0;
         T2* ubn = UB[(k + 1) % 3];
         T2* ubk = UB[k % 3];
@@ -1804,7 +1973,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         const int ps = ctx->prof_start(s);
         k_dot<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, ubn, XS(q + 2), d_part.p, npw);
         k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d1.p);
-        k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 0);
+        k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 0, d_tact.p);
         k_adj_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, ubn, XS(q + 2), XS(q + 1), XS(q), d_c[0].p, d_c[1].p, WB, d_part.p, d_part2.p,
                                               npw);
         k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d2.p);
@@ -1817,7 +1986,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         } else if (dunif) {
           BatchView bvt = bva;
           bvt.t2out = T2B;
-          launch_smul<ST, true, true, true>(op, bvt, blk, YB, AY, d_part.p, npw, grid, s);
+          launch_smul<ST, true, true, 1>(op, bvt, blk, YB, AY, d_part.p, npw, grid, s);
         } else {
           apply_SD<ST>(op, bva, dunif, YB, TMP, T2B, d_part.p, npw, grid, s);
           k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, T2B, YB, PCEB, true, YB, false, nullptr, 1.0, true, AY, d_part.p, npw);
@@ -1845,9 +2014,12 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
       if (gq < 0) continue;
       for (int e = 0; e < ngd; ++e) grad_out[(size_t)gq * ngd + e] = cadd(grad_out[(size_t)gq * ngd + e], hgacc[(size_t)bt * ngd + e]);
     }
-    const int nsd = dunif ? 1 : 2;                       // launches of one S application
-    const int nap = gen ? 2 * nsd + 3 : nsd + 1;         // launches of one operator application
-    ctx->launches += 1 + (int64_t)kmax * ((nap + 3) + (keep ? 0 : nap + 2) + (nap + 11));
+    // launches per level: forward (operator, a reduction unless in the step, Lanczos update), recomputation (scalars,
+    // operator, update), reverse (fused: 9; else 11 and the operator); the depth test's separate reductions not counted
+    const int nsd = dunif ? 1 : 2;                                       // one S application
+    const int nap = gen ? 2 * nsd + 3 : (dunif ? 1 : nsd + 1);           // one operator application
+    const int fwd = fusedrev ? 2 : nap + 2, rev = fusedrev ? 9 : nap + 11;
+    ctx->launches += 1 + (int64_t)kmax * (fwd + (keep ? 0 : nap + 2) + rev);
   }
   ASR_TRY(check_wait_error(ctx));
   return ASR_OK;
@@ -1961,10 +2133,8 @@ __global__ void k_ed3_reduce_a(BatchView bv, const double2* part_a, const double
   bv.lane_wact[L] = 0;
   if (grp < 0 || !bv.lane_act[L]) return;
   double2 a = make_double2(0, 0), c = make_double2(0, 0);
-  for (int q = 0; q < bpt; ++q) {
-    a = cadd(a, part_a[((size_t)tile * bpt + q) * TL + lane]);
-    c = cadd(c, part_c[((size_t)tile * bpt + q) * TL + lane]);
-  }
+  a = cadd(a, sum_ordered(part_a + (size_t)tile * bpt * TL + lane, bpt, TL));
+  c = cadd(c, sum_ordered(part_c + (size_t)tile * bpt * TL + lane, bpt, TL));
   bv.acur[L] = a;
   bv.acoef[(size_t)L * NLMAX + k - 1] = a;
   ccoef[(size_t)L * NLMAX + k - 1] = c;
@@ -2311,7 +2481,7 @@ __global__ void k_epi_store_c(BatchView bv, const double2* part, int bpt, int k,
   int L = tile * TL + lane;
   if (bv.lane_group[L] < 0 || !bv.lane_act[L]) return;
   double2 c = make_double2(0, 0);
-  for (int q = 0; q < bpt; ++q) c = cadd(c, part[((size_t)tile * bpt + q) * TL + lane]);
+  c = cadd(c, sum_ordered(part + (size_t)tile * bpt * TL + lane, bpt, TL));
   ccoef[(size_t)L * NLMAX + k - 1] = cmul(c, bv.su[L]);
 }
 

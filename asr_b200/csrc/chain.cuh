@@ -30,6 +30,18 @@ struct GroupInfo {
   double dd[9];           // uniform d per orbital (GF_D_UNIFORM)
 };
 
+// Epilogue of the adjoint's operator application (the fused step kernel applied to wbar_k with unit scales): instead of
+// A wbar it stores ubar_k = A wbar_k + ca Y_k - cb wbar_k - cc wbar_{k+1} and the per-lane partial dots ubar_k . X_k.
+struct AdjEpi {
+  const void* yk;          // Y_k = A u_k of the forward
+  const void* wbn;         // wbar_{k+1}
+  const void* xk;          // X_k (unscaled)
+  void* ubk;               // output ubar_k
+  const double2* ca;       // per lane: 2 abar_k
+  const double2* cb;       // a_k
+  const double2* cc;       // b_k (0 at the lane's last level)
+};
+
 // One batch: ntile tiles x TL lanes.  Lane L = tile * TL + j.
 struct BatchView {
   int ntile, nn, nsm, kstep, mode, project, tail, nlevmax;
@@ -57,6 +69,7 @@ struct BatchView {
                            // epilogue of the tile's last block instead of separate reduction launches
   void* t2out;             // optional: the fused step kernel also stores t2 = S (d o U) (unscaled, the vector type of the
                            // batch) for the adjoint's parameter gradient
+  AdjEpi adj;              // the adjoint epilogue's vectors and coefficients (read only by that instantiation)
 };
 
 struct RunOptions {

@@ -25,7 +25,8 @@ struct asr_ctx {
   std::vector<cudaEvent_t> ev_pool;   // pairs (start, end) of the timed launches
   std::vector<int> ev_kind;           // kernel kind of every recorded pair
   int ev_used = 0;                    // pairs recorded and not yet read
-  // starts a timed region on stream s (returns its pair index, -1 when profiling is off); no synchronisation
+  // starts a timed region on stream s (returns its pair index, -1 when profiling is off); regions may nest (a level of
+  // the reverse sweep and its kernels); no synchronisation
   int prof_start(cudaStream_t s) {
     if (!profile) return -1;
     while ((int)ev_pool.size() < 2 * (ev_used + 1)) {
@@ -35,19 +36,28 @@ struct asr_ctx {
     }
     if ((int)ev_kind.size() < ev_used + 1) ev_kind.resize(ev_used + 1);
     if (cudaEventRecord(ev_pool[2 * ev_used], s) != cudaSuccess) return -1;
-    return ev_used;
+    ev_kind[ev_used] = -1;   // open until prof_stop
+    return ev_used++;
   }
   // ends the region `slot` of prof_start as one launch of `kind` with the given algorithmic bytes and flops
   void prof_stop(cudaStream_t s, int slot, int kind, double bytes, double flops) {
-    if (slot < 0 || slot != ev_used) return;
+    if (slot < 0 || slot >= ev_used || ev_kind[slot] != -1) return;
     if (cudaEventRecord(ev_pool[2 * slot + 1], s) != cudaSuccess) return;
     ev_kind[slot] = kind;
-    ++ev_used;
     prof[kind].bytes += bytes;
     prof[kind].flops += flops;
     prof[kind].launches += 1;
   }
   unsigned char* cf_scratch = nullptr;   // device address of asr_cf_eval_noalloc's static array (resolved on first use)
+  // the adjoint's vector slab, kept between calls while ws_hold is set (asr_ctx_hold_workspace)
+  int ws_hold = 0;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  void ws_release() {
+    if (ws) cudaFree(ws);
+    ws = nullptr;
+    ws_bytes = 0;
+  }
 };
 
 namespace asrb {

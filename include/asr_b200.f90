@@ -178,6 +178,9 @@ module asr_b200
     integer(c_int) function asr_ctx_profile(ctx, on) bind(c)
       import; type(c_ptr), value :: ctx; integer(c_int), value :: on
     end function
+    integer(c_int) function asr_ctx_hold_workspace(ctx, on) bind(c)
+      import; type(c_ptr), value :: ctx; integer(c_int), value :: on
+    end function
     integer(c_int) function asr_ctx_kernel_stats(ctx, ms, launches, bytes, flops) bind(c)
       import; type(c_ptr), value :: ctx; real(c_double) :: ms, bytes, flops; integer(c_int64_t) :: launches
     end function

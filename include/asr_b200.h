@@ -61,10 +61,19 @@ enum {
   ASR_KERNEL_STEP = 0,      /* chain step operator (S application, diagonal terms, a-dot) */
   ASR_KERNEL_LANCZOS = 1,   /* Lanczos update w = y - a u - b u', projection, b-dot */
   ASR_KERNEL_KPM = 2,       /* KPM Chebyshev step (block matvec, recurrence, moments) */
-  ASR_KERNEL_ADJOINT = 3,   /* one level of the adjoint's reverse sweep */
-  ASR_KERNEL_KINDS = 4
+  ASR_KERNEL_ADJOINT = 3,   /* one level of the adjoint's reverse sweep (all its kernels; the four kinds below split it) */
+  ASR_KERNEL_ADJ_STEP = 4,  /* reverse sweep: the operator applied to wbar (fused step kernel with the ubar epilogue) */
+  ASR_KERNEL_ADJ_VEC = 5,   /* reverse sweep: the vector updates (wbar = P(...), and ybar, ubar where not fused) */
+  ASR_KERNEL_ADJ_GRAD = 6,  /* reverse sweep: the parameter gradient partials and their per-tile sums */
+  ASR_KERNEL_ADJ_SCAL = 7,  /* reverse sweep: per-lane dot sums and the recurrence scalars */
+  ASR_KERNEL_KINDS = 8
 };
 int asr_ctx_profile(asr_ctx* ctx, int on);
+/* on = 1: the adjoint (asr_chains_adjoint, asr_chains_adjoint_ext) keeps its device vector memory (at most half of the
+ * device memory free when it is first needed) in the context after it returns and reuses it on the next call, instead of
+ * allocating and freeing it per call; on = 0 (the default) frees it.  For loops that take many gradients on one
+ * operator.  No counterpart in the reference (which has no derivatives). */
+int asr_ctx_hold_workspace(asr_ctx* ctx, int on);
 int asr_ctx_kernel_stats(asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops);
 int asr_ctx_kernel_stats_kind(asr_ctx* ctx, int kind, double* ms, int64_t* launches, double* bytes, double* flops);
 /* number of kernels this context has launched (all kinds) */

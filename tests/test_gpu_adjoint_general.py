@@ -161,3 +161,21 @@ def test_kept_vectors_and_checkpoints_give_the_same_bits():
     for stride in (1, 3, 40):
         gr = CH.chains_adjoint_ext(op, specs, z, w, 0.0, "hull", "fp64", True, stride=stride)[2]
         assert np.array_equal(gr, ref), stride
+
+
+def test_held_workspace_gives_the_same_bits():
+    """asr_ctx_hold_workspace: the vector memory kept in the context and reused by the next calls (also by a smaller
+    call) gives the gradient of the allocating call bit for bit; turning it off frees it."""
+    op, specs, _ = _setup(seed=4)
+    z = np.linspace(-0.4, 0.2, 5) + 0.06j
+    w = np.ones((5, 3), complex)
+    ref = CH.chains_adjoint_ext(op, specs, z, w, 0.0, "hull", "fp64", True)[2]
+    op.ctx.hold_workspace(True)
+    try:
+        for zz, ww in ((z, w), (z, w), (z[:2], w[:2])):
+            gr = CH.chains_adjoint_ext(op, specs, zz, ww, 0.0, "hull", "fp64", True)[2]
+            if zz is z:
+                assert np.array_equal(gr, ref)
+    finally:
+        op.ctx.hold_workspace(False)
+    assert np.array_equal(CH.chains_adjoint_ext(op, specs, z, w, 0.0, "hull", "fp64", True)[2], ref)
