@@ -2664,6 +2664,10 @@ static void smem_attrs() {
   cudaFuncSetAttribute(k_smul<double, true, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   cudaFuncSetAttribute(k_smul<float, true, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   cudaFuncSetAttribute(k_smul<float, true, true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, true, true, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<double, true, true, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, true, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+  cudaFuncSetAttribute(k_smul<float, true, true, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
   cudaFuncSetAttribute(k_smul_bulk<double, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_smul_bulk<double, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_smul_bulk<double, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
