@@ -138,25 +138,36 @@ __device__ __forceinline__ void block_reduce_store(double2 v, double2* part, int
   }
 }
 
-// Ticket of a finished block: true in every thread of the block of `tile` that stored its partials last, once all bpt
-// blocks of the tile have stored theirs (no block waits on another).  The last block resets the ticket for the next
-// launch.  Every thread of the block calls it, after block_reduce_store.
-// sum_{q < n} p[q * stride] added in the order q = 0, 1, ... (the bits of the plain loop), with the loads issued sixteen
-// at a time so that one L2 latency covers sixteen partials instead of one (the per-tile partial arrays hold nn / 32 rows)
-__device__ __forceinline__ double2 sum_ordered(const double2* __restrict__ p, int n, size_t stride) {
+// sum_{q < n} p[q * stride] (one double2 per lane, p[lane] the first row) over the warps of the calling block (every
+// thread calls it; at most WPB warps): warp w adds the rows q = w, w + nw, ... in order with the loads issued eight at
+// a time (one L2 latency per eight rows of the nn / 32 partials of a tile), then warp 0 adds the nw warp sums in the
+// order w = 0 .. nw - 1.
+// A fixed order, so the same bits on every run; the result is valid in warp 0 (lane = threadIdx.x).
+__device__ __forceinline__ double2 block_sum_rows(const double2* __restrict__ p, int n, size_t stride, bool load = true) {
+  __shared__ double2 wsum[WPB][TL];
+  const int nw = blockDim.x / TL, w = threadIdx.x / TL, lane = threadIdx.x % TL;
+  const double2* pl = p + lane;
   double2 s = make_double2(0, 0);
-  int q = 0;
-  for (; q + 16 <= n; q += 16) {
-    double2 v[16];
+  int q = load ? w : n;   // a lane without a column (load = false) adds nothing
+  for (; q + 7 * nw < n; q += 8 * nw) {
+    double2 v[8];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __ldcg(p + (size_t)(q + j) * stride);
+    for (int j = 0; j < 8; ++j) v[j] = __ldcg(pl + (size_t)(q + j * nw) * stride);
 #pragma unroll
-    for (int j = 0; j < 16; ++j) s = cadd(s, v[j]);
+    for (int j = 0; j < 8; ++j) s = cadd(s, v[j]);
   }
-  for (; q < n; ++q) s = cadd(s, __ldcg(p + (size_t)q * stride));
+  for (; q < n; q += nw) s = cadd(s, __ldcg(pl + (size_t)q * stride));
+  wsum[w][lane] = s;
+  __syncthreads();
+  if (w == 0)
+    for (int k = 1; k < nw; ++k) s = cadd(s, wsum[k][lane]);
+  __syncthreads();
   return s;
 }
 
+// Ticket of a finished block: true in every thread of the block of `tile` that stored its partials last, once all bpt
+// blocks of the tile have stored theirs (no block waits on another).  The last block resets the ticket for the next
+// launch.  Every thread of the block calls it, after block_reduce_store.
 __device__ __forceinline__ bool last_block_of_tile(int* tick, int tile, int bpt) {
   __shared__ int s_last;
   __threadfence();   // the partials this block stored, before its ticket
@@ -171,16 +182,15 @@ __device__ __forceinline__ bool last_block_of_tile(int* tick, int tile, int bpt)
   return s_last != 0;
 }
 
-// a_k = sum of the partials (fixed order) for one lane of a tile; depth test every 4 levels from 8
+// a_k (asum: the tile's partials summed by block_sum_rows) for one lane of a tile; depth test every 4 levels from 8
 // (src/asr_edc.f90:121-127) when DEPTH (without it the caller guarantees that no depth test is due at level k)
 template <bool DEPTH>
-__device__ __forceinline__ void reduce_a_lane(const BatchView& bv, const double2* part, int bpt, int k, int tile, int lane) {
+__device__ __forceinline__ void reduce_a_lane(const BatchView& bv, double2 asum, int k, int tile, int lane) {
   int L = tile * TL + lane;
   int grp = bv.lane_group[L];
   bv.lane_wact[L] = 0;
   if (grp < 0 || !bv.lane_act[L]) return;
-  double2 a = make_double2(0, 0);
-  a = cadd(a, sum_ordered(part + (size_t)tile * bpt * TL + lane, bpt, TL));
+  const double2 a = asum;
   bv.acur[L] = a;
   bv.acoef[(size_t)L * NLMAX + k - 1] = a;
   bv.lane_m[L] = k;
@@ -202,15 +212,15 @@ __device__ __forceinline__ void reduce_a_lane(const BatchView& bv, const double2
   else bv.lane_act[L] = 0;
 }
 
-// b_k = sqrt(w . w); |b| < tol ends the chain; scales of the next step (u <- w / b, up <- u).  One full warp per tile.
-__device__ __forceinline__ void reduce_b_lane(const BatchView& bv, const double2* part, int bpt, int k, double btol, int tile,
-                                              int lane, bool tile_live) {
+// b_k = sqrt(w . w) (wsum: the tile's partials summed by block_sum_rows); |b| < tol ends the chain; scales of the next
+// step (u <- w / b, up <- u).  One full warp per tile.
+__device__ __forceinline__ void reduce_b_lane(const BatchView& bv, double2 wsum, int k, double btol, int tile, int lane,
+                                              bool tile_live) {
   int L = tile * TL + lane;
   int grp = bv.lane_group[L];
   bool act = false;
   if (tile_live && grp >= 0 && bv.lane_wact[L]) {
-    double2 ww = make_double2(0, 0);
-    ww = cadd(ww, sum_ordered(part + (size_t)tile * bpt * TL + lane, bpt, TL));
+    const double2 ww = wsum;
     double2 b = bv.mode == ASR_MODE_PLAIN ? make_double2(sqrt(ww.x), 0.0) : csqrt_p(ww);
     bv.bcoef[(size_t)L * NLMAX + k - 1] = b;
     bool ok = bv.mode == ASR_MODE_PLAIN ? (b.x >= btol) : (cmag(b) >= btol);   // |b| < 1e-12 ends the chain
@@ -434,8 +444,10 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
   }
   if (FINAL) {
     block_reduce_store(dot, part, it.tile, bpt);
-    if (bv.tick && last_block_of_tile(bv.tick, it.tile, bpt) && threadIdx.x < TL)
-      reduce_a_lane<false>(bv, part, bpt, bv.kstep, it.tile, threadIdx.x);
+    if (bv.tick && last_block_of_tile(bv.tick, it.tile, bpt)) {
+      const double2 a = block_sum_rows(part + (size_t)it.tile * bpt * TL, bpt, TL);
+      if (threadIdx.x < TL) reduce_a_lane<false>(bv, a, bv.kstep, it.tile, threadIdx.x);
+    }
   }
 }
 
@@ -779,8 +791,10 @@ __global__ void __launch_bounds__(WPB * TL) k_lanczos_w(OpView op, BatchView bv,
     for (int l = 0; l < 9; ++l) stv(dst + vix(it.tile, bv.nn, i, l) + lane, x[l]);
   }
   block_reduce_store(dot, part, it.tile, bpt);
-  if (bv.tick && last_block_of_tile(bv.tick, it.tile, bpt) && threadIdx.x < TL)
-    reduce_b_lane(bv, part, bpt, bv.kstep, 1.0e-12, it.tile, threadIdx.x, true);
+  if (bv.tick && last_block_of_tile(bv.tick, it.tile, bpt)) {
+    const double2 ww = block_sum_rows(part + (size_t)it.tile * bpt * TL, bpt, TL);
+    if (threadIdx.x < TL) reduce_b_lane(bv, ww, bv.kstep, 1.0e-12, it.tile, threadIdx.x, true);
+  }
 }
 
 // in-place projection of a batch vector (asr_op_project_c)
@@ -805,16 +819,21 @@ __global__ void __launch_bounds__(WPB * TL) k_project(OpView op, BatchView bv, t
 }
 
 // ------------------------------------------------------------------------------------------------ per-lane scalars
+// the per-tile reduction kernels: one block of RED_THREADS per tile (block_sum_rows), warp 0 finishes per lane
+constexpr int RED_THREADS = WPB * TL;
 __global__ void k_reduce_a(BatchView bv, const double2* part, int bpt, int k) {
-  int tile = blockIdx.x, lane = threadIdx.x;
+  int tile = blockIdx.x;
   if (tile >= bv.ntile || !bv.tile_act[tile]) return;
-  reduce_a_lane<true>(bv, part, bpt, k, tile, lane);
+  const double2 a = block_sum_rows(part + (size_t)tile * bpt * TL, bpt, TL);
+  if (threadIdx.x < TL) reduce_a_lane<true>(bv, a, k, tile, threadIdx.x);
 }
 
 __global__ void k_reduce_b(BatchView bv, const double2* part, int bpt, int k, double btol) {
-  int tile = blockIdx.x, lane = threadIdx.x;
+  int tile = blockIdx.x;
   if (tile >= bv.ntile) return;
-  reduce_b_lane(bv, part, bpt, k, btol, tile, lane, bv.tile_act[tile] != 0);
+  const bool live = bv.tile_act[tile] != 0;
+  const double2 ww = live ? block_sum_rows(part + (size_t)tile * bpt * TL, bpt, TL) : make_double2(0, 0);
+  if (threadIdx.x < TL) reduce_b_lane(bv, ww, k, btol, tile, threadIdx.x, live);
 }
 
 // final fraction of every lane: cf_species with the chosen tail (edc mode); lmap: batch lane -> output lane (-1: none)
@@ -1166,7 +1185,7 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
         ctx->prof_stop(s, ps, ASR_KERNEL_STEP, (double)nt * nn * (2.0 * 9 * TL * sizeof(T2) + tab),
                        (double)nt * nn * TL * (op->nslot + 1) * 81.0 * 4.0);
       }
-      if (!a_in_step) k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+      if (!a_in_step) k_reduce_a<<<nt, RED_THREADS, 0, s>>>(bv, d_part.p, bpt, k);
       BatchView bvw = bv;
       bvw.tick = d_tick.p;
       ps = ctx->prof_start(s);
@@ -1470,24 +1489,21 @@ __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, 
 }
 
 // gacc[tile][NGK][9][nsp] += sum over the blocks of the step's partials (fixed order)
+// grid (ntile, ceil(ng / 32)), RED_THREADS per block: lane j of the block's warps sums entry 32 blockIdx.y + j
 __global__ void k_adj_gsum(int ntile, int gbpt, int ng, const int* tile_act, const double2* gpart, double2* gacc) {
-  int tile = blockIdx.x;
+  const int tile = blockIdx.x;
   if (tile >= ntile || !tile_act[tile]) return;
-  for (int e = threadIdx.x; e < ng; e += blockDim.x) {
-    double2 sum = make_double2(0, 0);
-    sum = cadd(sum, sum_ordered(gpart + (size_t)tile * gbpt * ng + e, gbpt, ng));
-    gacc[(size_t)tile * ng + e] = cadd(gacc[(size_t)tile * ng + e], sum);
-  }
+  const int e0 = blockIdx.y * TL, e = e0 + threadIdx.x % TL;
+  const double2 sum = block_sum_rows(gpart + (size_t)tile * gbpt * ng + e0, gbpt, ng, e < ng);
+  if (threadIdx.x < TL && e < ng) gacc[(size_t)tile * ng + e] = cadd(gacc[(size_t)tile * ng + e], sum);
 }
 
 // per-lane sum of partials: out[L] = sum_q part[(tile * bpt + q) * TL + lane]
 __global__ void k_lane_sum(int ntile, int bpt, const int* tile_act, const double2* part, double2* out) {
-  int tile = blockIdx.x, lane = threadIdx.x;
+  int tile = blockIdx.x;
   if (tile >= ntile) return;
-  double2 sum = make_double2(0, 0);
-  if (tile_act[tile])
-    sum = cadd(sum, sum_ordered(part + (size_t)tile * bpt * TL + lane, bpt, TL));
-  out[tile * TL + lane] = sum;
+  const double2 sum = tile_act[tile] ? block_sum_rows(part + (size_t)tile * bpt * TL, bpt, TL) : make_double2(0, 0);
+  if (threadIdx.x < TL) out[tile * TL + threadIdx.x] = sum;
 }
 
 // scalars of reverse step k for every lane (state arrays indexed [lane][NLMAX], k 1-based):
@@ -1816,7 +1832,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
                                                   YS(q), d_part.p, npw);
         }
         ctx->prof_stop(s, ps, ASR_KERNEL_STEP, step_bytes(3), step_flops);
-        if (!a_in_step) k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+        if (!a_in_step) k_reduce_a<<<nt, RED_THREADS, 0, s>>>(bv, d_part.p, bpt, k);
         BatchView bvw = bv;
         bvw.kstep = k;
         bvw.tick = d_tick.p;
@@ -1847,7 +1863,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, AY, U, PCEB, true, U, false, nullptr, 1.0, true, Y, d_part.p, npw);
       }
       ctx->prof_stop(s, ps, ASR_KERNEL_STEP, step_bytes(2), step_flops);
-      if (!a_in_step) k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+      if (!a_in_step) k_reduce_a<<<nt, RED_THREADS, 0, s>>>(bv, d_part.p, bpt, k);
       BatchView bvw = bv;
       bvw.kstep = k;
       bvw.tick = d_tick.p;
@@ -1942,8 +1958,8 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
                                               npw);
         ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_VEC, vstream * 5.0, 0.0);
         pp = ctx->prof_start(s);
-        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d2.p);
-        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_d3.p);
+        k_lane_sum<<<nt, RED_THREADS, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d2.p);
+        k_lane_sum<<<nt, RED_THREADS, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_d3.p);
         k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 2);
         ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_SCAL, 0.0, 0.0);
         BatchView bvt = bva;
@@ -1953,13 +1969,13 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         launch_smul<ST, true, true, 2>(op, bvt, blk, wk, nullptr, d_part.p, npw, grid, s);
         ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_STEP, vstream * 6.0, sflops);
         pp = ctx->prof_start(s);
-        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d1.p);
+        k_lane_sum<<<nt, RED_THREADS, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d1.p);
         ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_SCAL, 0.0, 0.0);
         AdjVecs av{wk, T2B, nullptr, nullptr, nullptr, XS(q + 1), TS(q), nullptr, nullptr, nullptr};
         pp = ctx->prof_start(s);
         k_adj_grad<ST, false, true><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb,
                                                                    d_gpart.p, d_c[2].p);
-        k_adj_gsum<<<nt, 128, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
+        k_adj_gsum<<<dim3(nt, (ngd + TL - 1) / TL), RED_THREADS, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
         ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_GRAD, vstream * 4.0, 0.0);
         // one fused reverse level: 15 vector streams per (node, lane) (w-bar 5, step 6, parameter gradient 4); flops of its
         // one S application
@@ -1972,12 +1988,12 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         T2* ubp = UB[(k + 2) % 3];
         const int ps = ctx->prof_start(s);
         k_dot<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, ubn, XS(q + 2), d_part.p, npw);
-        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d1.p);
+        k_lane_sum<<<nt, RED_THREADS, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d1.p);
         k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 0, d_tact.p);
         k_adj_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, ubn, XS(q + 2), XS(q + 1), XS(q), d_c[0].p, d_c[1].p, WB, d_part.p, d_part2.p,
                                               npw);
-        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d2.p);
-        k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_d3.p);
+        k_lane_sum<<<nt, RED_THREADS, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_d2.p);
+        k_lane_sum<<<nt, RED_THREADS, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_d3.p);
         k_adj_scal<<<(nlp + 127) / 128, 128, 0, s>>>(S, nlp, d_lgroup.p, k, 1);
         k_adj_y<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, WB, XS(q + 1), d_c[2].p, d_c[3].p, YB, k > 1 ? ubp : nullptr, npw);
         // A ybar (unit scale) and t2bar = S R_d ybar (the general operator: also h ybar, O h ybar, S D O h ybar)
@@ -1997,7 +2013,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
           k_adj_grad<ST, true><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb, d_gpart.p);
         else
           k_adj_grad<ST, false><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb, d_gpart.p);
-        k_adj_gsum<<<nt, 128, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
+        k_adj_gsum<<<dim3(nt, (ngd + TL - 1) / TL), RED_THREADS, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
         ASR_CUDA(cudaMemsetAsync(ubn, 0, cpy, s));   // becomes ubar_{k-2}
         // one reverse level: 26 vector streams per (node, lane) over its kernels (dot 2, w-bar 5, y-bar 4, S application
         // 2, combine 3, u-bar 5, parameter gradient 4, clear 1); flops of its one S application
@@ -2128,13 +2144,13 @@ __global__ void k_ed3_reduce_a(BatchView bv, const double2* part_a, const double
                                double2* fprev, const double* tnorm) {
   int tile = blockIdx.x, lane = threadIdx.x;
   if (tile >= bv.ntile || !bv.tile_act[tile]) return;
+  const double2 a = block_sum_rows(part_a + (size_t)tile * bpt * TL, bpt, TL);
+  const double2 c = block_sum_rows(part_c + (size_t)tile * bpt * TL, bpt, TL);
+  if (lane >= TL) return;
   int L = tile * TL + lane;
   int grp = bv.lane_group[L];
   bv.lane_wact[L] = 0;
   if (grp < 0 || !bv.lane_act[L]) return;
-  double2 a = make_double2(0, 0), c = make_double2(0, 0);
-  a = cadd(a, sum_ordered(part_a + (size_t)tile * bpt * TL + lane, bpt, TL));
-  c = cadd(c, sum_ordered(part_c + (size_t)tile * bpt * TL + lane, bpt, TL));
   bv.acur[L] = a;
   bv.acoef[(size_t)L * NLMAX + k - 1] = a;
   ccoef[(size_t)L * NLMAX + k - 1] = c;
@@ -2360,8 +2376,8 @@ int run_ed3_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
     ASR_TRY(apply_hp(bv, grid, V[1].p, T1));
     if (project) k_project<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, T1, npw);
     k_ed3_dots<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, T1, d_oc.p, d_part.p, d_part2.p, npw);
-    k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_sv.p);
-    k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_sa.p);
+    k_lane_sum<<<nt, RED_THREADS, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_sv.p);
+    k_lane_sum<<<nt, RED_THREADS, 0, s>>>(nt, bpt, d_tact.p, d_part2.p, d_sa.p);
     std::vector<double2> hsv(nlp), hsa(nlp);
     ASR_CUDA(cudaMemcpyAsync(hsv.data(), d_sv.p, nlp * sizeof(double2), cudaMemcpyDeviceToHost, s));
     ASR_CUDA(cudaMemcpyAsync(hsa.data(), d_sa.p, nlp * sizeof(double2), cudaMemcpyDeviceToHost, s));
@@ -2390,9 +2406,9 @@ int run_ed3_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
       k_ed3_t3<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, U, T1, T3, npw);                  // t3 = u u - Qt t1
       apply_SD<ST>(op, bv, dunif, T3, TMP, SA, d_part.p, npw, grid, s);               // S d t3
       k_ed3_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, U, T1, T3, SA, TV, Y, d_part.p, d_part2.p, npw);
-      k_ed3_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, d_part2.p, bpt, k, d_c.p, d_fprev.p, d_tn.p);
+      k_ed3_reduce_a<<<nt, RED_THREADS, 0, s>>>(bv, d_part.p, d_part2.p, bpt, k, d_c.p, d_fprev.p, d_tn.p);
       k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, Y, U, UP, d_part.p, npw);
-      k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
+      k_reduce_b<<<nt, RED_THREADS, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
     }
     ASR_CUDA(cudaGetLastError());
     ctx->launches += 8 + (int64_t)kmax * (dunif ? 8 : 10);
@@ -2478,10 +2494,10 @@ __global__ void k_epi_start(BatchView bv, const typename St2<ST>::T* __restrict_
 __global__ void k_epi_store_c(BatchView bv, const double2* part, int bpt, int k, double2* ccoef) {
   int tile = blockIdx.x, lane = threadIdx.x;
   if (tile >= bv.ntile || !bv.tile_act[tile]) return;
+  const double2 c = block_sum_rows(part + (size_t)tile * bpt * TL, bpt, TL);
+  if (lane >= TL) return;
   int L = tile * TL + lane;
   if (bv.lane_group[L] < 0 || !bv.lane_act[L]) return;
-  double2 c = make_double2(0, 0);
-  c = cadd(c, sum_ordered(part + (size_t)tile * bpt * TL + lane, bpt, TL));
   ccoef[(size_t)L * NLMAX + k - 1] = cmul(c, bv.su[L]);
 }
 
@@ -2591,7 +2607,7 @@ int run_epi_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
     k_combine<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, SA, W1, E3_G, false, W1, false, nullptr, 1.0, false, W2, d_part.p, npw);
     if (project) k_project<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, W2, npw);
     k_dot<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, W2, W2, d_part.p, npw);
-    k_lane_sum<<<nt, TL, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_sv.p);
+    k_lane_sum<<<nt, RED_THREADS, 0, s>>>(nt, bpt, d_tact.p, d_part.p, d_sv.p);
     std::vector<double2> hsv(nlp);
     ASR_CUDA(cudaMemcpyAsync(hsv.data(), d_sv.p, nlp * sizeof(double2), cudaMemcpyDeviceToHost, s));
     ASR_CUDA(cudaStreamSynchronize(s));
@@ -2611,11 +2627,11 @@ int run_epi_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
       T2* UP = V[(k + 2) % 3].p;
       T2* Y = V[(k + 1) % 3].p;
       k_dot<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, TV, U, d_part2.p, npw);
-      k_epi_store_c<<<nt, TL, 0, s>>>(bv, d_part2.p, bpt, k, d_c.p);
+      k_epi_store_c<<<nt, RED_THREADS, 0, s>>>(bv, d_part2.p, bpt, k, d_c.p);
       ASR_TRY(step_apply<ST>(ctx, op, bv, fused, any_o, dunif, U, Y, W1, W2, W3, W4, d_part.p, npw, grid));
-      k_reduce_a<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k);
+      k_reduce_a<<<nt, RED_THREADS, 0, s>>>(bv, d_part.p, bpt, k);
       k_lanczos_w<ST><<<grid, WPB * TL, 0, s>>>(ov, bv, Y, U, UP, d_part.p, npw);
-      k_reduce_b<<<nt, TL, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
+      k_reduce_b<<<nt, RED_THREADS, 0, s>>>(bv, d_part.p, bpt, k, 1.0e-12);
     }
     ASR_CUDA(cudaGetLastError());
     ctx->launches += 8 + (int64_t)kmax * (5 + (fused ? 1 : (any_o ? 7 : (dunif ? 2 : 3))));

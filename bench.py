@@ -80,6 +80,9 @@ def parse():
                         "EPI), 0: none, or a comma list of leg names")
     p.add_argument("--lanes", type=int, default=0,
                    help="1: run the multi-GPU step (task split, lane chains, all-reduce of the shares) also on one GPU")
+    p.add_argument("--adj-groups", type=int, default=0, help="adjoint leg: the first N chain groups (0: all 54)")
+    p.add_argument("--adj-energies", type=int, default=48, help="adjoint leg: the first N of the 48 contour energies")
+    p.add_argument("--adj-depth", type=int, default=0, help="adjoint leg: every chain this deep (0: the drawn depths)")
     p.add_argument("--link", default="auto", choices=["auto", "general", "fixed"],
                    help="step-kernel link gathers: the autotuner's choice (auto; general without --autotune), or pinned")
     return p.parse_args()
@@ -589,8 +592,12 @@ def adjoint_leg(args, A, op, specs, groups, z_all, stream):
     """Forward plus reverse sweep of all 54 groups over the 48 contour energies (seeds: the contour charge weights), in
     FP64 and in the mixed form, against the forward alone on the same energies; the mixed gradient's error against FP64."""
     import torch
+    if args.adj_groups > 0 or args.adj_depth > 0:   # a smaller case of the same operator (profiling captures)
+        groups = [dict(g, nlev=args.adj_depth or g["nlev"]) for g in groups[: args.adj_groups or len(groups)]]
+        specs = specs_of(groups)
     depth = np.array([g["nlev"] for g in groups])
     zc, wc = contour_weights(z_all)
+    zc, wc = zc[: args.adj_energies], wc[: args.adj_energies]
     w = np.repeat(wc[:, None], len(specs), axis=1)
     steps_adj = int(depth.sum()) * zc.shape[0]
     out, grads = {}, {}
