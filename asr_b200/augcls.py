@@ -65,7 +65,8 @@ class Context:
                     "adj_scal": 7}
 
     def hold_workspace(self, on: bool):
-        """Keep the adjoint's device vector memory in this context between calls (on) or free it (off, the default)."""
+        """Keep the device vector memory of the chain runs and the adjoint in this context between calls (on) or free it
+        (off, the default)."""
         check(lib().asr_ctx_hold_workspace(self.h, int(bool(on))))
 
     def profile(self, on: bool):

@@ -1032,6 +1032,28 @@ int step_apply(asr_ctx* ctx, asr_op* op, const BatchView& bv, bool fused, bool a
   return ASR_OK;
 }
 
+// The vector memory of a batched run as one slab: the context's held slab (asr_ctx_hold_workspace; grown when too small
+// and kept after the call), else `own`, allocated here and freed with the caller's scope.  Calls on one context run in
+// its stream order and return after their last kernel, so a held slab is never in use by two calls.
+int vector_slab(asr_ctx* ctx, size_t bytes, Dev<unsigned char>& own, void** base) {
+  if (ctx->ws_hold) {
+    if (ctx->ws_bytes < bytes) {
+      ctx->ws_release();
+      if (cudaMalloc(&ctx->ws, bytes) != cudaSuccess) {
+        ctx->ws = nullptr;
+        set_error("chains: device allocation of %zu bytes failed", bytes);
+        return ASR_ENOMEM;
+      }
+      ctx->ws_bytes = bytes;
+    }
+    *base = ctx->ws;
+    return ASR_OK;
+  }
+  ASR_TRY(own.alloc(bytes));
+  *base = own.p;
+  return ASR_OK;
+}
+
 template <typename ST>
 int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, const std::vector<double>& gblob,
                 const GroupLayout& GL, const std::vector<int>& lane_group, const double2* d_lane_z, int nlane,
@@ -1065,6 +1087,7 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   const int nvec = 3 + (fused ? 0 : (any_o ? 4 : 2));
   size_t freeb = 0, totb = 0;
   cudaMemGetInfo(&freeb, &totb);
+  freeb += ctx->ws_bytes;   // a held slab is this call's to reuse
   // 32-lane tiles per batch: larger batches amortise the per-level reductions and launch gaps; the caller's shape, else
   // the operator's autotuned one, else the measured defaults of the fcc ternary workload (FP64 16 tiles, FP32 8, 4 nodes
   // per warp)
@@ -1095,8 +1118,13 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
   ASR_TRY(d_a.alloc((size_t)nlp * NLMAX)); ASR_TRY(d_b.alloc((size_t)nlp * NLMAX));
   ASR_TRY(d_gprev.alloc(nlp)); ASR_TRY(d_acur.alloc(nlp)); ASR_TRY(d_bprev.alloc(nlp)); ASR_TRY(d_su.alloc(nlp));
   ASR_TRY(d_sup.alloc(nlp)); ASR_TRY(d_part.alloc((size_t)tpb * bpt * TL)); ASR_TRY(d_z.alloc(nlp));
-  Dev<T2> V[7];
-  for (int q = 0; q < nvec; ++q) ASR_TRY(V[q].alloc((size_t)tpb * nn * 9 * TL));
+  const size_t vlen = (size_t)tpb * nn * 9 * TL;
+  Dev<unsigned char> own;
+  T2* vbase = nullptr;
+  ASR_TRY(vector_slab(ctx, (size_t)nvec * vlen * sizeof(T2), own, (void**)&vbase));
+  struct VecRef { T2* p; };
+  VecRef V[7];
+  for (int q = 0; q < nvec; ++q) V[q].p = vbase + (size_t)q * vlen;
   Dev<double2> d_cpr;
   ProjView PV{0, 1, nlevmax, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   if (proj) {
@@ -1709,27 +1737,11 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   ASR_TRY(d_sn.alloc(nlp)); ASR_TRY(d_sk.alloc(nlp)); ASR_TRY(d_sp.alloc(nlp));
   for (int q = 0; q < 6; ++q) ASR_TRY(d_c[q].alloc(nlp));
   ASR_TRY(d_d1.alloc(nlp)); ASR_TRY(d_d2.alloc(nlp)); ASR_TRY(d_d3.alloc(nlp)); ASR_TRY(d_one.alloc(nlp));
-  // the vectors: one slab, from the context when it holds one large enough (asr_ctx_hold_workspace), else allocated
-  // here and freed on return
+  // the vectors: one slab (the context's held one, or allocated here and freed on return)
   const size_t vlen = (size_t)tpb * nn * 9 * TL;
-  const size_t slab = (size_t)nvec * vlen * sizeof(T2);
   Dev<unsigned char> own;
   T2* vbase = nullptr;
-  if (ctx->ws_hold) {
-    if (ctx->ws_bytes < slab) {
-      ctx->ws_release();
-      if (cudaMalloc(&ctx->ws, slab) != cudaSuccess) {
-        ctx->ws = nullptr;
-        set_error("adjoint: device allocation of %zu bytes failed", slab);
-        return ASR_ENOMEM;
-      }
-      ctx->ws_bytes = slab;
-    }
-    vbase = (T2*)ctx->ws;
-  } else {
-    ASR_TRY(own.alloc(slab));
-    vbase = (T2*)own.p;
-  }
+  ASR_TRY(vector_slab(ctx, (size_t)nvec * vlen * sizeof(T2), own, (void**)&vbase));
   struct VecRef { T2* p; };
   std::vector<VecRef> V(nvec);
   for (int q = 0; q < nvec; ++q) V[q].p = vbase + (size_t)q * vlen;

@@ -69,10 +69,11 @@ enum {
   ASR_KERNEL_KINDS = 8
 };
 int asr_ctx_profile(asr_ctx* ctx, int on);
-/* on = 1: the adjoint (asr_chains_adjoint, asr_chains_adjoint_ext) keeps its device vector memory (at most half of the
- * device memory free when it is first needed) in the context after it returns and reuses it on the next call, instead of
- * allocating and freeing it per call; on = 0 (the default) frees it.  For loops that take many gradients on one
- * operator.  No counterpart in the reference (which has no derivatives). */
+/* on = 1: the batched chain runs (asr_chains_run and its lane and device forms) and the adjoint (asr_chains_adjoint,
+ * asr_chains_adjoint_ext) keep their device vector memory (one slab, at most half of the device memory free when it is
+ * first needed, grown when a later call needs more) in the context after they return and reuse it on the next call,
+ * instead of allocating and freeing it per call; on = 0 (the default) frees it.  For loops that run many chain sets or
+ * gradients on one operator.  No counterpart in the reference (whose arrays are allocated per call). */
 int asr_ctx_hold_workspace(asr_ctx* ctx, int on);
 int asr_ctx_kernel_stats(asr_ctx* ctx, double* ms, int64_t* launches, double* bytes, double* flops);
 int asr_ctx_kernel_stats_kind(asr_ctx* ctx, int kind, double* ms, int64_t* launches, double* bytes, double* flops);

@@ -93,3 +93,28 @@ def test_dos_final_matches_oracle():
     assert edos.shape == (ndos, 3, 3, 2)
     assert np.max(np.abs(edos - edos_o)) <= 1e-8 * np.max(np.abs(edos_o))
     assert np.min(edos_o) > -1e-10      # a DOS: non-negative
+
+
+def test_held_workspace_forward_gives_the_same_bits():
+    """asr_ctx_hold_workspace on the batched chain runs: the kept vector slab, reused by the next calls, gives the bits of
+    the allocating call."""
+    case = S.cubic_case("bcc", 3, 2, [0.5, 0.5], seed=0, group="d4h")
+    fl = np.ones(case["graph"].n, np.int32)
+    fl[0] = 0
+    op = A.build_augcls_operator(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, 2, maxrank=1,
+                                 flippable=fl)
+    specs = []
+    for cen in (1, 2):
+        ed = S.edc_params(S.draw_species(2, cen), cen)
+        for l0 in (1, 3, 5):
+            specs.append(A.ChainSpec(c=ed["c"], d=ed["d"], o=ed["o"], e=ed["e"], pa=ed["pa"], pb=ed["pb"], frozen_sp=cen,
+                                     start_orb=l0, nlev=14))
+    z = np.linspace(-0.6, 0.4, 40) + 0.02j
+    ref = A.chains_run(op, specs, z, "edc", 0.0, "hull", "fp64")["g"]
+    op.ctx.hold_workspace(True)
+    try:
+        for zz in (z, z, z[:7]):
+            g = A.chains_run(op, specs, zz, "edc", 0.0, "hull", "fp64")["g"]
+            assert np.array_equal(g, ref[: zz.size])
+    finally:
+        op.ctx.hold_workspace(False)
