@@ -7,8 +7,8 @@ differentiated with respect to the species parameters (c_l, d_l, Delta_l).
 
 * ``ChainGreens`` -- G(group, energy) of a batch of chain groups as a function of the groups' parameter arrays
   (c, d, o, e, pa, pb per orbital and species).  Forward: ``asr_chains_run``; backward: ``asr_chains_adjoint_ext``, the
-  device adjoint (Lanczos vectors kept every sqrt(depth) levels and recomputed, reverse sweep through the recurrence,
-  reverse mode of the continued fraction).
+  device adjoint (the Lanczos vectors of every level kept where they fit, else every sqrt(depth) levels and
+  recomputed; reverse sweep through the recurrence; reverse mode of the continued fraction).
 * ``edc_group_arrays``, ``edc_group_o`` -- the map of ``edc_setup`` from species parameters to a group's arrays, in
   torch.
 * ``contour_moments`` -- M_k = -(1/pi) Im sum_j w_j (z_j - E_nu)^k G_j.
@@ -43,8 +43,8 @@ class ChainGreens(torch.autograd.Function):
 
     Inputs: c, d, e, pa, pb -- (ngroup, nsp, 9) float64 tensors (each group's (9, nsp) arrays); o -- the same shape or
     None (o = 0); op -- the operator; groups -- [(frozen_sp, start_orb, nlev)] per group; z (nz) complex energies; tail
-    ('none' | 'hull' | 'bp' | 'avg2'); precision ('fp64' | 'fp32'); project; stride (checkpoint spacing, 0: sqrt(depth));
-    depth_tol (> 0: the depth test of src/asr_edc.f90:121-127, the derivative taken at the depth each chain stopped at).
+    ('none' | 'hull' | 'bp' | 'avg2'); precision ('fp64' | 'fp32'); project; stride (checkpoint spacing; 0: every level
+    where it fits, else sqrt(depth)); depth_tol (> 0: the depth test of src/asr_edc.f90:121-127, the derivative taken at the depth each chain stopped at).
 
     The backward pass gives d(real loss)/dpar = Re(sum conj(dL/dG) dG/dpar): the seeds of the adjoint are the conjugated
     output gradients.  e and pb enter the operator the same way and share one derivative (and c with them when o = 0)."""

@@ -246,8 +246,9 @@ int asr_ed3_blocks(asr_ctx* ctx, asr_op* op, const asr_ed3_group* groups, int ng
  * kind 0 the diagonal c (the same derivative applies to e and pb, which enter only as c + e + pb when o = 0), kind 1 d,
  * kind 2 pa.  w(nz, ngroup) complex seeds.  The entries are symmetrised over the orbits of the orbitals under the
  * operator's point group (the group-reduced operator represents only parameters constant on each orbit): derivatives
- * along every group-invariant direction (per l, per orbit) are exact.  The Lanczos vectors are kept every `stride` levels
- * (0: ceil(sqrt(depth))) and recomputed in between.  Every tail (none, hull, bp, avg2).  Groups with o != 0 are refused
+ * along every group-invariant direction (per l, per orbit) are exact.  stride > 0: the Lanczos vectors are kept every
+ * `stride` levels and recomputed in between; stride = 0: every level's vectors are kept when a batch of 4 tiles fits in
+ * half the free device memory (no recomputation), else every ceil(sqrt(depth)) levels.  Both give the same bits.  Every tail (none, hull, bp, avg2).  Groups with o != 0 are refused
  * (asr_chains_adjoint_ext).  No counterpart in the reference (gradients of the chain with respect to the species
  * parameters of src/asr_edc.f90:41-71). */
 int asr_chains_adjoint(asr_ctx* ctx, asr_op* op, const asr_chain_group* groups, int ngroup, const double* z, int nz,
