@@ -259,6 +259,98 @@ template <> struct Pair<float> { typedef float2 T; };
 
 constexpr int RW = 12;   // padded row of a shared-memory block (16-byte aligned pairs for FP64 and FP32)
 
+// Block products of the step kernel: acc_l += sum_lp B[l][lp] x[lp] over the nine rows of one shared-memory block, the
+// nine products of a row added in the order lp = 0 .. 8.  FP64: rows of RW doubles.  FP32: rows 2p and 2p + 1 (p < 4)
+// interleaved as {B[2p][lp], B[2p+1][lp]} pairs (18 floats, padded to 20), then row 8 alone (padded to 12); one paired
+// FMA (__ffma2_rn, each half rounded as a scalar FMA) updates one component of two rows, so the bits are those of the
+// scalar products with half their FMA instructions and no more shared-memory bytes.
+template <typename ST> struct BlockAcc;
+template <> struct BlockAcc<double> {
+  static constexpr int BLK = 9 * RW;   // elements per block
+  __device__ static void put(double* blk, int l, int lp, double v) { blk[l * RW + lp] = v; }
+  double2 a[9];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int l = 0; l < 9; ++l) a[l] = make_double2(0.0, 0.0);
+  }
+  __device__ __forceinline__ void mac(const double* __restrict__ blk, const double2* x) {
+#pragma unroll
+    for (int l = 0; l < 9; ++l) {
+      const double* row = blk + l * RW;
+#pragma unroll
+      for (int lp = 0; lp < 8; lp += 2) {
+        const double2 bb = *(const double2*)(row + lp);
+        a[l].x = fma(bb.x, x[lp].x, a[l].x);
+        a[l].y = fma(bb.x, x[lp].y, a[l].y);
+        a[l].x = fma(bb.y, x[lp + 1].x, a[l].x);
+        a[l].y = fma(bb.y, x[lp + 1].y, a[l].y);
+      }
+      a[l].x = fma(row[8], x[8].x, a[l].x);
+      a[l].y = fma(row[8], x[8].y, a[l].y);
+    }
+  }
+  __device__ __forceinline__ void out(double2* acc) const {
+#pragma unroll
+    for (int l = 0; l < 9; ++l) acc[l] = a[l];
+  }
+};
+template <> struct BlockAcc<float> {
+  static constexpr int BLK = 4 * 20 + 12;
+  __device__ static void put(float* blk, int l, int lp, double v) {
+    if (l < 8) blk[(l >> 1) * 20 + 2 * lp + (l & 1)] = (float)v;
+    else blk[80 + lp] = (float)v;
+  }
+  float2 ax[4], ay[4], a8;   // {row 2p, row 2p + 1} of the real and of the imaginary parts; row 8
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int p = 0; p < 4; ++p) { ax[p] = make_float2(0.f, 0.f); ay[p] = ax[p]; }
+    a8 = make_float2(0.f, 0.f);
+  }
+  __device__ __forceinline__ void mac(const float* __restrict__ blk, const float2* x) {
+#pragma unroll
+    for (int lp = 0; lp < 8; lp += 2) {
+      const float2 x0 = make_float2(x[lp].x, x[lp].x), y0 = make_float2(x[lp].y, x[lp].y);
+      const float2 x1 = make_float2(x[lp + 1].x, x[lp + 1].x), y1 = make_float2(x[lp + 1].y, x[lp + 1].y);
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const float4 bb = *(const float4*)(blk + p * 20 + 2 * lp);
+        ax[p] = __ffma2_rn(make_float2(bb.x, bb.y), x0, ax[p]);
+        ay[p] = __ffma2_rn(make_float2(bb.x, bb.y), y0, ay[p]);
+        ax[p] = __ffma2_rn(make_float2(bb.z, bb.w), x1, ax[p]);
+        ay[p] = __ffma2_rn(make_float2(bb.z, bb.w), y1, ay[p]);
+      }
+    }
+    {
+      const float2 x8 = make_float2(x[8].x, x[8].x), y8 = make_float2(x[8].y, x[8].y);
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const float2 bb = *(const float2*)(blk + p * 20 + 16);
+        ax[p] = __ffma2_rn(bb, x8, ax[p]);
+        ay[p] = __ffma2_rn(bb, y8, ay[p]);
+      }
+    }
+    const float* r8 = blk + 80;
+#pragma unroll
+    for (int lp = 0; lp < 8; lp += 2) {
+      const float2 bb = *(const float2*)(r8 + lp);
+      a8.x = fmaf(bb.x, x[lp].x, a8.x);
+      a8.y = fmaf(bb.x, x[lp].y, a8.y);
+      a8.x = fmaf(bb.y, x[lp + 1].x, a8.x);
+      a8.y = fmaf(bb.y, x[lp + 1].y, a8.y);
+    }
+    a8.x = fmaf(r8[8], x[8].x, a8.x);
+    a8.y = fmaf(r8[8], x[8].y, a8.y);
+  }
+  __device__ __forceinline__ void out(float2* acc) const {
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      acc[2 * p] = make_float2(ax[p].x, ay[p].x);
+      acc[2 * p + 1] = make_float2(ax[p].y, ay[p].y);
+    }
+    acc[8] = a8;
+  }
+};
+
 // packed orbital operation of the identity: permutation pi(l) = l in bits 4l..4l+3, no signs (bits 40..48)
 constexpr unsigned long long PW_IDENTITY = 0x876543210ull;
 constexpr unsigned long long PW_PERM_MASK = 0xFFFFFFFFFull;   // the nine 4-bit orbital indices
@@ -340,7 +432,7 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int ns1 = op.nslot + 1;
   ST* Bs = (ST*)smem_raw;                                                        // [ntype][ns1][9][RW]
-  unsigned long long* piw = (unsigned long long*)(smem_raw + (((size_t)op.ntype * ns1 * 9 * RW * sizeof(ST) + 15) & ~(size_t)15));
+  unsigned long long* piw = (unsigned long long*)(smem_raw + (((size_t)op.ntype * ns1 * BlockAcc<ST>::BLK * sizeof(ST) + 15) & ~(size_t)15));
   NodeIter it;
   int bpt;
   bool live = node_iter(bv, npw, it, bpt);
@@ -360,7 +452,7 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
       double v = (double)blocks[q];
       if (FUSE_D && dd) v *= dd[lp];
       if (FINAL && dd) v *= dd[l];
-      Bs[((size_t)tk * 9 + l) * RW + lp] = (ST)v;
+      BlockAcc<ST>::put(Bs + (size_t)tk * BlockAcc<ST>::BLK, l, lp, v);
     }
     for (int g = threadIdx.x; g < op.nop; g += blockDim.x) {
       unsigned long long w = 0ull;
@@ -377,25 +469,14 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
   for (int qn = 0; qn < npw; ++qn) {
     int i = it.first + w + WPB * qn;
     if (i >= bv.nn) break;
-    const ST* B = Bs + (size_t)op.typ[i] * ns1 * 9 * RW;
-    T2 acc[9];
-    for (int l = 0; l < 9; ++l) { acc[l].x = 0; acc[l].y = 0; }
+    const ST* B = Bs + (size_t)op.typ[i] * ns1 * BlockAcc<ST>::BLK;
+    BlockAcc<ST> A;
+    A.zero();
     {   // on-site block
       const T2* src = in + vix(it.tile, bv.nn, i, 0) + lane;
       T2 v[9];
       for (int l2 = 0; l2 < 9; ++l2) v[l2] = src[l2 * TL];
-      for (int l = 0; l < 9; ++l) {
-        const ST* row = B + l * RW;
-        for (int lp = 0; lp < 8; lp += 2) {
-          P2 bb = *(const P2*)(row + lp);
-          acc[l].x = fma_(bb.x, v[lp].x, acc[l].x);
-          acc[l].y = fma_(bb.x, v[lp].y, acc[l].y);
-          acc[l].x = fma_(bb.y, v[lp + 1].x, acc[l].x);
-          acc[l].y = fma_(bb.y, v[lp + 1].y, acc[l].y);
-        }
-        acc[l].x = fma_(row[8], v[8].x, acc[l].x);
-        acc[l].y = fma_(row[8], v[8].y, acc[l].y);
-      }
+      A.mac(B, v);
     }
     // the node's links, one slot per lane, read once with a coalesced load and broadcast by shuffles: the row gathers
     // then wait on one global latency per slot instead of two dependent ones (link, then row)
@@ -426,20 +507,10 @@ __global__ void __launch_bounds__(WPB * TL) k_smul(OpView op, BatchView bv, cons
           v[lp] = flip_if(src[p * TL], (uint32_t)((pw >> (40 + lp)) & 1ull));
         }
       }
-      const ST* Bk = B + (size_t)(k + 1) * 9 * RW;
-      for (int l = 0; l < 9; ++l) {
-        const ST* row = Bk + l * RW;
-        for (int lp = 0; lp < 8; lp += 2) {
-          P2 bb = *(const P2*)(row + lp);
-          acc[l].x = fma_(bb.x, v[lp].x, acc[l].x);
-          acc[l].y = fma_(bb.x, v[lp].y, acc[l].y);
-          acc[l].x = fma_(bb.y, v[lp + 1].x, acc[l].x);
-          acc[l].y = fma_(bb.y, v[lp + 1].y, acc[l].y);
-        }
-        acc[l].x = fma_(row[8], v[8].x, acc[l].x);
-        acc[l].y = fma_(row[8], v[8].y, acc[l].y);
-      }
+      A.mac(B + (size_t)(k + 1) * BlockAcc<ST>::BLK, v);
     }
+    T2 acc[9];
+    A.out(acc);
     smul_node_out<ST, FINAL, EPI>(op, bv, it.tile, i, lane, L, grp, gflags, gfrozen, piw, in, out, acc, dot);
   }
   if (FINAL) {
