@@ -1353,7 +1353,7 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
 // and dR_p / dpar(l, s) is the random operator with the weights mt(own, k', s, class) (local_weights,
 // src/asr_augcls.f90:362-377).  The Lanczos vectors are recomputed per segment from checkpoints every `stride` levels.
 
-constexpr int MAXSP = 8;        // species held in registers by the gradient kernel
+constexpr int MAXSP = 8;        // species of the gradient kernel's register accumulators (at most)
 constexpr int GPW = 9;          // warps per gradient block: one per orbital
 
 // per-lane weighted dot: part = sum_i norb_i a_i . b_i (raw, unscaled vectors)
@@ -1479,7 +1479,17 @@ struct AdjVecs {   // per level: node side (yb: ybar; tb = S D ybar; hb = h ybar
   const void *yb, *tb, *hb, *rb, *qb;
   const void *xk, *tk, *hk, *rk, *qk;
 };
-template <typename ST, bool GEN, bool WY = false>
+// a[sp] += v with sp known only at run time: an unrolled select over the NS accumulators keeps them in registers (an
+// indexed array would live in local memory); the accumulator sees the same additions in the same order
+template <int NS>
+__device__ __forceinline__ void add_sp(double2 (&a)[NS], int sp, double2 v) {
+#pragma unroll
+  for (int q = 0; q < NS; ++q)
+    if (q == sp) a[q] = cadd(a[q], v);
+}
+
+// NS: a compile-time bound on the operator's species count (nsp <= NS), which sizes the register accumulators
+template <typename ST, bool GEN, bool WY = false, int NS = MAXSP>
 __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, const double* mt, const int* spc, int ldspc,
                                                        AdjVecs V, const double2* sk, int nodes_per_block, double2* gpart,
                                                        const double2* cy = nullptr) {
@@ -1493,8 +1503,9 @@ __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, 
   const int L = tile * TL + lane;
   const int grp = bv.tile_group[tile];
   const int nsp = op.nsp, nsm = op.nsmax;
-  double2 gc[MAXSP], gd[MAXSP], ge[MAXSP], go[MAXSP];   // pa = z e-kind
-  for (int q = 0; q < MAXSP; ++q) { gc[q] = make_double2(0, 0); gd[q] = gc[q]; ge[q] = gc[q]; go[q] = gc[q]; }
+  double2 gc[NS], gd[NS], ge[NS], go[NS];   // pa = z e-kind
+#pragma unroll
+  for (int q = 0; q < NS; ++q) { gc[q] = make_double2(0, 0); gd[q] = gc[q]; ge[q] = gc[q]; go[q] = gc[q]; }
   const bool live = bv.lane_group[L] >= 0 && grp >= 0;
   double2 z = make_double2(0, 0);
   if (live) {
@@ -1539,29 +1550,32 @@ __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, 
         }
         qe = cscale(qe, nb); qc = cscale(qc, nb); qd = cscale(qd, nb); qo = cscale(qo, nb);
         if (fs > 0) {
-          ge[fs - 1] = cadd(ge[fs - 1], qe);
-          gd[fs - 1] = cadd(gd[fs - 1], qd);
-          if (GEN) { gc[fs - 1] = cadd(gc[fs - 1], qc); go[fs - 1] = cadd(go[fs - 1], qo); }
+          add_sp<NS>(ge, fs - 1, qe);
+          add_sp<NS>(gd, fs - 1, qd);
+          if (GEN) { add_sp<NS>(gc, fs - 1, qc); add_sp<NS>(go, fs - 1, qo); }
           continue;
         }
         for (int sidx = 0; sidx < nk; ++sidx) {
           double m = mt[own + nsm * (kp + nsm * (sidx + (size_t)nsm * kap))];
           if (m == 0.0) continue;
           int sp = spc[sidx + ldspc * kap] - 1;
-          ge[sp] = cadd(ge[sp], cscale(qe, m));
-          gd[sp] = cadd(gd[sp], cscale(qd, m));
-          if (GEN) { gc[sp] = cadd(gc[sp], cscale(qc, m)); go[sp] = cadd(go[sp], cscale(qo, m)); }
+          add_sp<NS>(ge, sp, cscale(qe, m));
+          add_sp<NS>(gd, sp, cscale(qd, m));
+          if (GEN) { add_sp<NS>(gc, sp, cscale(qc, m)); add_sp<NS>(go, sp, cscale(qo, m)); }
         }
       }
     }
   }
   // sum over the 32 lanes (one warp = one orbital), fixed order; pa = z e per lane before the sum
-  double2 gpa[MAXSP];
-  for (int q = 0; q < nsp; ++q) {
+  double2 gpa[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
     gpa[q] = cmul(z, ge[q]);
     if (!GEN) gc[q] = ge[q];   // o = 0: c enters as e does
   }
-  for (int q = 0; q < nsp; ++q) {
+#pragma unroll
+  for (int q = 0; q < NS; ++q) {
+    if (q >= nsp) break;
     for (int off = 16; off > 0; off >>= 1) {
       gc[q].x += __shfl_xor_sync(0xffffffffu, gc[q].x, off);
       gc[q].y += __shfl_xor_sync(0xffffffffu, gc[q].y, off);
@@ -1577,7 +1591,9 @@ __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, 
   }
   if (lane == 0) {
     double2* out = gpart + ((size_t)(tile * gbpt + blk) * NGK) * 9 * nsp;
-    for (int q = 0; q < nsp; ++q) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) {
+      if (q >= nsp) break;
       out[(0 * 9 + l) * nsp + q] = gc[q];
       out[(1 * 9 + l) * nsp + q] = gd[q];
       out[(2 * 9 + l) * nsp + q] = gpa[q];
@@ -1585,6 +1601,19 @@ __global__ void __launch_bounds__(GPW * TL) k_adj_grad(OpView op, BatchView bv, 
       out[(4 * 9 + l) * nsp + q] = ge[q];
     }
   }
+}
+
+// k_adj_grad with the register accumulators sized for the operator's species count
+template <typename ST, bool GEN, bool WY = false>
+void launch_adj_grad(int nsp, unsigned grid, cudaStream_t s, const OpView& ov, const BatchView& bv, const double* mt,
+                     const int* spc, int ldspc, const AdjVecs& av, const double2* sk, int gnpb, double2* gpart,
+                     const double2* cy = nullptr) {
+  if (nsp <= 3)
+    k_adj_grad<ST, GEN, WY, 3><<<grid, GPW * TL, 0, s>>>(ov, bv, mt, spc, ldspc, av, sk, gnpb, gpart, cy);
+  else if (nsp <= 5)
+    k_adj_grad<ST, GEN, WY, 5><<<grid, GPW * TL, 0, s>>>(ov, bv, mt, spc, ldspc, av, sk, gnpb, gpart, cy);
+  else
+    k_adj_grad<ST, GEN, WY, MAXSP><<<grid, GPW * TL, 0, s>>>(ov, bv, mt, spc, ldspc, av, sk, gnpb, gpart, cy);
 }
 
 // gacc[tile][NGK][9][nsp] += sum over the blocks of the step's partials (fixed order)
@@ -2056,8 +2085,8 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_SCAL, 0.0, 0.0);
         AdjVecs av{wk, T2B, nullptr, nullptr, nullptr, XS(q + 1), TS(q), nullptr, nullptr, nullptr};
         pp = ctx->prof_start(s);
-        k_adj_grad<ST, false, true><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb,
-                                                                   d_gpart.p, d_c[2].p);
+        launch_adj_grad<ST, false, true>(nsp, nt * gbpt, s, ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb, d_gpart.p,
+                                         d_c[2].p);
         k_adj_gsum<<<dim3(nt, (ngd + TL - 1) / TL), RED_THREADS, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
         ctx->prof_stop(s, pp, ASR_KERNEL_ADJ_GRAD, vstream * 4.0, 0.0);
         // one fused reverse level: 15 vector streams per (node, lane) (w-bar 5, step 6, parameter gradient 4); flops of its
@@ -2093,9 +2122,9 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
         k_adj_u<ST><<<grid, WPB * TL, 0, s>>>(ov, bva, AY, YS(q), WB, d_c[4].p, d_c[5].p, ubk, npw);
         AdjVecs av{YB, T2B, HB, RB, QB, XS(q + 1), TS(q), HS(q), RS(q), QS(q)};
         if (gen)
-          k_adj_grad<ST, true><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb, d_gpart.p);
+          launch_adj_grad<ST, true>(nsp, nt * gbpt, s, ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb, d_gpart.p);
         else
-          k_adj_grad<ST, false><<<nt * gbpt, GPW * TL, 0, s>>>(ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb, d_gpart.p);
+          launch_adj_grad<ST, false>(nsp, nt * gbpt, s, ov, bva, d_mt.p, d_spc.p, op->ldspc, av, d_sk.p, gnpb, d_gpart.p);
         k_adj_gsum<<<dim3(nt, (ngd + TL - 1) / TL), RED_THREADS, 0, s>>>(nt, gbpt, ngd, d_tact.p, d_gpart.p, d_gacc.p);
         ASR_CUDA(cudaMemsetAsync(ubn, 0, cpy, s));   // becomes ubar_{k-2}
         // one reverse level: 26 vector streams per (node, lane) over its kernels (dot 2, w-bar 5, y-bar 4, S application
