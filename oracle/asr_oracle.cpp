@@ -525,11 +525,20 @@ static void local_weights(const Op& op, const double* par, std::vector<double>& 
 }
 #define WT(w, lam, k, kk, kap) (w)[(lam) + 9 * ((k) + (size_t)nsm * ((kk) + (size_t)nsm * (kap)))]
 
+// Threads of the node loops of one operator application, for large parity cases in the tests: 1 unless the caller sets
+// more, and always serial inside an enclosing parallel region (chain_greens' tasks).  Every output node is computed by
+// one thread with the same operations in the same order, so the results are the same bits for every thread count.
+static int g_apply_threads = 1;
+extern "C" void orc_set_apply_threads(int n) { g_apply_threads = n < 1 ? 1 : n; }
+extern "C" int orc_apply_threads() { return g_apply_threads; }
+#define ORC_NODE_LOOP _Pragma("omp parallel for schedule(static) num_threads(g_apply_threads) if (g_apply_threads > 1 && !omp_in_parallel())")
+
 // apply_rand src/asr_augcls.f90:380-403 (amplitude coordinates)
 static void apply_rand(const Op& op, const double* par, const double* x, double* w) {
   std::vector<double> wt;
   local_weights(op, par, wt);
   const int nsm = op.nsmax;
+  ORC_NODE_LOOP
   for (int i = 0; i < op.nn; ++i) {
     const double* xi = x + 9 * (size_t)i;
     double* wi = w + 9 * (size_t)i;
@@ -557,6 +566,7 @@ static void apply_rand(const Op& op, const double* par, const double* x, double*
 static void apply_h(const Op& op, const double* x, double* hx, double* t1, double* t2, double* t3) {
   apply_rand(op, op.d.data(), x, t1);
   const int ns = op.nslot, nop = op.nop;
+  ORC_NODE_LOOP
   for (int i = 0; i < op.nn; ++i) {
     int t = op.stype[op.site[i] - 1] - 1;
     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -578,8 +588,9 @@ static void apply_h(const Op& op, const double* x, double* hx, double* t1, doubl
   }
   apply_rand(op, op.d.data(), t2, t3);
   apply_rand(op, op.c.data(), x, hx);
-  size_t nd = 9 * (size_t)op.nn;
-  for (size_t q = 0; q < nd; ++q) hx[q] = hx[q] + t3[q];
+  const long nd = 9 * (long)op.nn;
+  ORC_NODE_LOOP
+  for (long q = 0; q < nd; ++q) hx[q] = hx[q] + t3[q];
 }
 
 // augcls_apply src/asr_augcls.f90:275-297: y = H x in normalised coordinates, H = E_nu + h - h o h
@@ -587,12 +598,14 @@ struct Work { std::vector<double> w[8]; void init(size_t n) { for (auto& v : w) 
 static void augcls_apply(const Op& op, Work& wk, const double* x, double* y) {
   size_t nd = 9 * (size_t)op.nn;
   if (wk.w[0].size() != nd) wk.init(nd);
+  ORC_NODE_LOOP
   for (int i = 0; i < op.nn; ++i)
     for (int l = 0; l < 9; ++l) wk.w[6][9 * (size_t)i + l] = x[9 * (size_t)i + l] / op.sq[i];
   apply_h(op, wk.w[6].data(), wk.w[0].data(), wk.w[3].data(), wk.w[4].data(), wk.w[5].data());
   apply_rand(op, op.o.data(), wk.w[0].data(), wk.w[1].data());
   apply_h(op, wk.w[1].data(), wk.w[2].data(), wk.w[3].data(), wk.w[4].data(), wk.w[5].data());
   apply_rand(op, op.e.data(), wk.w[6].data(), wk.w[7].data());
+  ORC_NODE_LOOP
   for (int i = 0; i < op.nn; ++i)
     for (int l = 0; l < 9; ++l) {
       size_t q = 9 * (size_t)i + l;

@@ -65,6 +65,8 @@ def lib():
         L.orc_sqrt_tail.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, _d]
         L.orc_periodic_g.argtypes = [C.c_double, C.c_double, _d, _d, C.c_int, _d]
         L.orc_lanczos.argtypes = [C.c_void_p, _d, C.c_int, C.c_double, _d, _d, _i]
+        L.orc_set_apply_threads.argtypes = [C.c_int]
+        L.orc_apply_threads.restype = C.c_int
         L.orc_edc_green.argtypes = [C.c_void_p, C.c_int, _d, _d, _d, C.c_double, C.c_double, C.c_int, C.c_int, C.c_double,
                                     C.c_int, C.c_int, _d, _d, _d, _i, _l]
         L.orc_edc_green_blk.argtypes = [C.c_void_p, C.c_int, _d, _d, _d, _d, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int,
@@ -87,6 +89,24 @@ def lib():
         L.orc_kpm_dos.argtypes = [_d, C.c_int, C.c_double, C.c_double, _d, C.c_int, _d]
         _LIB = L
     return _LIB
+
+
+class apply_threads:
+    """Context manager: the node loops of the oracle's operator applications on n threads (all host threads by default)
+    inside the block, serial again after it.  Every node is computed by one thread with the same operations, so the
+    results are the same bits as on one thread; only single-chain oracle calls use it (chain_greens' tasks stay serial)."""
+
+    def __init__(self, n: int = 0):
+        self.n = n if n > 0 else (os.cpu_count() or 1)
+
+    def __enter__(self):
+        self.prev = lib().orc_apply_threads()
+        lib().orc_set_apply_threads(self.n)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_apply_threads(self.prev)
+        return False
 
 
 def _pd(a):

@@ -175,7 +175,8 @@ def test_plain_lanczos_and_bp_dos_match_oracle():
         a, b, n = A.lanczos(gop, l0, 12)
         v0 = np.zeros(oop.dim)
         v0[l0 - 1] = 1.0
-        ao, bo, no = oop.lanczos(v0, 12)
+        with O.apply_threads():   # 2.8 M nodes: the oracle's node loops on every host thread (the same bits)
+            ao, bo, no = oop.lanczos(v0, 12)
         assert n == no
         assert np.max(np.abs(a[:n] - ao[:n]) / np.abs(ao[:n])) < 1e-9
         assert np.max(np.abs(b[:n] - bo[:n]) / np.abs(bo[:n])) < 1e-9

@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 from asr_b200 import synthetic as S
+from tests import cases as K
 from oracle import oracle as O
 
 
@@ -82,3 +83,20 @@ def test_reduced_edc_chain_equals_the_dense_unreduced_inverse():
             gc = opr.edc_green(ed, z, l0, 600, tail="none")[0]
             worst = max(worst, abs(gc - gd) / abs(gd))
     assert worst < 1e-9, worst
+
+
+def test_threaded_node_loops_give_the_same_bits():
+    """The oracle's node loops on several host threads (oracle.apply_threads) give the serial chain bit for bit."""
+    case = K.cubic("bcc", 3, 2, (0.5, 0.5), group="d2h", maxlevel=2)
+    oop = O.OracleOp(case["graph"], case["model"], case["cls"], case["perm"], case["dmat"], 1, case["maxlevel"],
+                     case["maxrank"], case["flippable"])
+    c, d, o, e = S.plain_params(S.draw_species(2, 0))
+    oop.set_params(c, d, o + 0.01, e + 0.02)
+    oop.set_start(1)
+    v0 = np.zeros(oop.dim)
+    v0[0] = 1.0
+    ref = oop.lanczos(v0, 10)
+    with O.apply_threads(4):
+        got = oop.lanczos(v0, 10)
+    assert O.lib().orc_apply_threads() == 1
+    assert np.array_equal(ref[0], got[0]) and np.array_equal(ref[1], got[1]) and ref[2] == got[2]
