@@ -89,7 +89,7 @@ def chains_adjoint(op: AugclsOp, specs, z, w, tail: str = "hull", precision: str
     grad[q, kind, s, l] = sum_j w[j, q] dG[j, q] / dpar_kind(l, s) of group q, kind 0: c (equally e and pb, which enter
     as c + e + pb), 1: d, 2: pa.  w (nz, ngroup) complex seeds.  stride > 0: Lanczos vectors kept every ``stride``
     levels and recomputed in between; 0: every level kept when it fits in half the free device memory, else every
-    ceil(sqrt(depth)) levels (the same gradient either way; bitwise the same on the operators of the stride tests)."""
+    ceil(sqrt(depth)) levels (the same G; the same gradient to rounding, bitwise on the operators of the stride tests)."""
     z = np.ascontiguousarray(np.atleast_1d(z), dtype=np.complex128)
     nz = z.shape[0]
     ng = len(specs)

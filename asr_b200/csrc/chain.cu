@@ -1767,8 +1767,8 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   if (mmax > NLMAX) { set_error("adjoint: depth above %d", NLMAX); return ASR_EINVAL; }
   // Vectors kept for the reverse sweep: every level's (keep = true, no recomputation) when the caller leaves the stride
   // to the library and a batch of at least 4 tiles fits in half the free device memory; else checkpoints every c
-  // levels (c = stride, or ceil(sqrt(depth))) with the segments recomputed.  Both give the same gradient (bitwise the
-  // same on the operators of the stride tests).
+  // levels (c = stride, or ceil(sqrt(depth))) with the segments recomputed.  Both give the same G and the same gradient
+  // to rounding (bitwise on the operators of the stride tests).
   size_t freeb0 = 0, totb0 = 0;
   cudaMemGetInfo(&freeb0, &totb0);
   freeb0 += ctx->ws_bytes;   // a held slab is this call's to reuse
