@@ -32,8 +32,9 @@ _TAB = 18 * 5 + 3 * 5 + 20
 NCU_STEP_TRAFFIC = {
     ("fp64", "fixed-offset"): (3.171e9, 16 * 20969 * (2 * 4608.0 + _TAB),
                                "ncu capture of k_smul<double,1,1,1> (fixed-offset link gathers, a_k epilogue) at 16 tiles"),
-    ("fp32", "fixed-offset"): (0.770e9, 8 * 20969 * (2 * 2304.0 + _TAB),
-                               "ncu capture of k_smul<float,1,1,1> (fixed-offset link gathers, a_k epilogue) at 8 tiles"),
+    ("fp32", "fixed-offset"): (0.762e9, 8 * 20969 * (2 * 2304.0 + _TAB),
+                               "ncu capture of k_smul<float,1,1,1> (fixed-offset link gathers, a_k epilogue, paired FMAs) at "
+                               "8 tiles"),
     ("fp64", "general"): (3.30e9, 16 * 20969 * (2 * 4608.0 + _TAB),
                           "ncu capture of the general-link k_smul<double,1,1,0> at 16 tiles (before the a_k epilogue)"),
 }
