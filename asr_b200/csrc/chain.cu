@@ -1224,6 +1224,7 @@ int run_lanes_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, c
     ASR_CUDA(cudaEventRecord(tev[0], s));
   }
   for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
+    NvtxRange batch_range("chain batch");
     const int nt = std::min(tpb, ntile_all - t0);
     int kmax = 0;
     std::vector<int> tact(tpb, 0), ones(nlp, 0), tgroup(tpb, -1);
@@ -1877,6 +1878,9 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
   OpView ov = op->view();
   const ST* blk = std::is_same<ST, double>::value ? (const ST*)op->d_blocks : (const ST*)op->d_blocks_f;
   for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
+    NvtxRange batch_range("adjoint batch");
+    NvtxPhase phase;
+    phase.next("adjoint forward");
     const int nt = std::min(tpb, ntile_all - t0);
     std::vector<int> tact(tpb, 0), act(nlp, 0), tgroup(tpb, -1);
     for (int q = 0; q < nlp; ++q) {
@@ -1992,6 +1996,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
     // the forward retired finished tiles; the recomputation visits every tile of the batch, the reverse step k the tiles
     // with a lane at least k deep (k_adj_scal)
     ASR_CUDA(cudaMemcpyAsync(d_tact.p, d_tact0.p, tpb * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    phase.next("fraction adjoint (host)");
     // ---- fraction adjoint on the host: G and the seeds abar, bbar
     ASR_CUDA(cudaMemcpyAsync(hm.data(), d_m.p, nlp * sizeof(int), cudaMemcpyDeviceToHost, s));
     ASR_CUDA(cudaMemcpyAsync(ha.data(), d_a.p, ha.size() * sizeof(double2), cudaMemcpyDeviceToHost, s));
@@ -2026,6 +2031,7 @@ int run_adjoint_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo,
       ASR_CUDA(cudaMemsetAsync(d_d1.p, 0, nlp * sizeof(double2), s));
     }
     T2* WBF[2] = {WB, YB};
+    phase.next("adjoint reverse");
     for (int j = nseg - 1; j >= 0; --j) {
       const int k0 = 1 + j * c, k1 = std::min(kmax, k0 + c - 1);
       if (k0 > kmax) continue;
@@ -2448,6 +2454,7 @@ int run_ed3_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
     return ASR_OK;
   };
   for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
+    NvtxRange batch_range("ed3 batch");
     const int nt = std::min(tpb, ntile_all - t0);
     std::vector<int> tact(tpb, 0), act(nlp, 0), tgroup(tpb, -1);
     for (int q = 0; q < nlp; ++q) {
@@ -2679,6 +2686,7 @@ int run_epi_t(asr_ctx* ctx, asr_op* op, const std::vector<GroupInfo>& ginfo, con
   std::vector<double> hnv(nlp);
   ASR_CUDA(cudaMemsetAsync(d_nfall.p, 0, sizeof(int), s));
   for (int t0 = 0; t0 < ntile_all; t0 += tpb) {
+    NvtxRange batch_range("epi batch");
     const int nt = std::min(tpb, ntile_all - t0);
     std::vector<int> tact(tpb, 0), act(nlp, 0), tgroup(tpb, -1);
     for (int q = 0; q < nlp; ++q) {

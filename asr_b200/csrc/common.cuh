@@ -1,6 +1,7 @@
 // Shared definitions of the asr_b200 CUDA library (sm_100a).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -49,8 +50,31 @@ struct DeviceGuard {
     if (prev >= 0) cudaSetDevice(prev);
   }
 };
-#define ASR_ON_DEVICE(dev)       \
-  ::asrb::DeviceGuard dguard_;   \
+// NVTX range over a scope (an ABI call, a chain batch): names the span on the timeline of a profiler (nsys, ncu
+// --nvtx); without one attached the calls do nothing
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+// consecutive named phases inside one scope: next() ends the open phase and starts the next; the last ends with the scope
+struct NvtxPhase {
+  bool open = false;
+  void next(const char* name) {
+    if (open) nvtxRangePop();
+    nvtxRangePushA(name);
+    open = true;
+  }
+  ~NvtxPhase() {
+    if (open) nvtxRangePop();
+  }
+};
+
+// every entry point that works on a device: an NVTX range named after the entry point, and its device made current
+#define ASR_ON_DEVICE(dev)                  \
+  ::asrb::NvtxRange nvtx_call_(__func__);   \
+  ::asrb::DeviceGuard dguard_;              \
   ASR_TRY(dguard_.set(dev))
 
 // device error codes written into a flag word (the first error wins)
