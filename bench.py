@@ -77,8 +77,8 @@ def parse():
                         "small cluster, 3 converged at full size")
     p.add_argument("--autotune", type=int, default=1, help="choose the batch shape by timing first (1) or use the defaults (0)")
     p.add_argument("--legs", default="1",
-                   help="1: measure every leg (mixed precision with its DOS error, adjoint, KPM, plain, example, spectral, "
-                        "EPI), 0: none, or a comma list of leg names")
+                   help="1: measure every leg (mixed precision with its DOS error, adjoint, general operator form, KPM, "
+                        "plain, example, spectral, EPI), 0: none, or a comma list of leg names")
     p.add_argument("--lanes", type=int, default=0,
                    help="1: run the multi-GPU step (task split, lane chains, all-reduce of the shares) also on one GPU")
     p.add_argument("--adj-groups", type=int, default=0, help="adjoint leg: the first N chain groups (0: all 54)")
@@ -542,7 +542,56 @@ def heusler_leg(torch):
             "forward_chain_steps_per_s": chains * 20 / t_fwd, "jacobian_norm": float(np.linalg.norm(np.array(jac)))}
 
 
-LEGS = ("mixed", "adjoint", "heusler", "kpm", "plain", "example", "spectral", "epi")
+def general_leg(args, A, op, groups, z_all, stream):
+    """The reference's whole operator form on the workload: edc_setup's o (o_l D_s / D_c, src/asr_edc.f90:66, with o_l
+    drawn per spin from the spin's seed) in every group, so each chain step applies H = E_nu + h - h o h + X(z) as the
+    unfused kernel sequence with two S applications.  FP64 chain-steps/s over one slice of real-axis energies next to the
+    fused o = 0 step on the same slice, and the device time of the step's kernels per launch."""
+    import torch
+    from asr_b200 import synthetic as S
+    nzs = args.nz_slice
+    zs = z_all[48: 48 + nzs]
+    specs_o = []
+    for g in groups:
+        sp = S.draw_species(3, seed=1 + g["spin"])
+        ed = S.edc_params_o(sp, S.draw_o(3, 1 + g["spin"]), g["cen"])
+        specs_o.append(A.ChainSpec(c=ed["c"], d=ed["d"], o=ed["o"], e=ed["e"], pa=ed["pa"], pb=ed["pb"], frozen_sp=g["cen"],
+                                   start_orb=g["l0"], nlev=g["nlev"]))
+    steps = int(sum(g["nlev"] for g in groups)) * nzs
+    out = {"energies": nzs, "groups": len(groups), "precision": "fp64",
+           "o": "edc_setup's o = o_l D_s / D_c, o_l = synthetic.draw_o(3, 1 + spin)"}
+    op.ctx.hold_workspace(True)
+    try:
+        for name, sp_ in (("o_edc_setup", specs_o), ("o_zero", specs_of(groups))):
+            A.chains_run(op, sp_, zs[:32], "edc", 0.0, "hull", "fp64")   # kernels loaded, workspace sized
+            torch.cuda.synchronize()
+            op.ctx.profile(True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            A.chains_run(op, sp_, zs, "edc", 0.0, "hull", "fp64")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            op.ctx.profile(False)
+            ms = e0.elapsed_time(e1)
+            st = op.ctx.kernel_stats("step")
+            out[name] = {"chain_steps_per_s": steps / (ms / 1000.0), "ms": ms, "operator_ms": st["ms"],
+                         "operator_launches": st["launches"],
+                         "operator_ms_per_launch": st["ms"] / max(st["launches"], 1)}
+    finally:
+        op.ctx.hold_workspace(False)
+    out["o_zero_over_o_edc_setup"] = out["o_zero"]["chain_steps_per_s"] / out["o_edc_setup"]["chain_steps_per_s"]
+    return out
+
+
+def guarded(fn, *a):
+    """A leg that raises is reported in the line (its error message) instead of ending the run."""
+    try:
+        return fn(*a)
+    except Exception as e:
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
+LEGS = ("mixed", "adjoint", "general", "heusler", "kpm", "plain", "example", "spectral", "epi")
 
 
 def contour_weights(z_all):
@@ -668,6 +717,8 @@ def run_legs(args, A, op, specs, groups, z_all, step, stream, world):
         out.update(mixed_leg(args, A, op, specs, groups, z_all, step, stream, world))
     if "adjoint" in want:
         out["adjoint"] = adjoint_leg(args, A, op, specs, groups, z_all, stream)
+    if "general" in want:
+        out["general"] = guarded(general_leg, args, A, op, groups, z_all, stream)
     out["fp64_peak_tflops"] = fp64_peak_tflops(torch)
     out["fp32_peak_tflops"] = fp32_peak_tflops(torch)
     if "kpm" in want:
