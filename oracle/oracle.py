@@ -97,7 +97,7 @@ class apply_threads:
     results are the same bits as on one thread; only single-chain oracle calls use it (chain_greens' tasks stay serial)."""
 
     def __init__(self, n: int = 0):
-        self.n = n if n > 0 else (os.cpu_count() or 1)
+        self.n = n if n > 0 else len(os.sched_getaffinity(0))
 
     def __enter__(self):
         self.prev = lib().orc_apply_threads()
